@@ -1,0 +1,140 @@
+/* harmony_b200.h -- C ABI of the B200 Harmony integration engine (sm_100a).
+ *
+ * Every entry point takes plain device pointers, sizes and a cudaStream_t
+ * (passed as void*) and returns an int status.  On failure hb_last_error()
+ * returns a message for the calling thread.  The library never allocates
+ * device memory: callers pass a workspace of hb_plan_workspace_bytes() bytes,
+ * mirroring the caller-allocated workspaces of the reference
+ * (src/rapids_singlecell/preprocessing/_harmony/__init__.py:356-384,593-599,648-656).
+ *
+ * Reference interfaces replaced (paths inside the rapids_singlecell tree):
+ *   hb_harmonize          -> harmonize() driving _harmony_clustering_cuda.clustering_loop and
+ *                            _harmony_correction_batched_cuda.correction_batched
+ *                            (preprocessing/_harmony/__init__.py:41-289;
+ *                             _cuda/harmony/clustering/clustering.cu:397-469;
+ *                             _cuda/harmony/correction/correction_batched.cu:134-164)
+ *   hb_l2_normalize       -> _harmony_normalize_cuda.l2_row_normalize
+ *                            (_cuda/harmony/normalize/kernels_normalize.cuh:7-54)
+ *   hb_block_lists        -> pcg_hash_kernel + iota + cub::DeviceRadixSort::SortPairs
+ *                            (_cuda/harmony/clustering/clustering.cu:292-305)
+ *   hb_penalty            -> _harmony_pen_cuda.penalty (_cuda/harmony/pen/kernels_pen.cuh:8-21)
+ *   hb_ridge_inverse      -> _harmony_correction_cuda.compute_inv_mat
+ *                            (_cuda/harmony/correction/kernels_correction_fast.cuh:24-123)
+ *   hb_lambda_kb          -> _compute_lambda_kb (preprocessing/_harmony/__init__.py:454-480)
+ */
+#ifndef HARMONY_B200_H
+#define HARMONY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define HB_API __attribute__((visibility("default")))
+#else
+#define HB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define HB_OK 0
+#define HB_ERR_INVALID 1      /* bad argument (shape, parameter range)            */
+#define HB_ERR_WORKSPACE 2    /* workspace smaller than hb_plan_workspace_bytes()  */
+#define HB_ERR_TIMEOUT 3      /* a bounded device-side wait gave up               */
+#define HB_ERR_CUDA 4         /* CUDA runtime error                                */
+#define HB_ERR_INTERNAL 5     /* device-side consistency check failed             */
+#define HB_ERR_UNSUPPORTED 6  /* size outside the engine's supported range        */
+
+/* arithmetic of the soft k-means (storage of Z_norm and R) */
+#define HB_FP32 0  /* plain float32, the drop-in for harmony_integrate(dtype=np.float32) */
+#define HB_FP64 1  /* plain float64, the drop-in for the reference default dtype         */
+#define HB_BF16 2  /* bf16 Z_norm / R, tensor-core similarity + centroids, fp32 accumulate */
+#define HB_FP16 3  /* fp16 Z_norm / R, tensor-core similarity + centroids, fp32 accumulate */
+
+typedef struct hb_params {
+  int64_t n_cells;
+  int32_t n_pcs;
+  int32_t n_clusters;
+  int32_t n_batches;
+  int32_t precision;            /* HB_FP32 ... HB_FP16 */
+  int64_t block_size;           /* int(n_cells * block_proportion), >= 1 */
+  int32_t max_iter_harmony;
+  int32_t max_iter_clustering;
+  double tol_harmony;
+  double tol_clustering;
+  double sigma;
+  double ridge_lambda;
+  double alpha;
+  double batch_prune_threshold; /* used when prune != 0 */
+  int32_t prune;                /* batch_prune_threshold is not None */
+  int32_t stabilized_penalty;   /* harmony2 penalty */
+  int32_t dynamic_lambda;       /* harmony2 lambda = alpha * E */
+  int32_t reserved;
+  uint64_t random_state;
+} hb_params;
+
+typedef struct hb_plan hb_plan;
+
+/* Outputs of one run (host memory owned by the caller). */
+typedef struct hb_outputs {
+  double* objectives;         /* [1 + max_iter_harmony]: initial + one per outer iteration */
+  int32_t* n_objectives;
+  double* kmeans_objectives;  /* optional [max_iter_harmony * max_iter_clustering] */
+  int32_t* kmeans_iters;      /* optional [max_iter_harmony]: k-means iterations run per outer */
+  int32_t* converged;         /* 1 if the outer loop met tol_harmony */
+} hb_outputs;
+
+HB_API int hb_plan_create(const hb_params* params, hb_plan** plan);
+HB_API void hb_plan_destroy(hb_plan* plan);
+HB_API size_t hb_plan_workspace_bytes(const hb_plan* plan);
+
+/* Full Harmony integration of one problem.
+ *   X             device [n_cells, n_pcs] row-major; float64 for HB_FP64, else float32
+ *   cats          device int32 [n_cells] batch code per cell (0 .. n_batches-1)
+ *   cell_index    device int32 [n_cells] cells sorted by batch (stable)
+ *   batch_offsets host int64 [n_batches + 1] CSR offsets into cell_index
+ *   theta         host float64 [n_batches] (tau discount already applied)
+ *   Y0            device [n_clusters, n_pcs] initial centroids, same dtype as X
+ *   Z_hat         device [n_cells, n_pcs] output, same dtype as X
+ */
+HB_API int hb_harmonize(hb_plan* plan, const void* X, const int32_t* cats, const int32_t* cell_index,
+                 const int64_t* batch_offsets, const double* theta, const void* Y0,
+                 void* workspace, size_t workspace_bytes, void* Z_hat, hb_outputs* out,
+                 void* stream);
+
+/* ---- kernel-level entry points (the reference's per-kernel bindings) ---- */
+
+/* dst[r, :cols] = src[r, :cols] * min(rsqrt(sum src^2), 1e12); dtype HB_FP32 / HB_FP64 */
+HB_API int hb_l2_normalize(const void* src, void* dst, int64_t rows, int32_t cols, int32_t dtype,
+                    void* stream);
+
+/* Cell lists of every block of `n_iters` k-means iterations (seeds given on the host):
+ * idx[c*n + j*block_size + r] = r-th cell (ascending index) of block j for seed c. */
+HB_API size_t hb_block_lists_workspace_bytes(int64_t n, int64_t block_size);
+HB_API int hb_block_lists(int64_t n, int64_t block_size, const uint32_t* seeds, int32_t n_iters,
+                   int32_t* idx, void* workspace, size_t workspace_bytes, void* stream);
+
+/* penalty[b,k] = ((E+1)/(O[+E]+1)) ** theta[b]; float64 arrays [B,K], theta [B] */
+HB_API int hb_penalty(const double* E, const double* O, const double* theta, double* penalty,
+               int32_t n_batches, int32_t n_clusters, int32_t stabilized, void* stream);
+
+/* lambda[b,k] per _compute_lambda_kb; float64 [B,K], N_b [B] */
+HB_API int hb_lambda_kb(const double* E, const double* O, const double* N_b, double* lambda_kb,
+                 int32_t n_batches, int32_t n_clusters, double alpha, double threshold,
+                 int32_t prune, double ridge_lambda, int32_t dynamic_lambda, void* stream);
+
+/* inv[k] = closed-form inverse of [[N_k, O_k^T],[O_k, diag(O_k + lambda_k)]], float64,
+ * inv is [n_clusters, n_batches+1, n_batches+1] */
+HB_API int hb_ridge_inverse(const double* O, const double* lambda_kb, double* inv, int32_t n_batches,
+                     int32_t n_clusters, void* stream);
+
+HB_API const char* hb_last_error(void);
+HB_API const char* hb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HARMONY_B200_H */

@@ -1,0 +1,425 @@
+// Plan, workspace layout and the Harmony iteration driver behind the C ABI.
+//
+// The loop structure follows harmonize() (preprocessing/_harmony/__init__.py:
+// 41-289) and clustering_loop_impl (_cuda/harmony/clustering/clustering.cu:
+// 241-393); the kernels it launches are this engine's own (hb_simt.cu,
+// hb_membership.cu).
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+#include "hb_internal.h"
+
+namespace hb {
+
+static thread_local char g_err[1024] = "";
+
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+int num_sms() {
+  int dev = 0, v = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess)
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+  return v > 0 ? v : 148;
+}
+
+}  // namespace hb
+
+using namespace hb;
+
+struct hb_plan {
+  hb_params p;
+  int esz;        // bytes of the plain compute type (4 or 8)
+  int ldz, ldr, ldy;
+  MembershipLayout ml;
+  int cen_chunks; // split-n chunks of the centroid sum
+  int cen_tiles;  // output tiles per chunk
+  int max_m_chunks, max_apply_tiles;
+  int64_t m_chunk_len;
+  size_t ws_bytes;
+};
+
+namespace {
+
+struct Work {
+  void* Zn;
+  void* R;
+  void* Yn;
+  void* Ypart;
+  void* Mpart;
+  void* W;
+  double* O[3];
+  double* Pr;
+  double* theta;
+  double* Nb;
+  double* obj_acc;
+  double* obj_out;
+  double* M;
+  int32_t* idx;
+  AccumChunk* cen_chunks;
+  AccumChunk* m_chunks;
+  int32_t* batch_chunk_off;
+  ApplyTile* apply_tiles;
+  MembershipBufs mb;
+};
+
+void carve(const hb_plan& P, Carver& cv, Work& w) {
+  const hb_params& p = P.p;
+  const int64_t n = p.n_cells;
+  const int K = p.n_clusters, B = p.n_batches, d = p.n_pcs;
+  const int e = P.esz;
+  w.Zn = cv.take<char>((size_t)n * P.ldz * e);
+  w.R = cv.take<char>((size_t)n * P.ldr * e);
+  w.Yn = cv.take<char>((size_t)K * P.ldy * e);
+  w.Ypart = cv.take<char>((size_t)P.cen_chunks * K * d * e);
+  w.Mpart = cv.take<char>((size_t)P.max_m_chunks * K * d * e);
+  w.W = cv.take<char>((size_t)B * K * d * e);
+  for (int i = 0; i < 3; ++i) w.O[i] = cv.take<double>((size_t)B * K);
+  w.Pr = cv.take<double>(B);
+  w.theta = cv.take<double>(B);
+  w.Nb = cv.take<double>(B);
+  w.obj_acc = cv.take<double>(1);
+  w.obj_out = cv.take<double>(std::max(p.max_iter_clustering, 1) + 1);
+  w.M = cv.take<double>((size_t)K * (B + 1) * d);
+  w.idx = cv.take<int32_t>((size_t)kMaxIterChunk * n);
+  w.cen_chunks = cv.take<AccumChunk>(P.cen_chunks);
+  w.m_chunks = cv.take<AccumChunk>(P.max_m_chunks);
+  w.batch_chunk_off = cv.take<int32_t>(B + 1);
+  w.apply_tiles = cv.take<ApplyTile>(P.max_apply_tiles);
+  membership_carve(cv, P.ml, w.mb);
+}
+
+int validate(const hb_params& p) {
+  if (p.n_cells < 1 || p.n_cells > 2147483647LL) { set_error("n_cells must be in [1, 2^31)"); return HB_ERR_INVALID; }
+  if (p.n_pcs < 1) { set_error("n_pcs must be >= 1"); return HB_ERR_INVALID; }
+  if (p.n_clusters < 1) { set_error("n_clusters must be >= 1"); return HB_ERR_INVALID; }
+  if (p.n_batches < 1) { set_error("n_batches must be >= 1"); return HB_ERR_INVALID; }
+  if (p.block_size < 1) { set_error("block_size = int(n_cells * block_proportion) must be >= 1"); return HB_ERR_INVALID; }
+  if (p.max_iter_harmony < 1) { set_error("max_iter_harmony must be >= 1"); return HB_ERR_INVALID; }
+  if (p.max_iter_clustering < 0) { set_error("max_iter_clustering must be >= 0"); return HB_ERR_INVALID; }
+  if (!(p.sigma > 0)) { set_error("sigma must be > 0"); return HB_ERR_INVALID; }
+  const int64_t nblk = (p.n_cells + p.block_size - 1) / p.block_size;
+  if (nblk > kMaxBlocks) {
+    set_error("block_proportion too small: %lld blocks per iteration (max %d)", (long long)nblk, kMaxBlocks);
+    return HB_ERR_UNSUPPORTED;
+  }
+  if (p.n_clusters > 256) { set_error("n_clusters=%d exceeds the supported maximum of 256", p.n_clusters); return HB_ERR_UNSUPPORTED; }
+  if (p.precision == HB_FP64 && p.n_pcs > 128) { set_error("n_pcs=%d exceeds 128 for float64", p.n_pcs); return HB_ERR_UNSUPPORTED; }
+  if (p.n_pcs > 256) { set_error("n_pcs=%d exceeds the supported maximum of 256", p.n_pcs); return HB_ERR_UNSUPPORTED; }
+  if (p.precision != HB_FP32 && p.precision != HB_FP64) {
+    set_error("precision %d is not available in this build", p.precision);
+    return HB_ERR_UNSUPPORTED;
+  }
+  const size_t smem = (size_t)(p.precision == HB_FP64 ? 8 : 4) * 2 * p.n_batches * p.n_clusters;
+  if (smem > 160 * 1024) {
+    set_error("n_batches * n_clusters = %d too large (shared-memory O/penalty tables)", p.n_batches * p.n_clusters);
+    return HB_ERR_UNSUPPORTED;
+  }
+  if (MembershipLayout ml = membership_layout(p.n_cells, p.block_size); ml.cap > 16384) {
+    set_error("n_cells=%lld too large for the block splitter select", (long long)p.n_cells);
+    return HB_ERR_UNSUPPORTED;
+  }
+  return HB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* hb_last_error(void) { return g_err; }
+const char* hb_version(void) { return "harmony_b200 0.1 (sm_100a)"; }
+
+int hb_plan_create(const hb_params* params, hb_plan** plan) {
+  if (!params || !plan) { set_error("null argument"); return HB_ERR_INVALID; }
+  HB_TRY(validate(*params));
+  hb_plan* P = new hb_plan();
+  P->p = *params;
+  const hb_params& p = P->p;
+  P->esz = p.precision == HB_FP64 ? 8 : 4;
+  const int vec = 16 / P->esz;
+  P->ldz = (int)align_up(p.n_pcs, vec);
+  P->ldr = (int)align_up(p.n_clusters, vec);
+  P->ldy = P->ldz;
+  P->ml = membership_layout(p.n_cells, p.block_size);
+  const int sms = num_sms();
+  P->cen_tiles = div_up(p.n_clusters, 128) * div_up(p.n_pcs, 64);
+  const int64_t target = std::max(1, 2 * sms / P->cen_tiles);
+  P->cen_chunks = (int)std::max<int64_t>(1, std::min<int64_t>(target, (p.n_cells + 255) / 256));
+  P->m_chunk_len = std::max<int64_t>(256, (p.n_cells + target - 1) / target);
+  P->max_m_chunks = (int)((p.n_cells + P->m_chunk_len - 1) / P->m_chunk_len) + p.n_batches;
+  P->max_apply_tiles = (int)((p.n_cells + 31) / 32) + p.n_batches;
+  Carver cv(nullptr, 0);
+  Work w;
+  carve(*P, cv, w);
+  P->ws_bytes = cv.off + 256;
+  *plan = P;
+  return HB_OK;
+}
+
+void hb_plan_destroy(hb_plan* plan) { delete plan; }
+
+size_t hb_plan_workspace_bytes(const hb_plan* plan) { return plan ? plan->ws_bytes : 0; }
+
+}  // extern "C"
+
+namespace {
+
+template <typename T>
+int block_update(const BlockArgs& a, const double* in, double* out, double* zero, cudaStream_t st) {
+  if (sizeof(T) == 8) return launch_block_update_f64(a, in, out, zero, st);
+  return launch_block_update_f32(a, in, out, zero, st);
+}
+
+struct ORing {
+  double* buf[3];
+  int cur = 0;
+  // launch a block update that reads the current state and produces the next
+  template <typename T>
+  int step(const BlockArgs& a, cudaStream_t st) {
+    const int out = (cur + 1) % 3, zero = (cur + 2) % 3;
+    HB_TRY(block_update<T>(a, buf[cur], buf[out], buf[zero], st));
+    cur = out;
+    return HB_OK;
+  }
+  double* state() const { return buf[cur]; }
+};
+
+template <typename T>
+int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_index,
+             const int64_t* batch_offsets, const double* theta, const T* Y0, void* ws,
+             size_t ws_bytes, T* Zhat, hb_outputs* out, cudaStream_t st) {
+  const hb_params& p = P->p;
+  const int64_t n = p.n_cells;
+  const int K = p.n_clusters, B = p.n_batches, d = p.n_pcs;
+  if (ws_bytes < P->ws_bytes || !ws) {
+    set_error("workspace too small: %zu < %zu", ws_bytes, P->ws_bytes);
+    return HB_ERR_WORKSPACE;
+  }
+  Carver cv((void*)align_up((size_t)ws, 256), ws_bytes - 256);
+  Work w;
+  carve(*P, cv, w);
+
+  // ---- host-side tables ----------------------------------------------------
+  std::vector<double> Nb(B), Pr(B), th(theta, theta + B);
+  for (int b = 0; b < B; ++b) {
+    Nb[b] = (double)(batch_offsets[b + 1] - batch_offsets[b]);
+    Pr[b] = Nb[b] / (double)n;
+  }
+  if (batch_offsets[0] != 0 || batch_offsets[B] != n) {
+    set_error("batch_offsets must start at 0 and end at n_cells");
+    return HB_ERR_INVALID;
+  }
+  std::vector<AccumChunk> cen(P->cen_chunks);
+  {
+    const int64_t len = (n + P->cen_chunks - 1) / P->cen_chunks;
+    for (int c = 0; c < P->cen_chunks; ++c) {
+      int64_t s = c * len, e = std::min<int64_t>(n, s + len);
+      cen[c] = AccumChunk{s, (int32_t)std::max<int64_t>(0, e - s), 0};
+    }
+  }
+  std::vector<AccumChunk> mch;
+  std::vector<int32_t> bco(B + 1, 0);
+  std::vector<ApplyTile> tiles;
+  for (int b = 0; b < B; ++b) {
+    bco[b] = (int32_t)mch.size();
+    for (int64_t s = batch_offsets[b]; s < batch_offsets[b + 1]; s += P->m_chunk_len)
+      mch.push_back(AccumChunk{s, (int32_t)std::min<int64_t>(P->m_chunk_len, batch_offsets[b + 1] - s), b});
+    for (int64_t s = batch_offsets[b]; s < batch_offsets[b + 1]; s += 32)
+      tiles.push_back(ApplyTile{s, (int32_t)std::min<int64_t>(32, batch_offsets[b + 1] - s), b});
+  }
+  bco[B] = (int32_t)mch.size();
+  HB_CUDA(cudaMemcpyAsync(w.Nb, Nb.data(), sizeof(double) * B, cudaMemcpyHostToDevice, st));
+  HB_CUDA(cudaMemcpyAsync(w.Pr, Pr.data(), sizeof(double) * B, cudaMemcpyHostToDevice, st));
+  HB_CUDA(cudaMemcpyAsync(w.theta, th.data(), sizeof(double) * B, cudaMemcpyHostToDevice, st));
+  HB_CUDA(cudaMemcpyAsync(w.cen_chunks, cen.data(), sizeof(AccumChunk) * cen.size(), cudaMemcpyHostToDevice, st));
+  if (!mch.empty())
+    HB_CUDA(cudaMemcpyAsync(w.m_chunks, mch.data(), sizeof(AccumChunk) * mch.size(), cudaMemcpyHostToDevice, st));
+  HB_CUDA(cudaMemcpyAsync(w.batch_chunk_off, bco.data(), sizeof(int32_t) * (B + 1), cudaMemcpyHostToDevice, st));
+  if (!tiles.empty())
+    HB_CUDA(cudaMemcpyAsync(w.apply_tiles, tiles.data(), sizeof(ApplyTile) * tiles.size(), cudaMemcpyHostToDevice, st));
+  for (int i = 0; i < 3; ++i) HB_CUDA(cudaMemsetAsync(w.O[i], 0, sizeof(double) * B * K, st));
+  HB_CUDA(cudaMemsetAsync(w.obj_acc, 0, sizeof(double), st));
+
+  T* Zn = (T*)w.Zn;
+  T* R = (T*)w.R;
+  T* Yn = (T*)w.Yn;
+  ORing ring{{w.O[0], w.O[1], w.O[2]}, 0};
+
+  BlockArgs base{};
+  base.Zn = Zn; base.ldz = P->ldz; base.R = R; base.ldr = P->ldr; base.cats = cats;
+  base.Yn = Yn; base.ldy = P->ldy; base.Pr = w.Pr; base.theta = w.theta; base.obj_acc = w.obj_acc;
+  base.sigma = p.sigma; base.d = d; base.K = K; base.B = B; base.stabilized = p.stabilized_penalty;
+
+  // ---- initial state (_harmony/__init__.py:292-353) ------------------------
+  HB_TRY(launch_l2_normalize<T, T>(X, n, d, d, Zn, P->ldz, st));
+  HB_TRY(launch_l2_normalize<T, T>(Y0, K, d, d, Yn, P->ldy, st));
+  {
+    BlockArgs a = base;
+    a.idx_new = nullptr; a.new_start = 0; a.n_new = n; a.idx_old = nullptr; a.n_old = 0;
+    a.init_mode = 1;
+    HB_TRY(ring.step<T>(a, st));
+  }
+  HB_TRY(launch_objective_finalize(ring.state(), w.Pr, w.theta, p.sigma, B, K, p.stabilized_penalty,
+                                   w.obj_acc, w.obj_out, st));
+  double h_obj = 0;
+  HB_CUDA(cudaMemcpyAsync(&h_obj, w.obj_out, sizeof(double), cudaMemcpyDeviceToHost, st));
+  HB_CUDA(cudaStreamSynchronize(st));
+  std::vector<double> objs{h_obj};
+  int converged = 0;
+  const MembershipLayout& ml = P->ml;
+  const int nblk = ml.nblk;
+  std::vector<uint32_t> seeds(kMaxIterChunk);
+  std::vector<double> kobj;
+
+  for (int outer = 0; outer < p.max_iter_harmony; ++outer) {
+    const uint32_t seed = (uint32_t)((p.random_state + (uint64_t)outer * 1000003ull) & 0xffffffffull);
+    kobj.clear();
+    bool stop = false;
+    for (int it0 = 0; it0 < p.max_iter_clustering && !stop; it0 += kMaxIterChunk) {
+      const int C = std::min(kMaxIterChunk, p.max_iter_clustering - it0);
+      for (int c = 0; c < C; ++c) seeds[c] = seed + (uint32_t)(it0 + c);
+      HB_TRY(membership_build(ml, w.mb, seeds.data(), C, w.idx, st));
+      for (int c = 0; c < C && !stop; ++c) {
+        const int32_t* idx = w.idx + (size_t)c * n;
+        // centroids Y = R^T Z_norm, L2-normalised (clustering.cu:272-281)
+        HB_TRY(launch_accum<T, T, T>(R, P->ldr, Zn, P->ldz, nullptr, w.cen_chunks, P->cen_chunks, K, d,
+                                     (T*)w.Ypart, st));
+        HB_TRY(launch_centroid_reduce<T, T>((T*)w.Ypart, P->cen_chunks, K, d, Yn, P->ldy, st));
+        // remove block 0's current rows, then sweep the blocks (clustering.cu:308-372)
+        {
+          BlockArgs a = base;
+          a.n_new = 0; a.idx_new = nullptr;
+          a.idx_old = idx; a.n_old = std::min<int64_t>(ml.bs, n);
+          HB_TRY(ring.step<T>(a, st));
+        }
+        for (int j = 0; j < nblk; ++j) {
+          BlockArgs a = base;
+          const int64_t s0 = (int64_t)j * ml.bs;
+          a.idx_new = idx + s0;
+          a.n_new = std::min<int64_t>(ml.bs, n - s0);
+          if (j + 1 < nblk) {
+            const int64_t s1 = s0 + ml.bs;
+            a.idx_old = idx + s1;
+            a.n_old = std::min<int64_t>(ml.bs, n - s1);
+          }
+          HB_TRY(ring.step<T>(a, st));
+        }
+        HB_TRY(launch_objective_finalize(ring.state(), w.Pr, w.theta, p.sigma, B, K,
+                                         p.stabilized_penalty, w.obj_acc, w.obj_out, st));
+        HB_CUDA(cudaMemcpyAsync(&h_obj, w.obj_out, sizeof(double), cudaMemcpyDeviceToHost, st));
+        HB_CUDA(cudaStreamSynchronize(st));
+        kobj.push_back(h_obj);
+        // window-3 convergence (clustering.cu:380-387)
+        const size_t m = kobj.size();
+        if (m >= 4) {
+          const double o = kobj[m - 2] + kobj[m - 3] + kobj[m - 4];
+          const double nw = kobj[m - 1] + kobj[m - 2] + kobj[m - 3];
+          if ((o - nw) < p.tol_clustering * std::fabs(o)) stop = true;
+        }
+      }
+    }
+    {
+      int err = 0;
+      HB_CUDA(cudaMemcpyAsync(&err, w.mb.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+      HB_CUDA(cudaStreamSynchronize(st));
+      if (err) { set_error("block splitter candidate buffer overflow"); return HB_ERR_INTERNAL; }
+    }
+    if (out && out->kmeans_objectives) {
+      for (size_t i = 0; i < kobj.size(); ++i)
+        out->kmeans_objectives[(size_t)outer * p.max_iter_clustering + i] = kobj[i];
+    }
+    if (out && out->kmeans_iters) out->kmeans_iters[outer] = (int32_t)kobj.size();
+    objs.push_back(kobj.empty() ? 0.0 : kobj.back());
+
+    // ---- ridge correction (correction_batched.cu:17-130) -------------------
+    HB_TRY(launch_accum<T, T, T>(R, P->ldr, X, d, cell_index, w.m_chunks, (int)mch.size(), K, d,
+                                 (T*)w.Mpart, st));
+    HB_TRY(launch_m_reduce<T>((T*)w.Mpart, mch.data(), (int)mch.size(), w.batch_chunk_off, K, B, d,
+                              w.M, st));
+    CorrArgs ca{w.M, ring.state(), w.Pr, w.Nb, p.alpha, p.ridge_lambda, p.batch_prune_threshold,
+                p.prune, p.dynamic_lambda, K, B, d};
+    HB_TRY(launch_ridge_solve<T>(ca, (T*)w.W, st));
+    HB_TRY(launch_apply_t<T, T, T>(X, d, R, P->ldr, (T*)w.W, cell_index, w.apply_tiles,
+                                   (int)tiles.size(), K, d, Zhat, d, Zn, P->ldz, st));
+    // outer convergence (_harmony/__init__.py:722-734)
+    const size_t m = objs.size();
+    if (m >= 2 && (objs[m - 2] - objs[m - 1]) < p.tol_harmony * std::fabs(objs[m - 2])) {
+      converged = 1;
+      break;
+    }
+  }
+  HB_CUDA(cudaStreamSynchronize(st));
+  if (out) {
+    if (out->objectives)
+      for (size_t i = 0; i < objs.size(); ++i) out->objectives[i] = objs[i];
+    if (out->n_objectives) *out->n_objectives = (int32_t)objs.size();
+    if (out->converged) *out->converged = converged;
+  }
+  return HB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hb_harmonize(hb_plan* plan, const void* X, const int32_t* cats, const int32_t* cell_index,
+                 const int64_t* batch_offsets, const double* theta, const void* Y0, void* workspace,
+                 size_t workspace_bytes, void* Z_hat, hb_outputs* out, void* stream) {
+  if (!plan || !X || !cats || !cell_index || !batch_offsets || !theta || !Y0 || !Z_hat) {
+    set_error("hb_harmonize: null argument");
+    return HB_ERR_INVALID;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plan->p.precision == HB_FP64)
+    return run_impl<double>(plan, (const double*)X, cats, cell_index, batch_offsets, theta,
+                            (const double*)Y0, workspace, workspace_bytes, (double*)Z_hat, out, st);
+  return run_impl<float>(plan, (const float*)X, cats, cell_index, batch_offsets, theta,
+                         (const float*)Y0, workspace, workspace_bytes, (float*)Z_hat, out, st);
+}
+
+int hb_l2_normalize(const void* src, void* dst, int64_t rows, int32_t cols, int32_t dtype, void* stream) {
+  if (rows < 0 || cols < 1) { set_error("bad shape"); return HB_ERR_INVALID; }
+  cudaStream_t st = (cudaStream_t)stream;
+  if (dtype == HB_FP64) return launch_l2_normalize<double, double>((const double*)src, rows, cols, cols, (double*)dst, cols, st);
+  if (dtype == HB_FP32) return launch_l2_normalize<float, float>((const float*)src, rows, cols, cols, (float*)dst, cols, st);
+  set_error("hb_l2_normalize: dtype must be HB_FP32 or HB_FP64");
+  return HB_ERR_INVALID;
+}
+
+size_t hb_block_lists_workspace_bytes(int64_t n, int64_t block_size) {
+  if (n < 1 || block_size < 1) return 0;
+  MembershipLayout L = membership_layout(n, block_size);
+  Carver cv(nullptr, 0);
+  MembershipBufs B;
+  membership_carve(cv, L, B);
+  return cv.off + 256;
+}
+
+int hb_block_lists(int64_t n, int64_t block_size, const uint32_t* seeds, int32_t n_iters, int32_t* idx,
+                   void* workspace, size_t workspace_bytes, void* stream) {
+  if (n < 1 || block_size < 1 || !seeds || !idx) { set_error("hb_block_lists: bad argument"); return HB_ERR_INVALID; }
+  MembershipLayout L = membership_layout(n, block_size);
+  if (L.nblk > kMaxBlocks) { set_error("too many blocks"); return HB_ERR_UNSUPPORTED; }
+  if (L.cap > 16384) { set_error("n too large"); return HB_ERR_UNSUPPORTED; }
+  if (workspace_bytes < hb_block_lists_workspace_bytes(n, block_size)) { set_error("workspace too small"); return HB_ERR_WORKSPACE; }
+  Carver cv((void*)align_up((size_t)workspace, 256), workspace_bytes - 256);
+  MembershipBufs B;
+  membership_carve(cv, L, B);
+  cudaStream_t st = (cudaStream_t)stream;
+  for (int c0 = 0; c0 < n_iters; c0 += kMaxIterChunk) {
+    const int C = std::min(kMaxIterChunk, n_iters - c0);
+    HB_TRY(membership_build(L, B, seeds + c0, C, idx + (size_t)c0 * n, st));
+  }
+  int err = 0;
+  HB_CUDA(cudaMemcpyAsync(&err, B.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  HB_CUDA(cudaStreamSynchronize(st));
+  if (err) { set_error("candidate overflow"); return HB_ERR_INTERNAL; }
+  return HB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,117 @@
+// Internal interfaces between the engine's translation units.
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+#include "hb_common.cuh"
+
+namespace hb {
+
+// ---- block membership -------------------------------------------------------
+struct MembershipLayout {
+  int64_t n, bs;
+  int nblk, ntiles, cap, max_slots;
+};
+struct MembershipBufs {
+  uint32_t* seeds;
+  uint32_t* hist;
+  int* bnd_slot;
+  uint32_t* bnd_q;
+  int* slot_bin;
+  int* nslots;
+  int16_t* lut;
+  uint32_t* cand_cnt;
+  uint32_t* cand;
+  uint32_t* split;
+  uint32_t* counts;
+  uint32_t* offsets;
+  int* err;
+};
+MembershipLayout membership_layout(int64_t n, int64_t bs);
+void membership_carve(Carver& cv, const MembershipLayout& L, MembershipBufs& B);
+int membership_build(const MembershipLayout& L, const MembershipBufs& B, const uint32_t* h_seeds,
+                     int n_iters, int32_t* idx, cudaStream_t st);
+int membership_build_dev(const MembershipLayout& L, const MembershipBufs& B, int n_iters,
+                         int32_t* idx, cudaStream_t st);
+__global__ void k_iota(int32_t* out, int64_t n);
+
+// ---- SIMT kernels of the plain (fp32 / fp64) path ----------------------------
+// Row L2 normalisation, inverse norm clamped to 1e12 (reference semantics).
+template <typename TI, typename TO>
+int launch_l2_normalize(const TI* src, int64_t rows, int cols, int ld_src, TO* dst, int ld_dst,
+                        cudaStream_t st);
+
+struct AccumChunk {  // a run of cells that all belong to batch `batch`
+  int64_t start;     // position in the cell list (identity or batch-sorted index)
+  int32_t len;
+  int32_t batch;
+};
+
+// P[chunk][k][c] = sum over the chunk's cells i of W[i][k] * V[i][c]
+template <typename TS, typename TV, typename TA>
+int launch_accum(const TS* W, int ldw, const TV* V, int ldv, const int32_t* cell_index,
+                 const AccumChunk* chunks, int n_chunks, int K, int d, TA* P, cudaStream_t st);
+
+// Y_norm[k] = l2norm(sum_chunks P[chunk][k]); optional 16-bit copy.
+template <typename TA, typename TY>
+int launch_centroid_reduce(const TA* P, int n_chunks, int K, int d, TY* Yn, int ldy,
+                           cudaStream_t st);
+
+struct BlockArgs {
+  const void* Zn;
+  int ldz;
+  void* R;
+  int ldr;
+  const int32_t* cats;
+  const void* Yn;
+  int ldy;
+  double* O;            // [B][K] observed counts (float64)
+  const double* Pr;     // [B] batch proportions
+  const double* theta;  // [B]
+  const int32_t* idx_new;  // nullptr -> identity (start at new_start)
+  int64_t new_start;
+  int64_t n_new;
+  const int32_t* idx_old;
+  int64_t n_old;
+  double* obj_acc;      // kmeans error + entropy of the new rows
+  double sigma;
+  int d, K, B;
+  int stabilized;
+  int init_mode;        // no penalty, L1 clamp 1e-12 (initial R)
+};
+int launch_block_update_f32(const BlockArgs& a, const double* O_in, double* O_out, double* O_zero,
+                            cudaStream_t st);
+int launch_block_update_f64(const BlockArgs& a, const double* O_in, double* O_out, double* O_zero,
+                            cudaStream_t st);
+
+int launch_objective_finalize(const double* O, const double* Pr, const double* theta, double sigma,
+                              int B, int K, int stabilized, double* obj_acc, double* obj_out,
+                              cudaStream_t st);
+
+struct CorrArgs {
+  const double* M;      // [K][B+1][d]
+  const double* O;      // [B][K]
+  const double* Pr;     // [B]
+  const double* Nb;     // [B]
+  double alpha, ridge_lambda, threshold;
+  int prune, dynamic_lambda;
+  int K, B, d;
+};
+template <typename TW>
+int launch_ridge_solve(const CorrArgs& a, TW* W, cudaStream_t st);
+
+template <typename TA>
+int launch_m_reduce(const TA* P, const AccumChunk* h_chunks, int n_chunks,
+                    const int32_t* d_batch_chunk_off, int K, int B, int d, double* M, cudaStream_t st);
+
+struct ApplyTile {
+  int64_t start;   // position in the batch-sorted cell list
+  int32_t len;
+  int32_t batch;
+};
+template <typename T, typename TS, typename TZ>
+int launch_apply_t(const T* X, int ldx, const TS* R, int ldr, const T* W, const int32_t* cell_index,
+                   const ApplyTile* tiles, int n_tiles, int K, int d, T* Zhat, int ldzh, TZ* Zn,
+                   int ldz, cudaStream_t st);
+
+}  // namespace hb

@@ -1,0 +1,674 @@
+// SIMT kernels of the plain (fp32 / fp64) Harmony path, plus the pieces shared
+// with the 16-bit path (normalisation, ridge solve, correction apply).
+#include <type_traits>
+#include "hb_internal.h"
+
+namespace hb {
+
+template <typename T>
+using compute_t = typename std::conditional<std::is_same<T, double>::value, double, float>::type;
+
+// ---------------------------------------------------------------------------
+// Row L2 normalise (kernels_normalize.cuh:7-54 semantics), one warp per row.
+// Columns [cols, ld_dst) of the destination are zero-filled (padding).
+template <typename TI, typename TO>
+__global__ void k_l2_normalize(const TI* __restrict__ src, int64_t rows, int cols, int lds,
+                               TO* __restrict__ dst, int ldd) {
+  using TC = compute_t<TI>;
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t r = warp; r < rows; r += nwarps) {
+    const TI* s = src + r * lds;
+    TC ss = 0;
+    for (int c = lane; c < cols; c += 32) {
+      TC v = (TC)to_f(s[c]);
+      ss += v * v;
+    }
+    ss = warp_sum(ss);
+    TC inv = num<TC>::rsqrt_(ss);
+    if (inv > TC(1e12)) inv = TC(1e12);
+    TO* o = dst + r * ldd;
+    for (int c = lane; c < ldd; c += 32)
+      o[c] = (c < cols) ? from_f<TO>((TC)to_f(s[c]) * inv) : from_f<TO>(TC(0));
+  }
+}
+
+template <typename TI, typename TO>
+int launch_l2_normalize(const TI* src, int64_t rows, int cols, int ld_src, TO* dst, int ld_dst,
+                        cudaStream_t st) {
+  if (rows == 0) return HB_OK;
+  int blocks = (int)std::min<int64_t>((rows + 7) / 8, (int64_t)num_sms() * 16);
+  k_l2_normalize<TI, TO><<<blocks, 256, 0, st>>>(src, rows, cols, ld_src, dst, ld_dst);
+  HB_LAUNCH_CHECK();
+  return HB_OK;
+}
+template int launch_l2_normalize<float, float>(const float*, int64_t, int, int, float*, int, cudaStream_t);
+template int launch_l2_normalize<double, double>(const double*, int64_t, int, int, double*, int, cudaStream_t);
+template int launch_l2_normalize<float, __half>(const float*, int64_t, int, int, __half*, int, cudaStream_t);
+template int launch_l2_normalize<float, __nv_bfloat16>(const float*, int64_t, int, int, __nv_bfloat16*, int, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Split-n weighted outer-product accumulation:
+//   P[chunk][k][c] = sum_{i in chunk} W[i][k] * V[i][c]
+// A CTA owns a 128 (k) x 64 (c) output tile of one chunk; 256 threads, 8 x 4
+// accumulators each.  Used for the centroid sum R^T Z_norm (identity cell
+// list, clustering.cu:272-276) and for the per-batch ridge moments R_b^T X_b
+// (batch-sorted cell list, correction_batched.cu:55-100).
+constexpr int ACC_BK = 128, ACC_BD = 64;
+
+template <typename TS, typename TV, typename TA>
+__global__ void __launch_bounds__(256) k_accum(const TS* __restrict__ W, int ldw,
+                                               const TV* __restrict__ V, int ldv,
+                                               const int32_t* __restrict__ cell_index,
+                                               const AccumChunk* __restrict__ chunks, int K,
+                                               int d, int ktiles, TA* __restrict__ P) {
+  constexpr int ACC_ROWS = sizeof(TA) == 8 ? 16 : 32;
+  __shared__ TA ws[ACC_ROWS][ACC_BK];
+  __shared__ TA vs[ACC_ROWS][ACC_BD];
+  __shared__ int64_t cid[ACC_ROWS];
+  const AccumChunk ch = chunks[blockIdx.x];
+  const int kt = blockIdx.y % ktiles, dt = blockIdx.y / ktiles;
+  const int k0 = kt * ACC_BK, d0 = dt * ACC_BD;
+  const int tid = threadIdx.x, tk = tid & 15, td = tid >> 4;
+  TA acc[8][4];
+#pragma unroll
+  for (int a = 0; a < 8; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = TA(0);
+
+  for (int pos = 0; pos < ch.len; pos += ACC_ROWS) {
+    const int nrow = min(ACC_ROWS, ch.len - pos);
+    __syncthreads();
+    if (tid < ACC_ROWS) {
+      int64_t q = ch.start + pos + tid;
+      cid[tid] = (tid < nrow) ? (cell_index ? (int64_t)cell_index[q] : q) : -1;
+    }
+    __syncthreads();
+    for (int e = tid; e < ACC_ROWS * ACC_BK; e += 256) {
+      const int r = e / ACC_BK, kk = e % ACC_BK;
+      const int64_t cell = cid[r];
+      ws[r][kk] = (cell >= 0 && k0 + kk < K) ? (TA)to_f(W[cell * ldw + k0 + kk]) : TA(0);
+    }
+    for (int e = tid; e < ACC_ROWS * ACC_BD; e += 256) {
+      const int r = e / ACC_BD, cc = e % ACC_BD;
+      const int64_t cell = cid[r];
+      vs[r][cc] = (cell >= 0 && d0 + cc < d) ? (TA)to_f(V[cell * ldv + d0 + cc]) : TA(0);
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int r = 0; r < ACC_ROWS; ++r) {
+      TA wv[8], vv[4];
+#pragma unroll
+      for (int a = 0; a < 8; ++a) wv[a] = ws[r][tk * 8 + a];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) vv[b] = vs[r][td * 4 + b];
+#pragma unroll
+      for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] += wv[a] * vv[b];
+    }
+  }
+  TA* out = P + (size_t)blockIdx.x * K * d;
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    const int k = k0 + tk * 8 + a;
+    if (k >= K) continue;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int c = d0 + td * 4 + b;
+      if (c < d) out[(size_t)k * d + c] = acc[a][b];
+    }
+  }
+}
+
+template <typename TS, typename TV, typename TA>
+int launch_accum(const TS* W, int ldw, const TV* V, int ldv, const int32_t* cell_index,
+                 const AccumChunk* chunks, int n_chunks, int K, int d, TA* P, cudaStream_t st) {
+  if (n_chunks == 0) return HB_OK;
+  const int ktiles = div_up(K, ACC_BK), dtiles = div_up(d, ACC_BD);
+  k_accum<TS, TV, TA><<<dim3(n_chunks, ktiles * dtiles), 256, 0, st>>>(W, ldw, V, ldv, cell_index,
+                                                                       chunks, K, d, ktiles, P);
+  HB_LAUNCH_CHECK();
+  return HB_OK;
+}
+template int launch_accum<float, float, float>(const float*, int, const float*, int, const int32_t*,
+                                               const AccumChunk*, int, int, int, float*, cudaStream_t);
+template int launch_accum<double, double, double>(const double*, int, const double*, int, const int32_t*,
+                                                  const AccumChunk*, int, int, int, double*, cudaStream_t);
+template int launch_accum<__half, float, float>(const __half*, int, const float*, int, const int32_t*,
+                                                const AccumChunk*, int, int, int, float*, cudaStream_t);
+template int launch_accum<__nv_bfloat16, float, float>(const __nv_bfloat16*, int, const float*, int,
+                                                       const int32_t*, const AccumChunk*, int, int, int,
+                                                       float*, cudaStream_t);
+template int launch_accum<__half, __half, float>(const __half*, int, const __half*, int, const int32_t*,
+                                                 const AccumChunk*, int, int, int, float*, cudaStream_t);
+template int launch_accum<__nv_bfloat16, __nv_bfloat16, float>(const __nv_bfloat16*, int,
+                                                               const __nv_bfloat16*, int, const int32_t*,
+                                                               const AccumChunk*, int, int, int, float*,
+                                                               cudaStream_t);
+
+// Y_norm[k] = l2normalise(sum over chunks of P[chunk][k]) -- fixed summation
+// order (deterministic), float64 accumulation.
+template <typename TA, typename TY>
+__global__ void k_centroid_reduce(const TA* __restrict__ P, int n_chunks, int K, int d,
+                                  TY* __restrict__ Yn, int ldy) {
+  extern __shared__ double ys[];
+  __shared__ double red[32];
+  const int k = blockIdx.x;
+  double ss = 0;
+  for (int c = threadIdx.x; c < d; c += blockDim.x) {
+    double s = 0;
+    for (int q = 0; q < n_chunks; ++q) s += (double)P[((size_t)q * K + k) * d + c];
+    ys[c] = s;
+    ss += s * s;
+  }
+  ss = block_sum(ss, red);
+  double inv = rsqrt(ss);
+  if (inv > 1e12) inv = 1e12;
+  for (int c = threadIdx.x; c < ldy; c += blockDim.x)
+    Yn[(size_t)k * ldy + c] = (c < d) ? from_f<TY>((compute_t<TY>)(ys[c] * inv)) : from_f<TY>(compute_t<TY>(0));
+}
+
+template <typename TA, typename TY>
+int launch_centroid_reduce(const TA* P, int n_chunks, int K, int d, TY* Yn, int ldy, cudaStream_t st) {
+  k_centroid_reduce<TA, TY><<<K, 128, sizeof(double) * d, st>>>(P, n_chunks, K, d, Yn, ldy);
+  HB_LAUNCH_CHECK();
+  return HB_OK;
+}
+template int launch_centroid_reduce<float, float>(const float*, int, int, int, float*, int, cudaStream_t);
+template int launch_centroid_reduce<double, double>(const double*, int, int, int, double*, int, cudaStream_t);
+template int launch_centroid_reduce<float, __half>(const float*, int, int, int, __half*, int, cudaStream_t);
+template int launch_centroid_reduce<float, __nv_bfloat16>(const float*, int, int, int, __nv_bfloat16*, int, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Fused block update (plain path).
+//
+// For the cells of block j (list idx_new) the CTA computes the similarity row
+// s = Z_norm[i] . Y_norm^T, the new assignment row
+//   R[i] = normalise_L1( exp(-2/sigma (1-s)) * pen[cat_i] )
+// (kernels_pen.cuh:27-82), writes it, and accumulates its contribution to the
+// observed counts O[cat_i] plus the kmeans-error and entropy terms of the
+// objective (kernels_kmeans.cuh:30-96, kernels_clustering.cuh:8-62).  For the
+// cells of block j+1 (list idx_old) it subtracts their current R rows from O,
+// which is the "remove old contribution" step the reference runs at the start
+// of the next block (clustering.cu:312-332).  E is never stored: E[b][k] =
+// Pr_b * sum_b' O[b'][k], the quantity the reference maintains incrementally
+// (clustering.cu:328-331,367-370).
+//
+// O is triple-buffered: the kernel reads the state O_in, accumulates
+// O_in + delta into O_out (zeroed beforehand), and zeroes O_zero (the buffer
+// the previous launch read), so no CTA ever reads a buffer another CTA of the
+// same launch is writing.
+constexpr int BU_TM = 64, BU_DC = 16, BU_THREADS = 256;
+
+struct BlockArgsDev {
+  BlockArgs a;
+  const double* O_in;
+  double* O_out;
+  double* O_zero;
+};
+
+template <typename T, int KPT>
+__global__ void __launch_bounds__(BU_THREADS) k_block_update(BlockArgsDev p) {
+  const BlockArgs& a = p.a;
+  const int K = a.K, B = a.B, d = a.d;
+  const int K16 = 16 * KPT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* pen = (T*)smem_raw;                       // [B][K]
+  T* osm = pen + (size_t)B * K;                // [B][K]
+  T* zt = osm + (size_t)B * K;                 // [TM][DC+1]
+  T* yt = zt + BU_TM * (BU_DC + 1);            // [K16][DC+1]
+  int64_t* cid = (int64_t*)(yt + (size_t)K16 * (BU_DC + 1));  // [TM]
+  int* ccat = (int*)(cid + BU_TM);             // [TM]
+  __shared__ double red[32];
+
+  const int tid = threadIdx.x, cg = tid >> 4, kg = tid & 15;
+  const T* Zn = (const T*)a.Zn;
+  const T* Yn = (const T*)a.Yn;
+  T* R = (T*)a.R;
+
+  // zero the buffer the previous launch read
+  if (p.O_zero)
+    for (int e = blockIdx.x * BU_THREADS + tid; e < B * K; e += gridDim.x * BU_THREADS) p.O_zero[e] = 0.0;
+
+  // penalty table from the current state (kernels_pen.cuh:8-21)
+  if (a.n_new > 0 && !a.init_mode) {
+    double* ocol = (double*)zt;  // scratch (K doubles fit in zt+yt)
+    for (int k = tid; k < K; k += BU_THREADS) {
+      double s = 0;
+      for (int b = 0; b < B; ++b) s += p.O_in[(size_t)b * K + k];
+      ocol[k] = s;
+    }
+    __syncthreads();
+    for (int e = tid; e < B * K; e += BU_THREADS) {
+      const int b = e / K, k = e % K;
+      const T o = (T)p.O_in[e];
+      const T E = (T)(a.Pr[b] * ocol[k]);
+      const T denom = a.stabilized ? (o + E + T(1)) : (o + T(1));
+      pen[e] = num<T>::pow_((E + T(1)) / denom, (T)a.theta[b]);
+    }
+  }
+  for (int e = tid; e < B * K; e += BU_THREADS) osm[e] = T(0);
+  __syncthreads();
+
+  const T term = T(-2) / (T)a.sigma;
+  const T sig = (T)a.sigma;
+  double obj_local = 0.0;
+  const int64_t ntiles_new = (a.n_new + BU_TM - 1) / BU_TM;
+  for (int64_t tile = blockIdx.x; tile < ntiles_new; tile += gridDim.x) {
+    const int64_t r0 = tile * BU_TM;
+    if (tid < BU_TM) {
+      const int64_t q = r0 + tid;
+      int64_t cell = -1;
+      if (q < a.n_new) cell = a.idx_new ? (int64_t)a.idx_new[q] : a.new_start + q;
+      cid[tid] = cell;
+      ccat[tid] = cell >= 0 ? a.cats[cell] : 0;
+    }
+    T s[4][KPT];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < KPT; ++j) s[i][j] = T(0);
+    for (int d0 = 0; d0 < d; d0 += BU_DC) {
+      __syncthreads();
+      for (int e = tid; e < BU_TM * BU_DC; e += BU_THREADS) {
+        const int r = e / BU_DC, c = e % BU_DC;
+        const int64_t cell = cid[r];
+        zt[r * (BU_DC + 1) + c] = (cell >= 0 && d0 + c < d) ? Zn[cell * a.ldz + d0 + c] : T(0);
+      }
+      for (int e = tid; e < K16 * BU_DC; e += BU_THREADS) {
+        const int k = e / BU_DC, c = e % BU_DC;
+        yt[k * (BU_DC + 1) + c] = (k < K && d0 + c < d) ? Yn[(size_t)k * a.ldy + d0 + c] : T(0);
+      }
+      __syncthreads();
+#pragma unroll 4
+      for (int c = 0; c < BU_DC; ++c) {
+        T z[4], y[KPT];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) z[i] = zt[(cg * 4 + i) * (BU_DC + 1) + c];
+#pragma unroll
+        for (int j = 0; j < KPT; ++j) y[j] = yt[(kg + 16 * j) * (BU_DC + 1) + c];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < KPT; ++j) s[i][j] += z[i] * y[j];
+      }
+    }
+    // epilogue: exp * penalty, L1 normalise, write, O delta, objective terms
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int row = cg * 4 + i;
+      const int64_t cell = cid[row];
+      const int cat = ccat[row];
+      T v[KPT];
+      T rs = T(0), km = T(0);
+#pragma unroll
+      for (int j = 0; j < KPT; ++j) {
+        const int k = kg + 16 * j;
+        T val = T(0);
+        if (k < K) {
+          val = num<T>::exp_(term * (T(1) - s[i][j]));
+          if (!a.init_mode) val *= pen[cat * K + k];
+          km += val * T(2) * (T(1) - s[i][j]);
+        }
+        v[j] = val;
+        rs += val;
+      }
+#pragma unroll
+      for (int o = 8; o > 0; o >>= 1) {
+        rs += __shfl_xor_sync(0xffffffffu, rs, o);
+        km += __shfl_xor_sync(0xffffffffu, km, o);
+      }
+      T inv;
+      if (a.init_mode) {
+        T nrm = rs < T(1e-12) ? T(1e-12) : rs;
+        inv = T(1) / nrm;
+      } else {
+        inv = T(1) / rs;
+      }
+      T rs2 = T(0);
+#pragma unroll
+      for (int j = 0; j < KPT; ++j) {
+        v[j] *= inv;
+        rs2 += v[j];
+      }
+#pragma unroll
+      for (int o = 8; o > 0; o >>= 1) rs2 += __shfl_xor_sync(0xffffffffu, rs2, o);
+      const T inv2 = T(1) / rs2;
+      T ent = T(0);
+#pragma unroll
+      for (int j = 0; j < KPT; ++j) {
+        const int k = kg + 16 * j;
+        if (k < K) {
+          const T x = v[j] * inv2;
+          ent += x * num<T>::log_(x + T(1e-12));
+        }
+      }
+#pragma unroll
+      for (int o = 8; o > 0; o >>= 1) ent += __shfl_xor_sync(0xffffffffu, ent, o);
+      if (cell >= 0) {
+        T* Rrow = R + cell * a.ldr;
+#pragma unroll
+        for (int j = 0; j < KPT; ++j) {
+          const int k = kg + 16 * j;
+          if (k < K) {
+            Rrow[k] = v[j];
+            atomicAdd(&osm[cat * K + k], v[j]);
+          } else if (k < a.ldr) {
+            Rrow[k] = T(0);
+          }
+        }
+        if (kg == 0) obj_local += (double)(km * inv) + (double)(sig * ent);
+      }
+    }
+  }
+
+  // remove the current rows of the next block's cells
+  {
+    const int lane = tid & 31, w = tid >> 5;
+    for (int64_t q = (int64_t)blockIdx.x * (BU_THREADS / 32) + w; q < a.n_old;
+         q += (int64_t)gridDim.x * (BU_THREADS / 32)) {
+      const int64_t cell = a.idx_old[q];
+      const int cat = a.cats[cell];
+      const T* Rrow = R + cell * a.ldr;
+      for (int k = lane; k < K; k += 32) atomicAdd(&osm[cat * K + k], -Rrow[k]);
+    }
+  }
+  __syncthreads();
+  for (int e = tid; e < B * K; e += BU_THREADS) {
+    double v = (double)osm[e];
+    if (blockIdx.x == 0) v += p.O_in ? p.O_in[e] : 0.0;
+    if (v != 0.0) atomicAdd(&p.O_out[e], v);
+  }
+  const double tot = block_sum(obj_local, red);
+  if (tid == 0 && tot != 0.0) atomicAdd(a.obj_acc, tot);
+}
+
+template <typename T, int KPT>
+static int launch_block_kpt(const BlockArgsDev& p, cudaStream_t st) {
+  const BlockArgs& a = p.a;
+  const size_t smem = sizeof(T) * ((size_t)2 * a.B * a.K + BU_TM * (BU_DC + 1) +
+                                    (size_t)16 * KPT * (BU_DC + 1)) +
+                      BU_TM * (sizeof(int64_t) + sizeof(int)) + 64;
+  if (smem > 227 * 1024) {
+    set_error("block update: B*K too large for shared memory (B=%d K=%d)", a.B, a.K);
+    return HB_ERR_UNSUPPORTED;
+  }
+  HB_CUDA(cudaFuncSetAttribute(k_block_update<T, KPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem));
+  int occ = 1;
+  HB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_block_update<T, KPT>, BU_THREADS, smem));
+  if (occ < 1) occ = 1;
+  const int64_t tiles = std::max<int64_t>((a.n_new + BU_TM - 1) / BU_TM,
+                                          (a.n_old + 7) / 8 / 4);
+  int grid = (int)std::min<int64_t>(std::max<int64_t>(tiles, 1), (int64_t)num_sms() * occ);
+  k_block_update<T, KPT><<<grid, BU_THREADS, smem, st>>>(p);
+  HB_LAUNCH_CHECK();
+  return HB_OK;
+}
+
+template <typename T>
+int launch_block_update_dev(const BlockArgsDev& p, cudaStream_t st) {
+  const int K = p.a.K;
+  if (K <= 64) return launch_block_kpt<T, 4>(p, st);
+  if (K <= 128) return launch_block_kpt<T, 8>(p, st);
+  if (K <= 208) return launch_block_kpt<T, 13>(p, st);
+  if (K <= 256) return launch_block_kpt<T, 16>(p, st);
+  set_error("n_clusters=%d exceeds the supported maximum of 256", K);
+  return HB_ERR_UNSUPPORTED;
+}
+
+int launch_block_update_f32(const BlockArgs& a, const double* O_in, double* O_out, double* O_zero,
+                            cudaStream_t st) {
+  return launch_block_update_dev<float>(BlockArgsDev{a, O_in, O_out, O_zero}, st);
+}
+int launch_block_update_f64(const BlockArgs& a, const double* O_in, double* O_out, double* O_zero,
+                            cudaStream_t st) {
+  return launch_block_update_dev<double>(BlockArgsDev{a, O_in, O_out, O_zero}, st);
+}
+
+// ---------------------------------------------------------------------------
+// Objective tail: diversity term from O (kernels_clustering.cuh:68-103) added to
+// the accumulated kmeans-error + entropy terms, all in float64.
+__global__ void k_objective_finalize(const double* __restrict__ O, const double* __restrict__ Pr,
+                                     const double* __restrict__ theta, double sigma, int B, int K,
+                                     int stabilized, double* __restrict__ obj_acc,
+                                     double* __restrict__ obj_out) {
+  __shared__ double red[32];
+  double acc = 0;
+  for (int k = threadIdx.x; k < K; k += blockDim.x) {
+    double col = 0;
+    for (int b = 0; b < B; ++b) col += O[(size_t)b * K + k];
+    for (int b = 0; b < B; ++b) {
+      const double o = O[(size_t)b * K + k];
+      const double E = Pr[b] * col;
+      const double num_ = stabilized ? (o + E + 1.0) : (o + 1.0);
+      acc += theta[b] * o * log(num_ / (E + 1.0));
+    }
+  }
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) {
+    *obj_out = *obj_acc + sigma * acc;
+    *obj_acc = 0.0;
+  }
+}
+
+int launch_objective_finalize(const double* O, const double* Pr, const double* theta, double sigma,
+                              int B, int K, int stabilized, double* obj_acc, double* obj_out,
+                              cudaStream_t st) {
+  k_objective_finalize<<<1, 256, 0, st>>>(O, Pr, theta, sigma, B, K, stabilized, obj_acc, obj_out);
+  HB_LAUNCH_CHECK();
+  return HB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Ridge moments: M[k][b+1][c] = sum over batch-b chunks of P, M[k][0] = sum_b.
+__global__ void k_m_reduce(const float* __restrict__ Pf, const double* __restrict__ Pd,
+                           const int32_t* __restrict__ batch_chunk_off, int K, int B, int d,
+                           double* __restrict__ M) {
+  const int k = blockIdx.x;
+  for (int c = threadIdx.x; c < d; c += blockDim.x) {
+    double row0 = 0;
+    for (int b = 0; b < B; ++b) {
+      double s = 0;
+      for (int q = batch_chunk_off[b]; q < batch_chunk_off[b + 1]; ++q) {
+        const size_t at = ((size_t)q * K + k) * d + c;
+        s += Pf ? (double)Pf[at] : Pd[at];
+      }
+      M[((size_t)k * (B + 1) + b + 1) * d + c] = s;
+      row0 += s;
+    }
+    M[((size_t)k * (B + 1)) * d + c] = row0;
+  }
+}
+
+template <typename TA>
+int launch_m_reduce(const TA* P, const AccumChunk*, int, const int32_t* d_batch_chunk_off, int K,
+                    int B, int d, double* M, cudaStream_t st) {
+  const float* Pf = std::is_same<TA, float>::value ? (const float*)P : nullptr;
+  const double* Pd = std::is_same<TA, double>::value ? (const double*)P : nullptr;
+  k_m_reduce<<<K, 128, 0, st>>>(Pf, Pd, d_batch_chunk_off, K, B, d, M);
+  HB_LAUNCH_CHECK();
+  return HB_OK;
+}
+template int launch_m_reduce<float>(const float*, const AccumChunk*, int, const int32_t*, int, int, int, double*, cudaStream_t);
+template int launch_m_reduce<double>(const double*, const AccumChunk*, int, const int32_t*, int, int, int, double*, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Ridge lambda (_harmony/__init__.py:454-480), closed-form arrowhead inverse
+// (kernels_correction_fast.cuh:24-123) and W = inv * M with W[0] = 0
+// (correction_batched.cu:102-120), one CTA per cluster, float64.  Because the
+// inverse is an arrowhead, row b+1 of inv*M is p_b u + f_b M[b+1] with
+// u = (M[0] + sum_j p_j M[j+1]) / c, so W costs O(B d) per cluster.
+// W is written as [B][K][d] so that each batch's K x d slice is contiguous.
+template <typename TW>
+__global__ void k_ridge_solve(CorrArgs a, TW* __restrict__ W) {
+  extern __shared__ double sh[];
+  double* f = sh;          // [B]
+  double* p = sh + a.B;    // [B]
+  __shared__ double red[32];
+  const int k = blockIdx.x, B = a.B, K = a.K, d = a.d;
+  double col = 0;
+  for (int b = 0; b < B; ++b) col += a.O[(size_t)b * K + k];  // N_k
+  double cneg = 0;
+  for (int b = threadIdx.x; b < B; b += blockDim.x) {
+    const double o = a.O[(size_t)b * K + k];
+    double lam;
+    if (!a.dynamic_lambda) {
+      lam = a.ridge_lambda;
+    } else {
+      lam = a.alpha * (a.Pr[b] * col);
+      if (a.prune) {
+        const double nb = a.Nb[b];
+        const double safe = nb > 0 ? nb : 1.0;
+        if (o / safe < a.threshold || nb == 0) lam = 1e30;
+      }
+    }
+    if (o + lam == 0.0) lam = 1e30;
+    const double fb = 1.0 / (o + lam);
+    f[b] = fb;
+    p[b] = -fb * o;
+    cneg += fb * o * o;
+  }
+  cneg = block_sum(cneg, red);
+  const double cinv = 1.0 / (col - cneg);
+  const double* Mk = a.M + (size_t)k * (B + 1) * d;
+  for (int c = threadIdx.x; c < d; c += blockDim.x) {
+    double u = Mk[c];
+    for (int b = 0; b < B; ++b) u += p[b] * Mk[(size_t)(b + 1) * d + c];
+    u *= cinv;
+    for (int b = 0; b < B; ++b)
+      W[((size_t)b * K + k) * d + c] = (TW)(p[b] * u + f[b] * Mk[(size_t)(b + 1) * d + c]);
+  }
+}
+
+template <typename TW>
+int launch_ridge_solve(const CorrArgs& a, TW* W, cudaStream_t st) {
+  k_ridge_solve<TW><<<a.K, 128, sizeof(double) * 2 * a.B, st>>>(a, W);
+  HB_LAUNCH_CHECK();
+  return HB_OK;
+}
+template int launch_ridge_solve<float>(const CorrArgs&, float*, cudaStream_t);
+template int launch_ridge_solve<double>(const CorrArgs&, double*, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Correction apply (kernels_outer.cuh:41-65) fused with the L2 renormalisation
+// of the corrected embedding (_harmony/__init__.py:276):
+//   Z_hat[i] = X[i] - R[i] . W[cat_i],   Z_norm[i] = l2normalise(Z_hat[i])
+// A CTA takes a tile of <= 32 cells of one batch (batch-sorted cell list), so
+// the batch's W slice is shared; 8 warps x 4 cells, lanes over PCs.
+constexpr int AP_TM = 32, AP_KC = 32;
+
+template <typename T, typename TS, typename TZ, int DQ>
+__global__ void __launch_bounds__(256) k_apply(const T* __restrict__ X, int ldx,
+                                               const TS* __restrict__ R, int ldr,
+                                               const T* __restrict__ W,
+                                               const int32_t* __restrict__ cell_index,
+                                               const ApplyTile* __restrict__ tiles, int K, int d,
+                                               T* __restrict__ Zhat, int ldzh, TZ* __restrict__ Zn,
+                                               int ldz) {
+  using TC = compute_t<T>;
+  __shared__ TC rt[AP_TM][AP_KC + 1];
+  __shared__ TC wt[AP_KC][32 * DQ];
+  __shared__ int64_t cid[AP_TM];
+  const ApplyTile tl = tiles[blockIdx.x];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  if (tid < AP_TM) cid[tid] = tid < tl.len ? (int64_t)cell_index[tl.start + tid] : -1;
+  TC acc[4][DQ];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int q = 0; q < DQ; ++q) acc[i][q] = TC(0);
+  const T* Wb = W + (size_t)tl.batch * K * d;
+  for (int k0 = 0; k0 < K; k0 += AP_KC) {
+    __syncthreads();
+    for (int e = tid; e < AP_TM * AP_KC; e += 256) {
+      const int r = e / AP_KC, kk = e % AP_KC;
+      const int64_t cell = cid[r];
+      rt[r][kk] = (cell >= 0 && k0 + kk < K) ? (TC)to_f(R[cell * ldr + k0 + kk]) : TC(0);
+    }
+    for (int e = tid; e < AP_KC * 32 * DQ; e += 256) {
+      const int kk = e / (32 * DQ), c = e % (32 * DQ);
+      wt[kk][c] = (k0 + kk < K && c < d) ? (TC)Wb[(size_t)(k0 + kk) * d + c] : TC(0);
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < AP_KC; ++kk) {
+      TC r[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) r[i] = rt[w * 4 + i][kk];
+#pragma unroll
+      for (int q = 0; q < DQ; ++q) {
+        const TC wv = wt[kk][lane + 32 * q];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) acc[i][q] += r[i] * wv;
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int64_t cell = cid[w * 4 + i];
+    TC zh[DQ];
+    TC ss = 0;
+#pragma unroll
+    for (int q = 0; q < DQ; ++q) {
+      const int c = lane + 32 * q;
+      zh[q] = (cell >= 0 && c < d) ? (TC)X[cell * ldx + c] - acc[i][q] : TC(0);
+      ss += zh[q] * zh[q];
+    }
+    ss = warp_sum(ss);
+    TC inv = num<TC>::rsqrt_(ss);
+    if (inv > TC(1e12)) inv = TC(1e12);
+    if (cell >= 0) {
+#pragma unroll
+      for (int q = 0; q < DQ; ++q) {
+        const int c = lane + 32 * q;
+        if (c < d) Zhat[cell * ldzh + c] = (T)zh[q];
+        if (c < ldz) Zn[cell * ldz + c] = from_f<TZ>(c < d ? zh[q] * inv : TC(0));
+      }
+    }
+  }
+}
+
+template <typename T, typename TS, typename TZ>
+int launch_apply_t(const T* X, int ldx, const TS* R, int ldr, const T* W, const int32_t* cell_index,
+                   const ApplyTile* tiles, int n_tiles, int K, int d, T* Zhat, int ldzh, TZ* Zn,
+                   int ldz, cudaStream_t st) {
+  if (n_tiles == 0) return HB_OK;
+  const int dq = div_up(std::max(d, ldz), 32);
+#define HB_AP(DQv)                                                                                 \
+  k_apply<T, TS, TZ, DQv><<<n_tiles, 256, 0, st>>>(X, ldx, R, ldr, W, cell_index, tiles, K, d, Zhat, \
+                                                   ldzh, Zn, ldz)
+  if (dq <= 1) HB_AP(1);
+  else if (dq <= 2) HB_AP(2);
+  else if (dq <= 4) HB_AP(4);
+  else if constexpr (sizeof(T) == 4) {
+    if (dq <= 8) HB_AP(8);
+    else {
+      set_error("n_pcs=%d exceeds the supported maximum of 256", d);
+      return HB_ERR_UNSUPPORTED;
+    }
+  } else {
+    set_error("n_pcs=%d exceeds the supported maximum (256 for fp32, 128 for fp64)", d);
+    return HB_ERR_UNSUPPORTED;
+  }
+#undef HB_AP
+  HB_LAUNCH_CHECK();
+  return HB_OK;
+}
+template int launch_apply_t<float, float, float>(const float*, int, const float*, int, const float*,
+                                                 const int32_t*, const ApplyTile*, int, int, int,
+                                                 float*, int, float*, int, cudaStream_t);
+template int launch_apply_t<double, double, double>(const double*, int, const double*, int,
+                                                    const double*, const int32_t*, const ApplyTile*,
+                                                    int, int, int, double*, int, double*, int,
+                                                    cudaStream_t);
+template int launch_apply_t<float, __half, __half>(const float*, int, const __half*, int, const float*,
+                                                   const int32_t*, const ApplyTile*, int, int, int,
+                                                   float*, int, __half*, int, cudaStream_t);
+template int launch_apply_t<float, __nv_bfloat16, __nv_bfloat16>(
+    const float*, int, const __nv_bfloat16*, int, const float*, const int32_t*, const ApplyTile*, int,
+    int, int, float*, int, __nv_bfloat16*, int, cudaStream_t);
+
+}  // namespace hb

@@ -1,0 +1,258 @@
+"""Harmony integration on B200: host-side driver over the C ABI.
+
+``harmonize`` mirrors ``rapids_singlecell.preprocessing._harmony.harmonize``
+(src/rapids_singlecell/preprocessing/_harmony/__init__.py:41-289): the same
+keyword arguments, defaults, parameter resolution and error types.  The work
+runs in one call into ``libharmony_b200.so`` (``hb_harmonize``) on the current
+CUDA stream; device memory for the run is one workspace tensor allocated here.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import warnings
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import HbOutputs, HbParams, PRECISIONS
+
+SUPPRESS_PENALTY = 1e30
+
+
+@dataclass
+class HarmonyInfo:
+    objectives_harmony: list
+    kmeans_objectives: list = field(default_factory=list)
+    converged: bool = False
+    n_outer: int = 0
+    n_clusters: int = 0
+    precision: str = "fp32"
+
+
+def get_batch_codes(batch_mat, batch_key):
+    """Categorical batch codes (``_get_batch_codes``, _helper.py:223-236): several
+    keys are joined with ","."""
+    import pandas as pd
+
+    if batch_key is None:
+        # labels given directly; a pandas Categorical keeps its (possibly unused) categories
+        vec = batch_mat if isinstance(batch_mat, pd.Series) else pd.Series(batch_mat)
+    elif isinstance(batch_key, str):
+        vec = batch_mat[batch_key]
+    elif len(batch_key) == 1:
+        vec = batch_mat[batch_key[0]]
+    else:
+        df = batch_mat[batch_key].astype("str")
+        vec = df.apply(lambda row: ",".join(row), axis=1)
+    return vec.astype("category")
+
+
+def theta_array(theta, n_batches: int) -> np.ndarray:
+    """theta per batch (``_get_theta_array``, _helper.py:277-307)."""
+    if isinstance(theta, (float, int)) and not isinstance(theta, bool):
+        return np.ones(n_batches, dtype=np.float64) * float(theta)
+    if isinstance(theta, (list, np.ndarray)):
+        arr = np.asarray(theta, dtype=np.float64)
+    elif isinstance(theta, torch.Tensor):
+        arr = theta.detach().cpu().numpy().astype(np.float64)
+    else:
+        raise ValueError(
+            f"Theta must be float, int, list, numpy array, or torch tensor, got {type(theta)}"
+        )
+    if arr.size != n_batches:
+        raise ValueError(
+            f"Theta array size ({arr.size}) must match number of batches ({n_batches})"
+        )
+    return arr.ravel()
+
+
+def default_n_clusters(n_cells: int) -> int:
+    return max(int(min(100, n_cells / 30)), 2)
+
+
+def seeded_centroids(Z: torch.Tensor, n_clusters: int, random_state: int) -> torch.Tensor:
+    """Initial centroids when none are given: ``n_clusters`` distinct cells chosen by
+    ``numpy.random.default_rng(random_state)``.  (The reference runs cuML k-means||,
+    a third-party library, here; pass ``init_centroids`` to reproduce a given start.)"""
+    rng = np.random.default_rng(random_state)
+    idx = rng.choice(Z.shape[0], size=n_clusters, replace=False)
+    return Z[torch.as_tensor(idx, device=Z.device)].contiguous()
+
+
+def _resolve_precision(precision, dtype) -> str:
+    if precision is None:
+        return "fp64" if dtype == torch.float64 else "fp32"
+    if precision not in PRECISIONS:
+        raise ValueError(f"precision must be one of {sorted(PRECISIONS)}, got {precision!r}")
+    return precision
+
+
+def resolve_parameters(n_cells, N_b, *, n_clusters, max_iter_harmony, theta, tau,
+                       block_proportion, dynamic_lambda, alpha, batch_prune_threshold,
+                       correction_method, colsum_algo):
+    """Host-side parameter resolution and validation, in the order of the reference
+    (_harmony/__init__.py:154-200).  Returns (n_clusters, theta per batch)."""
+    n_batches = len(N_b)
+    if max_iter_harmony < 1:
+        raise ValueError("max_iter_harmony must be >= 1")
+    if n_clusters is None:
+        n_clusters = default_n_clusters(n_cells)
+    if colsum_algo not in ("columns", "atomics", "gemm", "benchmark", None):
+        raise ValueError("colsum_algo must be 'columns', 'atomics', 'gemm', 'benchmark' or None")
+    th = theta_array(theta, n_batches)
+    if tau > 0:
+        th = th * (1 - np.exp(-np.asarray(N_b, dtype=np.float64) / (n_clusters * tau)) ** 2)
+    if not (0 < block_proportion <= 1):
+        raise ValueError("block_proportion must be in (0, 1]")
+    if int(n_cells * block_proportion) < 1:
+        raise ValueError("block_proportion * n_cells must be >= 1")
+    if dynamic_lambda:
+        if not np.isfinite(alpha) or alpha <= 0:
+            raise ValueError(
+                f"alpha must be a finite positive number when dynamic_lambda=True, got {alpha}."
+            )
+        if batch_prune_threshold is not None and not (0 <= batch_prune_threshold <= 1):
+            raise ValueError(
+                f"batch_prune_threshold must be in [0, 1] or None, got {batch_prune_threshold}."
+            )
+    if correction_method is not None and correction_method not in {"fast", "original", "batched"}:
+        raise ValueError("correction_method must be 'fast', 'original', or 'batched'.")
+    return int(n_clusters), th
+
+
+def harmonize(
+    Z,
+    batch_mat,
+    batch_key=None,
+    *,
+    n_clusters: int | None = None,
+    max_iter_harmony: int = 10,
+    max_iter_clustering: int = 200,
+    tol_harmony: float = 1e-4,
+    tol_clustering: float = 1e-5,
+    ridge_lambda: float = 1.0,
+    sigma: float = 0.1,
+    block_proportion: float = 0.05,
+    theta=2.0,
+    tau: int = 0,
+    correction_method: str | None = None,
+    colsum_algo: str | None = None,
+    random_state: int = 0,
+    stabilized_penalty: bool = True,
+    dynamic_lambda: bool = True,
+    alpha: float = 0.2,
+    batch_prune_threshold: float | None = 1e-5,
+    verbose: bool = False,
+    init_centroids=None,
+    precision: str | None = None,
+    return_info: bool = False,
+    device=None,
+):
+    """Integrate ``Z`` (cells x PCs) across the batches in ``batch_mat[batch_key]``.
+
+    Same parameters as the reference ``harmonize``; ``correction_method`` and
+    ``colsum_algo`` are accepted and validated but only select among equivalent
+    implementations there, so they do not change the computation here.  Extra:
+    ``init_centroids`` (n_clusters x PCs) fixes the starting centroids,
+    ``precision`` is one of "fp32", "fp64" (plain paths) or "bf16"/"fp16"
+    (tensor-core paths); by default it follows the dtype of ``Z``.
+    Returns the corrected embedding as a torch tensor on the GPU (and a
+    ``HarmonyInfo`` when ``return_info``).
+    """
+    n_cells, n_pcs = (int(v) for v in Z.shape)
+    codes = get_batch_codes(batch_mat, batch_key)
+    n_batches = int(codes.cat.categories.size)
+    cats_np = np.asarray(codes.cat.codes.values, dtype=np.int32)
+    if cats_np.shape[0] != n_cells:
+        raise ValueError("batch labels must have one entry per cell")
+    N_b = np.bincount(cats_np, minlength=n_batches).astype(np.int64)
+    n_clusters, th = resolve_parameters(
+        n_cells, N_b, n_clusters=n_clusters, max_iter_harmony=max_iter_harmony, theta=theta,
+        tau=tau, block_proportion=block_proportion, dynamic_lambda=dynamic_lambda, alpha=alpha,
+        batch_prune_threshold=batch_prune_threshold, correction_method=correction_method,
+        colsum_algo=colsum_algo)
+
+    lib = _lib.load()
+    if device is None:
+        device = Z.device if isinstance(Z, torch.Tensor) and Z.is_cuda else torch.device("cuda")
+    if isinstance(Z, torch.Tensor):
+        X = Z.to(device)
+    else:
+        X = torch.as_tensor(np.asarray(Z), device=device)
+    if X.dtype not in (torch.float32, torch.float64):
+        X = X.to(torch.float32)
+    prec = _resolve_precision(precision, X.dtype)
+    X = X.to(torch.float64 if prec == "fp64" else torch.float32).contiguous()
+
+    cats = torch.as_tensor(cats_np, device=device)
+    order = np.argsort(cats_np, kind="stable").astype(np.int32)
+    cell_index = torch.as_tensor(order, device=device)
+    offsets = np.zeros(n_batches + 1, dtype=np.int64)
+    offsets[1:] = np.cumsum(N_b)
+
+    if init_centroids is None:
+        Y0 = seeded_centroids(X, n_clusters, random_state)
+    else:
+        Y0 = torch.as_tensor(init_centroids, device=device)
+        if tuple(Y0.shape) != (n_clusters, n_pcs):
+            raise ValueError(
+                f"init_centroids must have shape ({n_clusters}, {n_pcs}), got {tuple(Y0.shape)}"
+            )
+    Y0 = Y0.to(X.dtype).contiguous()
+
+    p = HbParams()
+    p.n_cells = n_cells
+    p.n_pcs = n_pcs
+    p.n_clusters = n_clusters
+    p.n_batches = n_batches
+    p.precision = PRECISIONS[prec]
+    p.block_size = int(n_cells * block_proportion)
+    p.max_iter_harmony = max_iter_harmony
+    p.max_iter_clustering = max_iter_clustering
+    p.tol_harmony = tol_harmony
+    p.tol_clustering = tol_clustering
+    p.sigma = sigma
+    p.ridge_lambda = ridge_lambda
+    p.alpha = alpha
+    p.batch_prune_threshold = 0.0 if batch_prune_threshold is None else batch_prune_threshold
+    p.prune = 0 if batch_prune_threshold is None else 1
+    p.stabilized_penalty = int(bool(stabilized_penalty))
+    p.dynamic_lambda = int(bool(dynamic_lambda))
+    p.random_state = int(random_state) & 0xFFFFFFFFFFFFFFFF
+
+    plan = ctypes.c_void_p()
+    _lib.check(lib.hb_plan_create(ctypes.byref(p), ctypes.byref(plan)))
+    try:
+        ws_bytes = lib.hb_plan_workspace_bytes(plan)
+        ws = torch.empty(ws_bytes, dtype=torch.uint8, device=device)
+        Z_hat = torch.empty_like(X)
+        objs = (ctypes.c_double * (max_iter_harmony + 1))()
+        n_obj = ctypes.c_int32(0)
+        kobjs = (ctypes.c_double * max(1, max_iter_harmony * max_iter_clustering))()
+        kits = (ctypes.c_int32 * max_iter_harmony)()
+        conv = ctypes.c_int32(0)
+        out = HbOutputs(objs, ctypes.pointer(n_obj), kobjs, kits, ctypes.pointer(conv))
+        off_c = (ctypes.c_int64 * (n_batches + 1))(*offsets.tolist())
+        th_c = (ctypes.c_double * n_batches)(*th.tolist())
+        stream = torch.cuda.current_stream(device).cuda_stream
+        _lib.check(lib.hb_harmonize(plan, X.data_ptr(), cats.data_ptr(), cell_index.data_ptr(),
+                                    off_c, th_c, Y0.data_ptr(), ws.data_ptr(), ws_bytes,
+                                    Z_hat.data_ptr(), ctypes.byref(out), ctypes.c_void_p(stream)))
+    finally:
+        lib.hb_plan_destroy(plan)
+
+    n_outer = n_obj.value - 1
+    info = HarmonyInfo(
+        objectives_harmony=[objs[i] for i in range(n_obj.value)],
+        kmeans_objectives=[[kobjs[o * max_iter_clustering + i] for i in range(kits[o])]
+                           for o in range(n_outer)],
+        converged=bool(conv.value), n_outer=n_outer, n_clusters=n_clusters, precision=prec,
+    )
+    if info.converged and verbose:
+        print(f"Harmony converged in {n_outer} iterations")
+    if not info.converged:
+        warnings.warn("Harmony did not converge. Consider increasing the number of iterations")
+    return (Z_hat, info) if return_info else Z_hat

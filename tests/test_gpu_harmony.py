@@ -1,0 +1,115 @@
+"""End-to-end parity of the plain FP32 / FP64 paths against the CPU oracle,
+same seeded inputs and injected initial centroids."""
+
+import numpy as np
+import pandas as pd
+import pytest
+import torch
+
+from oracle import harmony_oracle as ho
+from rapids_singlecell_b200 import harmonize
+from rapids_singlecell_b200.synthetic import MixtureSpec, initial_centroids, make_config, make_mixture
+from tests._gpu import rel_maxabs
+
+pytestmark = pytest.mark.gpu
+
+# parity bars: relative max-abs error of Z_hat against the oracle of the same dtype
+TOL = {"fp32": 1e-4, "fp64": 1e-9}
+NP = {"fp32": np.float32, "fp64": np.float64}
+
+
+def _run_both(Z, cats, B, Y0, prec, **kw):
+    labels = pd.Categorical.from_codes(cats, categories=[f"b{i}" for i in range(B)])
+    Zt = torch.as_tensor(Z.astype(NP[prec]), device="cuda")
+    out, info = harmonize(Zt, labels, None, init_centroids=Y0, precision=prec, return_info=True, **kw)
+    okw = {k: v for k, v in kw.items() if k not in ("correction_method", "colsum_algo")}
+    ref = ho.harmonize(Z, cats, B, Y0, dtype=NP[prec], **okw)
+    return out.cpu().numpy(), info, ref
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_c1_small_parity(prec):
+    cfg = make_config("C1", seed=1, n_cells=4000)
+    Y0 = cfg["Y0"][:40]
+    out, info, ref = _run_both(cfg["Z"], cfg["cats"], cfg["n_batches"], Y0, prec, n_clusters=40,
+                               max_iter_harmony=3, max_iter_clustering=8)
+    assert info.n_outer == ref.n_outer
+    assert [len(k) for k in info.kmeans_objectives] == [len(k) for k in ref.kmeans_objectives]
+    np.testing.assert_allclose(info.objectives_harmony, ref.objectives_harmony, rtol=1e-5)
+    assert rel_maxabs(out, ref.Z_hat) < TOL[prec]
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_c1_full_default_tolerances(prec):
+    cfg = make_config("C1", seed=0)
+    out, info, ref = _run_both(cfg["Z"], cfg["cats"], cfg["n_batches"], cfg["Y0"], prec,
+                               n_clusters=100, max_iter_harmony=10, max_iter_clustering=20)
+    assert info.converged == ref.converged and info.n_outer == ref.n_outer
+    np.testing.assert_allclose(info.objectives_harmony, ref.objectives_harmony, rtol=1e-5)
+    assert rel_maxabs(out, ref.Z_hat) < TOL[prec]
+
+
+def test_harmony1_flavor_fixed_iterations():
+    cfg = make_config("C1", seed=2, n_cells=3000)
+    out, info, ref = _run_both(cfg["Z"], cfg["cats"], cfg["n_batches"], cfg["Y0"][:30], "fp32",
+                               n_clusters=30, max_iter_harmony=4, max_iter_clustering=5,
+                               tol_harmony=-np.inf, tol_clustering=-np.inf,
+                               stabilized_penalty=False, dynamic_lambda=False, ridge_lambda=1.0)
+    assert info.n_outer == 4
+    assert rel_maxabs(out, ref.Z_hat) < TOL["fp32"]
+
+
+@pytest.mark.parametrize("n,d,K,B,bp", [(1001, 3, 7, 1, 0.05), (997, 5, 17, 4, 0.07),
+                                        (2500, 33, 65, 6, 0.1), (640, 64, 129, 2, 0.5),
+                                        (5000, 100, 200, 12, 0.05)])
+def test_odd_shapes(n, d, K, B, bp):
+    spec = MixtureSpec(n, d, 5, B, "dirichlet", (), 0.5, (0.8, 1.2))
+    Z, cats, _ = make_mixture(spec, 11)
+    Y0 = initial_centroids(Z, K, 12)
+    out, info, ref = _run_both(Z, cats, B, Y0, "fp32", n_clusters=K, max_iter_harmony=2,
+                               max_iter_clustering=4, block_proportion=bp,
+                               tol_harmony=-np.inf, tol_clustering=-np.inf)
+    assert rel_maxabs(out, ref.Z_hat) < TOL["fp32"]
+
+
+def test_theta_list_tau_and_empty_category():
+    cfg = make_config("C1", seed=4, n_cells=3000)
+    Z, cats = cfg["Z"], cfg["cats"]
+    # a fourth, empty batch category: N_b = 0 is pruned
+    labels = pd.Categorical.from_codes(cats, categories=["a", "b", "c", "unused"])
+    Y0 = cfg["Y0"][:25]
+    kw = dict(n_clusters=25, max_iter_harmony=2, max_iter_clustering=5, theta=[1.0, 2.0, 0.5, 3.0],
+              tau=5)
+    out = harmonize(torch.as_tensor(Z, device="cuda"), labels, None, init_centroids=Y0, **kw)
+    ref = ho.harmonize(Z, cats, 4, Y0, dtype=np.float32, **kw)
+    assert rel_maxabs(out.cpu().numpy(), ref.Z_hat) < TOL["fp32"]
+
+
+def test_harmony_integrate_dropin_surface():
+    from rapids_singlecell_b200.pp import harmony_integrate
+
+    cfg = make_config("C1", seed=5, n_cells=2000)
+
+    class AData:
+        def __init__(self):
+            self.obsm = {"X_pca": cfg["Z"].astype(np.float64)}
+            self.obs = pd.DataFrame({"batch": [f"s{c}" for c in cfg["cats"]],
+                                     "lane": [f"l{c % 2}" for c in cfg["cats"]]})
+
+    a = AData()
+    harmony_integrate(a, "batch", init_centroids=cfg["Y0"][:66].astype(np.float64), n_clusters=66)
+    assert a.obsm["X_pca_harmony"].shape == a.obsm["X_pca"].shape
+    assert a.obsm["X_pca_harmony"].dtype == np.float64
+    ref = ho.harmonize(cfg["Z"].astype(np.float64), cfg["cats"], 3,
+                       cfg["Y0"][:66].astype(np.float64), n_clusters=66)
+    assert rel_maxabs(a.obsm["X_pca_harmony"], ref.Z_hat) < TOL["fp64"]
+    # two keys joined with "," (6 combined batches), float32
+    b = AData()
+    harmony_integrate(b, ["batch", "lane"], dtype=np.float32, max_iter_harmony=2)
+    assert np.isfinite(b.obsm["X_pca_harmony"]).all()
+    with pytest.raises(ValueError, match="alpha must be a finite positive"):
+        harmony_integrate(AData(), "batch", alpha=-1.0)
+    c = AData()
+    c.obsm["X_pca"][0, 0] = np.nan
+    with pytest.raises(RuntimeError, match="NaN"):
+        harmony_integrate(c, "batch")

@@ -1,0 +1,64 @@
+"""Host-side parameter resolution mirrors the reference's validation
+(tests/test_harmony.py:95-110 and _harmony/__init__.py:154-200); these raise
+before any GPU work, so they run on CPU."""
+
+import numpy as np
+import pandas as pd
+import pytest
+
+from rapids_singlecell_b200.harmony import default_n_clusters, harmonize, theta_array
+
+
+def _data(n=300):
+    rng = np.random.default_rng(0)
+    Z = rng.normal(size=(n, 10)).astype(np.float32)
+    obs = pd.DataFrame({"batch": rng.integers(0, 3, n).astype(str), "b2": rng.integers(0, 2, n).astype(str)})
+    return Z, obs
+
+
+@pytest.mark.parametrize("bad_alpha", [-0.1, 0.0, float("inf"), float("nan")])
+def test_bad_alpha(bad_alpha):
+    Z, obs = _data()
+    with pytest.raises(ValueError, match="alpha must be a finite positive"):
+        harmonize(Z, obs, "batch", alpha=bad_alpha)
+
+
+@pytest.mark.parametrize("bad_threshold", [-0.1, 1.5, 2.0])
+def test_bad_prune_threshold(bad_threshold):
+    Z, obs = _data()
+    with pytest.raises(ValueError, match="batch_prune_threshold must be in"):
+        harmonize(Z, obs, "batch", batch_prune_threshold=bad_threshold)
+
+
+def test_bad_correction_method_and_iters():
+    Z, obs = _data()
+    with pytest.raises(ValueError, match="correction_method must be"):
+        harmonize(Z, obs, "batch", correction_method="nope")
+    with pytest.raises(ValueError, match="max_iter_harmony must be >= 1"):
+        harmonize(Z, obs, "batch", max_iter_harmony=0)
+
+
+def test_theta_size_mismatch():
+    Z, obs = _data()
+    with pytest.raises(ValueError, match="Theta array size"):
+        harmonize(Z, obs, "batch", theta=[1.0, 2.0])
+    np.testing.assert_array_equal(theta_array(2, 3), [2.0, 2.0, 2.0])
+
+
+def test_default_n_clusters():
+    assert default_n_clusters(20_000) == 100
+    assert default_n_clusters(600) == 20
+    assert default_n_clusters(10) == 2
+
+
+def test_flavor_validation():
+    from rapids_singlecell_b200.pp import harmony_integrate
+
+    class A:
+        obsm = {"X_pca": np.zeros((10, 3))}
+        obs = pd.DataFrame({"batch": ["a"] * 10})
+
+    with pytest.raises(ValueError, match="flavor must be"):
+        harmony_integrate(A(), "batch", flavor="harmony3")
+    with pytest.raises(ValueError, match="is not available in adata.obsm"):
+        harmony_integrate(A(), "batch", basis="nope")

@@ -1,0 +1,333 @@
+"""Harmony cell-iterations/s on B200.
+
+One step = one full Harmony integration (fixed 10 outer x 20 k-means
+iterations, tolerances -inf) of the 500,000-cell x 50-PC workload (30 cell
+types, 8 batches with Dirichlet(1) sizes, per-batch shift N(0, 0.5^2) and
+scale U(0.8, 1.2), K = 100, theta = 2, sigma = 0.1), synthetic and seeded.
+
+  value   device-resident throughput of the fused 16-bit tensor-core path
+          (bf16 unless --precision says otherwise): inputs already in HBM
+  e2e     the same through the public ``harmonize`` call from pinned host
+          memory, host->device copy of the embedding and device->host copy of
+          the corrected embedding inside the timed region
+  plain   the float32 plain path (the drop-in for dtype=np.float32)
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Multi-GPU (torchrun): independent replicas, one per GPU; value = all ranks'
+cell-iterations / max-over-ranks time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+OUTER, INNER = 10, 20
+WORKLOAD = "C2"
+METRIC = "Harmony cell-iters/s & p50/p99 latency: BF16 batched vs FP32 plain on 1 B200"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="bf16", choices=["bf16", "fp16", "fp32"])
+    ap.add_argument("--no-plain", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), \
+        int(os.environ.get("LOCAL_RANK", 0))
+
+
+def workload():
+    from rapids_singlecell_b200.synthetic import make_config
+
+    cfg = make_config(WORKLOAD, seed=0)
+    return cfg
+
+
+def config_dict(cfg, extra=None):
+    n, d = cfg["Z"].shape
+    c = {"workload": f"{WORKLOAD}: {n} cells x {d} PCs, {cfg['n_batches']} batches, "
+                     f"K={cfg['n_clusters']}, {OUTER} outer x {INNER} k-means iterations fixed",
+         "n_cells": n, "n_pcs": d, "n_clusters": cfg["n_clusters"], "n_batches": cfg["n_batches"],
+         "outer_iters": OUTER, "kmeans_iters": INNER, "block_proportion": 0.05,
+         "l2": "inputs larger than L2 (R, Z_norm and X exceed 126 MB)"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ---------------------------------------------------------------------------
+def cpu_reference_step(cfg, outer, inner, dtype=np.float32):
+    """One bounded sample on the host: the CPU oracle (NumPy port of the
+    reference algorithm) for `outer` x `inner` iterations."""
+    from oracle import harmony_oracle as ho
+
+    t = time.perf_counter()
+    ho.harmonize(cfg["Z"], cfg["cats"], cfg["n_batches"], cfg["Y0"], n_clusters=cfg["n_clusters"],
+                 max_iter_harmony=outer, max_iter_clustering=inner, tol_harmony=-np.inf,
+                 tol_clustering=-np.inf, dtype=dtype)
+    return time.perf_counter() - t
+
+
+def blas_threads():
+    try:
+        from threadpoolctl import threadpool_info
+
+        return max([i.get("num_threads", 1) for i in threadpool_info()] or [1])
+    except Exception:  # noqa: BLE001
+        return os.cpu_count() or 1
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    cfg = workload()
+    n = cfg["Z"].shape[0]
+    # each step: 1 outer x 1 k-means iteration of the same workload on the host
+    for _ in range(args.warmup):
+        cpu_reference_step(cfg, 1, 1)
+    times = [cpu_reference_step(cfg, 1, 1) for _ in range(args.steps)]
+    t = float(np.median(times))
+    v = n * 1 / t
+    cores = blas_threads()
+    out = {"impl": "reference", "metric": METRIC, "value": v, "unit": "cell-iters/s",
+           "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": config_dict(cfg, {"sample": "1 outer x 1 k-means iteration per step"}),
+           "cpu_baseline": {"value": v, "unit": "cell-iters/s", "cores": cores, "kind": "port",
+                            "sample": "NumPy oracle (float32) of the reference algorithm, "
+                                      "1 outer x 1 k-means iteration of the full workload per step"},
+           "e2e": {"value": v, "unit": "cell-iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    def __init__(self, gpu_index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={gpu_index}", f"--query-gpu={q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:  # noqa: BLE001
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        self.p.wait(timeout=10)
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if len(r) > 8 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) > 8 and r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows if len(r) > 8 for i in range(4)
+                          if r[5 + i].strip() == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """dram bytes per block-update launch from the committed ncu summary, if any."""
+    f = ROOT / "profiles" / "block_update_C2_bf16.md"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+def run_ours(args):
+    import torch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist  # noqa: F811
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    from rapids_singlecell_b200.harmony import HarmonyProblem, harmonize
+
+    cfg = workload()
+    Z, cats, B, K = cfg["Z"], cfg["cats"], cfg["n_batches"], cfg["n_clusters"]
+    n = Z.shape[0]
+    theta = np.full(B, 2.0)
+    common = dict(n_clusters=K, max_iter_harmony=OUTER, max_iter_clustering=INNER,
+                  tol_harmony=-np.inf, tol_clustering=-np.inf)
+    cell_iters = n * OUTER * INNER
+    dev = torch.device("cuda", local)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        per = []
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        start.record()
+        for _ in range(steps):
+            e0.record()
+            fn()
+            e1.record()
+            e1.synchronize()
+            per.append(e0.elapsed_time(e1))
+        end.record()
+        torch.cuda.synchronize()
+        barrier()
+        total_ms = start.elapsed_time(end)
+        return max_over_ranks(total_ms) / steps, per
+
+    # ---- fused tensor-core path, device resident -----------------------------
+    X = torch.as_tensor(Z, device=dev)
+    prob = HarmonyProblem(X, cats, B, torch.as_tensor(cfg["Y0"], device=dev), theta,
+                          precision=args.precision, **common)
+    last = {}
+
+    def step_resident():
+        _, info = prob.run(profile=True)
+        last["info"] = info
+
+    clocks = ClockSampler(local) if rank == 0 else None
+    ms, per = timed(step_resident, args.steps, args.warmup)
+    clk = clocks.stop() if clocks else None
+    prof = last["info"].profile
+    value = cell_iters * world / (ms / 1e3)
+
+    # ---- end to end through the public API from pinned host memory ------------
+    Z_pin = torch.from_numpy(Z).pin_memory()
+    codes = cats.astype(np.int32)
+
+    def step_e2e():
+        out = harmonize(Z_pin, codes, None, init_centroids=cfg["Y0"], precision=args.precision,
+                        device=dev, **common)
+        last["e2e"] = out.cpu()
+
+    import warnings
+
+    warnings.simplefilter("ignore")
+    ms_e2e, per_e2e = timed(step_e2e, args.steps, args.warmup)
+    e2e_value = cell_iters * world / (ms_e2e / 1e3)
+
+    # ---- plain float32 path (the drop-in for dtype=np.float32) -----------------
+    plain = None
+    if not args.no_plain:
+        prob32 = HarmonyProblem(X, cats, B, torch.as_tensor(cfg["Y0"], device=dev), theta,
+                                precision="fp32", **common)
+        ms32, per32 = timed(lambda: prob32.run(), max(1, min(args.steps, 3)), 1)
+        plain = {"value": cell_iters * world / (ms32 / 1e3), "ms_per_step": ms32,
+                 "p50_ms": float(np.percentile(per32, 50)), "p99_ms": float(np.percentile(per32, 99))}
+        prob32.close()
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    # ---- roofline of the dominant kernel (fused block update) ------------------
+    peak, peak_kind = measured_peaks()
+    achieved = prof["block_bytes"] / (prof["block_ms"] / 1e3) / 1e9 if prof["block_ms"] > 0 else 0.0
+    launches = prof["block_launches"]
+    traffic = profiled_traffic()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                "kernel": "k_tc_block_update (fused similarity + exp/penalty + normalise + O delta)",
+                "algorithmic_bytes_per_launch": prof["block_bytes"] / max(1, launches),
+                "avg_launch_us": prof["block_ms"] / max(1, launches) * 1e3,
+                "block_time_share": prof["block_ms"] / ms,
+                "centroid": {"achieved_gbs": prof["centroid_bytes"] / (prof["centroid_ms"] / 1e3) / 1e9
+                             if prof["centroid_ms"] > 0 else 0.0,
+                             "time_share": prof["centroid_ms"] / ms}}
+
+    # ---- CPU baseline (bounded sample on the host cores) -----------------------
+    t_cpu = cpu_reference_step(cfg, 1, 1)
+    cpu = {"value": n / t_cpu, "unit": "cell-iters/s", "cores": blas_threads(), "kind": "port",
+           "sample": "NumPy float32 oracle of the reference algorithm: 1 outer x 1 k-means "
+                     f"iteration of the {n}-cell workload ({t_cpu:.1f} s)"}
+
+    h2d = Z.nbytes + codes.nbytes + cfg["Y0"].nbytes
+    d2h = Z.nbytes + 8 * (OUTER + 1)
+    res = {
+        "metric": METRIC, "value": value, "unit": "cell-iters/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": args.precision if args.precision != "fp32" else "f32", "data": "synthetic",
+        "config": config_dict(cfg, {"precision": args.precision,
+                                    "parallelism": "replicas" if world > 1 else "single"}),
+        "p50_ms": float(np.percentile(per, 50)), "p99_ms": float(np.percentile(per, 99)),
+        "e2e": {"value": e2e_value, "unit": "cell-iters/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e,
+                "p50_ms": float(np.percentile(per_e2e, 50)), "p99_ms": float(np.percentile(per_e2e, 99))},
+        "plain_fp32": plain,
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "clocks": clk,
+        "gpu_launches": int(prof["kernel_launches"]) * args.steps,
+    }
+    print(json.dumps(res))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -21,6 +21,8 @@
  *   hb_ridge_inverse      -> _harmony_correction_cuda.compute_inv_mat
  *                            (_cuda/harmony/correction/kernels_correction_fast.cuh:24-123)
  *   hb_lambda_kb          -> _compute_lambda_kb (preprocessing/_harmony/__init__.py:454-480)
+ *   hb_similarity         -> the similarity GEMM of clustering_loop_impl
+ *                            (_cuda/harmony/clustering/clustering.cu:284-289)
  */
 #ifndef HARMONY_B200_H
 #define HARMONY_B200_H
@@ -77,6 +79,17 @@ typedef struct hb_params {
 
 typedef struct hb_plan hb_plan;
 
+/* Optional device-time profile of one run (CUDA events around the timed launches). */
+typedef struct hb_profile {
+  int64_t kernel_launches;    /* kernels launched by the run */
+  int64_t block_launches;     /* fused block-update launches */
+  double block_ms;            /* summed device time of those launches */
+  double block_bytes;         /* algorithmic HBM bytes they move (unpadded rows) */
+  int64_t centroid_launches;  /* centroid-sum launch pairs (partials + reduce) */
+  double centroid_ms;
+  double centroid_bytes;
+} hb_profile;
+
 /* Outputs of one run (host memory owned by the caller). */
 typedef struct hb_outputs {
   double* objectives;         /* [1 + max_iter_harmony]: initial + one per outer iteration */
@@ -84,6 +97,7 @@ typedef struct hb_outputs {
   double* kmeans_objectives;  /* optional [max_iter_harmony * max_iter_clustering] */
   int32_t* kmeans_iters;      /* optional [max_iter_harmony]: k-means iterations run per outer */
   int32_t* converged;         /* 1 if the outer loop met tol_harmony */
+  hb_profile* profile;        /* optional: filled when not NULL */
 } hb_outputs;
 
 HB_API int hb_plan_create(const hb_params* params, hb_plan** plan);
@@ -111,10 +125,13 @@ HB_API int hb_l2_normalize(const void* src, void* dst, int64_t rows, int32_t col
                     void* stream);
 
 /* Cell lists of every block of `n_iters` k-means iterations (seeds given on the host):
- * idx[c*n + j*block_size + r] = r-th cell (ascending index) of block j for seed c. */
-HB_API size_t hb_block_lists_workspace_bytes(int64_t n, int64_t block_size);
+ * idx[c*n + j*block_size + r] is the r-th cell of block j for seed c.  Block j holds the
+ * cells whose shuffle keys rank in [j*block_size, (j+1)*block_size); inside a block cells
+ * are ordered by (cats[i], i), or by i when cats is NULL. */
+HB_API size_t hb_block_lists_workspace_bytes(int64_t n, int64_t block_size, int32_t n_batches);
 HB_API int hb_block_lists(int64_t n, int64_t block_size, const uint32_t* seeds, int32_t n_iters,
-                   int32_t* idx, void* workspace, size_t workspace_bytes, void* stream);
+                   const int32_t* cats, int32_t n_batches, int32_t* idx, void* workspace,
+                   size_t workspace_bytes, void* stream);
 
 /* penalty[b,k] = ((E+1)/(O[+E]+1)) ** theta[b]; float64 arrays [B,K], theta [B] */
 HB_API int hb_penalty(const double* E, const double* O, const double* theta, double* penalty,
@@ -129,6 +146,15 @@ HB_API int hb_lambda_kb(const double* E, const double* O, const double* N_b, dou
  * inv is [n_clusters, n_batches+1, n_batches+1] */
 HB_API int hb_ridge_inverse(const double* O, const double* lambda_kb, double* inv, int32_t n_batches,
                      int32_t n_clusters, void* stream);
+
+/* Similarity rows on the tensor core: S[q, k] = Zn[idx[q], :] . Yn[k, :] for q < n, k < n_clusters.
+ * Zn [*, ldz] and Yn [n_clusters, ldy] are 16-bit (dtype HB_FP16 / HB_BF16), zero-padded past
+ * n_pcs (<= 128); ldz, ldy multiples of 8.  S is float32 [n, n_clusters].  *err (device int32)
+ * is set non-zero if a bounded tensor-core wait gave up.  Replaces the similarity GEMM of
+ * the reference (_cuda/harmony/clustering/clustering.cu:284-289). */
+HB_API int hb_similarity(const void* Zn, int32_t ldz, const void* Yn, int32_t ldy, const int32_t* idx,
+                  int64_t n, int32_t n_pcs, int32_t n_clusters, int32_t dtype, float* S,
+                  int32_t* err, void* stream);
 
 HB_API const char* hb_last_error(void);
 HB_API const char* hb_version(void);

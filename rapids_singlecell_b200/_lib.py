@@ -29,7 +29,7 @@ PRECISIONS = {"fp32": HB_FP32, "fp64": HB_FP64, "bf16": HB_BF16, "fp16": HB_FP16
 EXPORTED = (
     "hb_plan_create", "hb_plan_destroy", "hb_plan_workspace_bytes", "hb_harmonize",
     "hb_l2_normalize", "hb_block_lists_workspace_bytes", "hb_block_lists", "hb_penalty",
-    "hb_lambda_kb", "hb_ridge_inverse", "hb_last_error", "hb_version",
+    "hb_lambda_kb", "hb_ridge_inverse", "hb_similarity", "hb_last_error", "hb_version",
 )
 
 
@@ -57,6 +57,18 @@ class HbParams(ctypes.Structure):
     ]
 
 
+class HbProfile(ctypes.Structure):
+    _fields_ = [
+        ("kernel_launches", ctypes.c_int64),
+        ("block_launches", ctypes.c_int64),
+        ("block_ms", ctypes.c_double),
+        ("block_bytes", ctypes.c_double),
+        ("centroid_launches", ctypes.c_int64),
+        ("centroid_ms", ctypes.c_double),
+        ("centroid_bytes", ctypes.c_double),
+    ]
+
+
 class HbOutputs(ctypes.Structure):
     _fields_ = [
         ("objectives", ctypes.POINTER(ctypes.c_double)),
@@ -64,6 +76,7 @@ class HbOutputs(ctypes.Structure):
         ("kmeans_objectives", ctypes.POINTER(ctypes.c_double)),
         ("kmeans_iters", ctypes.POINTER(ctypes.c_int32)),
         ("converged", ctypes.POINTER(ctypes.c_int32)),
+        ("profile", ctypes.POINTER(HbProfile)),
     ]
 
 
@@ -102,10 +115,10 @@ def load() -> ctypes.CDLL:
     lib.hb_harmonize.restype = c_int
     lib.hb_l2_normalize.argtypes = [c_void_p, c_void_p, c_i64, c_i32, c_i32, c_void_p]
     lib.hb_l2_normalize.restype = c_int
-    lib.hb_block_lists_workspace_bytes.argtypes = [c_i64, c_i64]
+    lib.hb_block_lists_workspace_bytes.argtypes = [c_i64, c_i64, c_i32]
     lib.hb_block_lists_workspace_bytes.restype = c_size
-    lib.hb_block_lists.argtypes = [c_i64, c_i64, P(ctypes.c_uint32), c_i32, c_void_p, c_void_p,
-                                   c_size, c_void_p]
+    lib.hb_block_lists.argtypes = [c_i64, c_i64, P(ctypes.c_uint32), c_i32, c_void_p, c_i32,
+                                   c_void_p, c_void_p, c_size, c_void_p]
     lib.hb_block_lists.restype = c_int
     lib.hb_penalty.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_i32, c_i32, c_i32, c_void_p]
     lib.hb_penalty.restype = c_int
@@ -115,6 +128,9 @@ def load() -> ctypes.CDLL:
     lib.hb_lambda_kb.restype = c_int
     lib.hb_ridge_inverse.argtypes = [c_void_p, c_void_p, c_void_p, c_i32, c_i32, c_void_p]
     lib.hb_ridge_inverse.restype = c_int
+    lib.hb_similarity.argtypes = [c_void_p, c_i32, c_void_p, c_i32, c_void_p, c_i64, c_i32, c_i32,
+                                  c_i32, c_void_p, c_void_p, c_void_p]
+    lib.hb_similarity.restype = c_int
     lib.hb_last_error.argtypes = []
     lib.hb_last_error.restype = ctypes.c_char_p
     lib.hb_version.argtypes = []

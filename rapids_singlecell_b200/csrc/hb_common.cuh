@@ -16,6 +16,7 @@ constexpr int kBinShift = 20;
 constexpr int kPartTile = 2048;     // cells per tile of the stable block partition
 constexpr int kMaxBlocks = 512;     // most block updates per k-means iteration
 constexpr int kMaxIterChunk = 8;    // k-means iterations whose block lists are built per launch
+constexpr int kMaxBuckets = 4096;   // (block, batch) buckets of the stable partition
 
 // Shuffle key of cell i for one k-means iteration.  This is the PCG-RXS-M-XS
 // 32-bit hash (M. O'Neill, "PCG: a family of simple fast space-efficient
@@ -72,18 +73,21 @@ __device__ __forceinline__ T warp_sum(T v) {
   return v;
 }
 
-// Block-wide sum; every thread receives the total.  `red` needs 32 slots.
+// Block-wide sum over all threads of a (1-, 2- or 3-D) block; every thread
+// receives the total.  `red` needs 32 slots; the thread count must be a
+// multiple of 32.
 template <typename T>
 __device__ __forceinline__ T block_sum(T v, T* red) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int nw = (blockDim.x + 31) >> 5;
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int lane = tid & 31, w = tid >> 5;
+  const int nw = (blockDim.x * blockDim.y * blockDim.z + 31) >> 5;
   v = warp_sum(v);
   __syncthreads();
   if (lane == 0) red[w] = v;
   __syncthreads();
-  T t = (threadIdx.x < (unsigned)nw) ? red[threadIdx.x] : T(0);
+  T t = (tid < nw) ? red[tid] : T(0);
   if (w == 0) t = warp_sum(t);
-  if (threadIdx.x == 0) red[0] = t;
+  if (tid == 0) red[0] = t;
   __syncthreads();
   T r = red[0];
   __syncthreads();
@@ -121,8 +125,11 @@ void set_error(const char* fmt, ...);
     }                                                                              \
   } while (0)
 
+extern thread_local int64_t g_launches;  // kernels launched by this thread (profiling)
+
 #define HB_LAUNCH_CHECK()                                                          \
   do {                                                                             \
+    ++::hb::g_launches;                                                            \
     cudaError_t _e = cudaGetLastError();                                           \
     if (_e != cudaSuccess) {                                                       \
       ::hb::set_error("%s:%d launch failed: %s", __FILE__, __LINE__, cudaGetErrorString(_e)); \

@@ -13,6 +13,7 @@
 namespace hb {
 
 static thread_local char g_err[1024] = "";
+thread_local int64_t g_launches = 0;
 
 void set_error(const char* fmt, ...) {
   va_list ap;
@@ -34,7 +35,9 @@ using namespace hb;
 
 struct hb_plan {
   hb_params p;
-  int esz;        // bytes of the plain compute type (4 or 8)
+  int esz;        // bytes of the input / output type (4 or 8)
+  int ssz;        // bytes of the Z_norm / R storage type (2, 4 or 8)
+  int asz;        // bytes of the split-n partial sums (4 or 8)
   int ldz, ldr, ldy;
   MembershipLayout ml;
   int cen_chunks; // split-n chunks of the centroid sum
@@ -42,6 +45,10 @@ struct hb_plan {
   int max_m_chunks, max_apply_tiles;
   int64_t m_chunk_len;
   size_t ws_bytes;
+  std::vector<cudaEvent_t> events;  // profiling pool (created on first profiled run)
+  ~hb_plan() {
+    for (cudaEvent_t e : events) cudaEventDestroy(e);
+  }
 };
 
 namespace {
@@ -61,6 +68,7 @@ struct Work {
   double* obj_out;
   double* M;
   int32_t* idx;
+  int* err;
   AccumChunk* cen_chunks;
   AccumChunk* m_chunks;
   int32_t* batch_chunk_off;
@@ -72,13 +80,12 @@ void carve(const hb_plan& P, Carver& cv, Work& w) {
   const hb_params& p = P.p;
   const int64_t n = p.n_cells;
   const int K = p.n_clusters, B = p.n_batches, d = p.n_pcs;
-  const int e = P.esz;
-  w.Zn = cv.take<char>((size_t)n * P.ldz * e);
-  w.R = cv.take<char>((size_t)n * P.ldr * e);
-  w.Yn = cv.take<char>((size_t)K * P.ldy * e);
-  w.Ypart = cv.take<char>((size_t)P.cen_chunks * K * d * e);
-  w.Mpart = cv.take<char>((size_t)P.max_m_chunks * K * d * e);
-  w.W = cv.take<char>((size_t)B * K * d * e);
+  w.Zn = cv.take<char>((size_t)n * P.ldz * P.ssz);
+  w.R = cv.take<char>((size_t)n * P.ldr * P.ssz);
+  w.Yn = cv.take<char>((size_t)K * P.ldy * P.ssz);
+  w.Ypart = cv.take<char>((size_t)P.cen_chunks * K * d * P.asz);
+  w.Mpart = cv.take<char>((size_t)P.max_m_chunks * K * d * P.asz);
+  w.W = cv.take<char>((size_t)B * K * d * P.esz);
   for (int i = 0; i < 3; ++i) w.O[i] = cv.take<double>((size_t)B * K);
   w.Pr = cv.take<double>(B);
   w.theta = cv.take<double>(B);
@@ -87,6 +94,7 @@ void carve(const hb_plan& P, Carver& cv, Work& w) {
   w.obj_out = cv.take<double>(std::max(p.max_iter_clustering, 1) + 1);
   w.M = cv.take<double>((size_t)K * (B + 1) * d);
   w.idx = cv.take<int32_t>((size_t)kMaxIterChunk * n);
+  w.err = cv.take<int>(4);
   w.cen_chunks = cv.take<AccumChunk>(P.cen_chunks);
   w.m_chunks = cv.take<AccumChunk>(P.max_m_chunks);
   w.batch_chunk_off = cv.take<int32_t>(B + 1);
@@ -111,8 +119,12 @@ int validate(const hb_params& p) {
   if (p.n_clusters > 256) { set_error("n_clusters=%d exceeds the supported maximum of 256", p.n_clusters); return HB_ERR_UNSUPPORTED; }
   if (p.precision == HB_FP64 && p.n_pcs > 128) { set_error("n_pcs=%d exceeds 128 for float64", p.n_pcs); return HB_ERR_UNSUPPORTED; }
   if (p.n_pcs > 256) { set_error("n_pcs=%d exceeds the supported maximum of 256", p.n_pcs); return HB_ERR_UNSUPPORTED; }
-  if (p.precision != HB_FP32 && p.precision != HB_FP64) {
-    set_error("precision %d is not available in this build", p.precision);
+  if (p.precision < HB_FP32 || p.precision > HB_FP16) {
+    set_error("unknown precision %d", p.precision);
+    return HB_ERR_INVALID;
+  }
+  if ((p.precision == HB_BF16 || p.precision == HB_FP16) && p.n_pcs > 128) {
+    set_error("n_pcs=%d exceeds 128 for the tensor-core path", p.n_pcs);
     return HB_ERR_UNSUPPORTED;
   }
   const size_t smem = (size_t)(p.precision == HB_FP64 ? 8 : 4) * 2 * p.n_batches * p.n_clusters;
@@ -120,7 +132,7 @@ int validate(const hb_params& p) {
     set_error("n_batches * n_clusters = %d too large (shared-memory O/penalty tables)", p.n_batches * p.n_clusters);
     return HB_ERR_UNSUPPORTED;
   }
-  if (MembershipLayout ml = membership_layout(p.n_cells, p.block_size); ml.cap > 16384) {
+  if (MembershipLayout ml = membership_layout(p.n_cells, p.block_size, 1); ml.cap > 16384) {
     set_error("n_cells=%lld too large for the block splitter select", (long long)p.n_cells);
     return HB_ERR_UNSUPPORTED;
   }
@@ -141,11 +153,13 @@ int hb_plan_create(const hb_params* params, hb_plan** plan) {
   P->p = *params;
   const hb_params& p = P->p;
   P->esz = p.precision == HB_FP64 ? 8 : 4;
-  const int vec = 16 / P->esz;
+  P->ssz = (p.precision == HB_BF16 || p.precision == HB_FP16) ? 2 : P->esz;
+  P->asz = P->esz;
+  const int vec = 16 / P->ssz;
   P->ldz = (int)align_up(p.n_pcs, vec);
   P->ldr = (int)align_up(p.n_clusters, vec);
   P->ldy = P->ldz;
-  P->ml = membership_layout(p.n_cells, p.block_size);
+  P->ml = membership_layout(p.n_cells, p.block_size, p.n_batches);
   const int sms = num_sms();
   P->cen_tiles = div_up(p.n_clusters, 128) * div_up(p.n_pcs, 64);
   const int64_t target = std::max(1, 2 * sms / P->cen_tiles);
@@ -165,34 +179,59 @@ void hb_plan_destroy(hb_plan* plan) { delete plan; }
 
 size_t hb_plan_workspace_bytes(const hb_plan* plan) { return plan ? plan->ws_bytes : 0; }
 
+int hb_similarity(const void* Zn, int32_t ldz, const void* Yn, int32_t ldy, const int32_t* idx, int64_t n,
+                  int32_t n_pcs, int32_t n_clusters, int32_t dtype, float* S, int32_t* err, void* stream) {
+  if (n < 1 || n_pcs < 1 || n_pcs > 128 || n_clusters < 1 || n_clusters > 256 || ldz % 8 || ldy % 8 ||
+      ldz < n_pcs || ldy < n_pcs || !Zn || !Yn || !idx || !S || !err) {
+    set_error("hb_similarity: bad argument");
+    return HB_ERR_INVALID;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  if (dtype == HB_FP16)
+    return launch_tc_similarity<__half>((const __half*)Zn, ldz, (const __half*)Yn, ldy, idx, nullptr, n, n_pcs,
+                                        n_clusters, S, err, st);
+  if (dtype == HB_BF16)
+    return launch_tc_similarity<__nv_bfloat16>((const __nv_bfloat16*)Zn, ldz, (const __nv_bfloat16*)Yn, ldy,
+                                               idx, nullptr, n, n_pcs, n_clusters, S, err, st);
+  set_error("hb_similarity: dtype must be HB_FP16 or HB_BF16");
+  return HB_ERR_INVALID;
+}
+
 }  // extern "C"
 
 namespace {
 
-template <typename T>
-int block_update(const BlockArgs& a, const double* in, double* out, double* zero, cudaStream_t st) {
-  if (sizeof(T) == 8) return launch_block_update_f64(a, in, out, zero, st);
-  return launch_block_update_f32(a, in, out, zero, st);
+template <typename S>
+int block_update(const BlockArgs& a, const double* in, double* out, double* zero, int* err,
+                 cudaStream_t st) {
+  if constexpr (std::is_same<S, double>::value) return launch_block_update_f64(a, in, out, zero, st);
+  else if constexpr (std::is_same<S, float>::value) return launch_block_update_f32(a, in, out, zero, st);
+  else return launch_tc_block_update<S>(a, in, out, zero, err, st);
 }
 
 struct ORing {
   double* buf[3];
+  int* err;
   int cur = 0;
   // launch a block update that reads the current state and produces the next
-  template <typename T>
+  template <typename S>
   int step(const BlockArgs& a, cudaStream_t st) {
     const int out = (cur + 1) % 3, zero = (cur + 2) % 3;
-    HB_TRY(block_update<T>(a, buf[cur], buf[out], buf[zero], st));
+    HB_TRY(block_update<S>(a, buf[cur], buf[out], buf[zero], err, st));
     cur = out;
     return HB_OK;
   }
   double* state() const { return buf[cur]; }
 };
 
-template <typename T>
+// T: type of X / Y0 / Z_hat (float or double); S: storage of Z_norm and R
+// (T itself on the plain paths, half / bfloat16 on the tensor-core path).
+template <typename T, typename S>
 int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_index,
              const int64_t* batch_offsets, const double* theta, const T* Y0, void* ws,
              size_t ws_bytes, T* Zhat, hb_outputs* out, cudaStream_t st) {
+  using TA = T;  // split-n partial sums
+  const int64_t launches0 = g_launches;
   const hb_params& p = P->p;
   const int64_t n = p.n_cells;
   const int K = p.n_clusters, B = p.n_batches, d = p.n_pcs;
@@ -244,11 +283,12 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
     HB_CUDA(cudaMemcpyAsync(w.apply_tiles, tiles.data(), sizeof(ApplyTile) * tiles.size(), cudaMemcpyHostToDevice, st));
   for (int i = 0; i < 3; ++i) HB_CUDA(cudaMemsetAsync(w.O[i], 0, sizeof(double) * B * K, st));
   HB_CUDA(cudaMemsetAsync(w.obj_acc, 0, sizeof(double), st));
+  HB_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
 
-  T* Zn = (T*)w.Zn;
-  T* R = (T*)w.R;
-  T* Yn = (T*)w.Yn;
-  ORing ring{{w.O[0], w.O[1], w.O[2]}, 0};
+  S* Zn = (S*)w.Zn;
+  S* R = (S*)w.R;
+  S* Yn = (S*)w.Yn;
+  ORing ring{{w.O[0], w.O[1], w.O[2]}, w.err, 0};
 
   BlockArgs base{};
   base.Zn = Zn; base.ldz = P->ldz; base.R = R; base.ldr = P->ldr; base.cats = cats;
@@ -256,25 +296,54 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
   base.sigma = p.sigma; base.d = d; base.K = K; base.B = B; base.stabilized = p.stabilized_penalty;
 
   // ---- initial state (_harmony/__init__.py:292-353) ------------------------
-  HB_TRY(launch_l2_normalize<T, T>(X, n, d, d, Zn, P->ldz, st));
-  HB_TRY(launch_l2_normalize<T, T>(Y0, K, d, d, Yn, P->ldy, st));
+  HB_TRY(launch_l2_normalize<T, S>(X, n, d, d, Zn, P->ldz, st));
+  HB_TRY(launch_l2_normalize<T, S>(Y0, K, d, d, Yn, P->ldy, st));
   {
     BlockArgs a = base;
     a.idx_new = nullptr; a.new_start = 0; a.n_new = n; a.idx_old = nullptr; a.n_old = 0;
     a.init_mode = 1;
-    HB_TRY(ring.step<T>(a, st));
+    HB_TRY(ring.step<S>(a, st));
   }
+  double* obj_init = w.obj_out + std::max(p.max_iter_clustering, 1);
   HB_TRY(launch_objective_finalize(ring.state(), w.Pr, w.theta, p.sigma, B, K, p.stabilized_penalty,
-                                   w.obj_acc, w.obj_out, st));
+                                   w.obj_acc, obj_init, st));
   double h_obj = 0;
-  HB_CUDA(cudaMemcpyAsync(&h_obj, w.obj_out, sizeof(double), cudaMemcpyDeviceToHost, st));
+  HB_CUDA(cudaMemcpyAsync(&h_obj, obj_init, sizeof(double), cudaMemcpyDeviceToHost, st));
   HB_CUDA(cudaStreamSynchronize(st));
   std::vector<double> objs{h_obj};
   int converged = 0;
   const MembershipLayout& ml = P->ml;
   const int nblk = ml.nblk;
-  std::vector<uint32_t> seeds(kMaxIterChunk);
   std::vector<double> kobj;
+  // With tol_clustering = -inf no iteration can stop early, so the per-iteration
+  // objective read-back (a host sync) is deferred to the end of the clustering call.
+  const bool early_stop = !(std::isinf(p.tol_clustering) && p.tol_clustering < 0);
+
+  // optional device-time profile: event pairs around block-update and centroid launches
+  hb_profile* prof = out ? out->profile : nullptr;
+  struct Span { int cat; int e0, e1; double bytes; };
+  std::vector<Span> spans;
+  size_t next_ev = 0;
+  auto ev = [&]() -> cudaEvent_t {
+    if (next_ev == P->events.size()) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      P->events.push_back(e);
+    }
+    return P->events[next_ev++];
+  };
+  auto span_begin = [&](int cat, double bytes) -> int {
+    if (!prof) return -1;
+    spans.push_back(Span{cat, (int)next_ev, -1, bytes});
+    cudaEventRecord(ev(), st);
+    return (int)spans.size() - 1;
+  };
+  auto span_end = [&](int i) {
+    if (i < 0) return;
+    spans[i].e1 = (int)next_ev;
+    cudaEventRecord(ev(), st);
+  };
+  const double zb = (double)d * P->ssz, rb = (double)K * P->ssz;
 
   for (int outer = 0; outer < p.max_iter_harmony; ++outer) {
     const uint32_t seed = (uint32_t)((p.random_state + (uint64_t)outer * 1000003ull) & 0xffffffffull);
@@ -282,20 +351,24 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
     bool stop = false;
     for (int it0 = 0; it0 < p.max_iter_clustering && !stop; it0 += kMaxIterChunk) {
       const int C = std::min(kMaxIterChunk, p.max_iter_clustering - it0);
-      for (int c = 0; c < C; ++c) seeds[c] = seed + (uint32_t)(it0 + c);
-      HB_TRY(membership_build(ml, w.mb, seeds.data(), C, w.idx, st));
+      HB_TRY(membership_build_dev(ml, w.mb, nullptr, seed + (uint32_t)it0, C, cats, w.idx, st));
       for (int c = 0; c < C && !stop; ++c) {
+        const int it = it0 + c;
         const int32_t* idx = w.idx + (size_t)c * n;
         // centroids Y = R^T Z_norm, L2-normalised (clustering.cu:272-281)
-        HB_TRY(launch_accum<T, T, T>(R, P->ldr, Zn, P->ldz, nullptr, w.cen_chunks, P->cen_chunks, K, d,
-                                     (T*)w.Ypart, st));
-        HB_TRY(launch_centroid_reduce<T, T>((T*)w.Ypart, P->cen_chunks, K, d, Yn, P->ldy, st));
+        int sp = span_begin(1, (double)n * (zb + rb));
+        HB_TRY(launch_accum<S, S, TA>(R, P->ldr, Zn, P->ldz, nullptr, w.cen_chunks, P->cen_chunks, K, d,
+                                      (TA*)w.Ypart, st));
+        HB_TRY(launch_centroid_reduce<TA, S>((TA*)w.Ypart, P->cen_chunks, K, d, Yn, P->ldy, st));
+        span_end(sp);
         // remove block 0's current rows, then sweep the blocks (clustering.cu:308-372)
         {
           BlockArgs a = base;
           a.n_new = 0; a.idx_new = nullptr;
           a.idx_old = idx; a.n_old = std::min<int64_t>(ml.bs, n);
-          HB_TRY(ring.step<T>(a, st));
+          sp = span_begin(0, (double)a.n_old * (rb + 8));
+          HB_TRY(ring.step<S>(a, st));
+          span_end(sp);
         }
         for (int j = 0; j < nblk; ++j) {
           BlockArgs a = base;
@@ -307,27 +380,38 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
             a.idx_old = idx + s1;
             a.n_old = std::min<int64_t>(ml.bs, n - s1);
           }
-          HB_TRY(ring.step<T>(a, st));
+          sp = span_begin(0, (double)a.n_new * (zb + rb + 8) + (double)a.n_old * (rb + 8));
+          HB_TRY(ring.step<S>(a, st));
+          span_end(sp);
         }
         HB_TRY(launch_objective_finalize(ring.state(), w.Pr, w.theta, p.sigma, B, K,
-                                         p.stabilized_penalty, w.obj_acc, w.obj_out, st));
-        HB_CUDA(cudaMemcpyAsync(&h_obj, w.obj_out, sizeof(double), cudaMemcpyDeviceToHost, st));
-        HB_CUDA(cudaStreamSynchronize(st));
-        kobj.push_back(h_obj);
-        // window-3 convergence (clustering.cu:380-387)
-        const size_t m = kobj.size();
-        if (m >= 4) {
-          const double o = kobj[m - 2] + kobj[m - 3] + kobj[m - 4];
-          const double nw = kobj[m - 1] + kobj[m - 2] + kobj[m - 3];
-          if ((o - nw) < p.tol_clustering * std::fabs(o)) stop = true;
+                                         p.stabilized_penalty, w.obj_acc, w.obj_out + it, st));
+        if (early_stop) {
+          HB_CUDA(cudaMemcpyAsync(&h_obj, w.obj_out + it, sizeof(double), cudaMemcpyDeviceToHost, st));
+          HB_CUDA(cudaStreamSynchronize(st));
+          kobj.push_back(h_obj);
+          // window-3 convergence (clustering.cu:380-387)
+          const size_t m = kobj.size();
+          if (m >= 4) {
+            const double o = kobj[m - 2] + kobj[m - 3] + kobj[m - 4];
+            const double nw = kobj[m - 1] + kobj[m - 2] + kobj[m - 3];
+            if ((o - nw) < p.tol_clustering * std::fabs(o)) stop = true;
+          }
         }
       }
     }
+    if (!early_stop && p.max_iter_clustering > 0) {
+      kobj.resize(p.max_iter_clustering);
+      HB_CUDA(cudaMemcpyAsync(kobj.data(), w.obj_out, sizeof(double) * p.max_iter_clustering,
+                              cudaMemcpyDeviceToHost, st));
+    }
     {
-      int err = 0;
-      HB_CUDA(cudaMemcpyAsync(&err, w.mb.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+      int err[2] = {0, 0};
+      HB_CUDA(cudaMemcpyAsync(&err[0], w.mb.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+      HB_CUDA(cudaMemcpyAsync(&err[1], w.err, sizeof(int), cudaMemcpyDeviceToHost, st));
       HB_CUDA(cudaStreamSynchronize(st));
-      if (err) { set_error("block splitter candidate buffer overflow"); return HB_ERR_INTERNAL; }
+      if (err[0]) { set_error("block splitter candidate buffer overflow"); return HB_ERR_INTERNAL; }
+      if (err[1]) { set_error("tensor-core wait timed out (code %d)", err[1]); return HB_ERR_TIMEOUT; }
     }
     if (out && out->kmeans_objectives) {
       for (size_t i = 0; i < kobj.size(); ++i)
@@ -337,14 +421,14 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
     objs.push_back(kobj.empty() ? 0.0 : kobj.back());
 
     // ---- ridge correction (correction_batched.cu:17-130) -------------------
-    HB_TRY(launch_accum<T, T, T>(R, P->ldr, X, d, cell_index, w.m_chunks, (int)mch.size(), K, d,
-                                 (T*)w.Mpart, st));
-    HB_TRY(launch_m_reduce<T>((T*)w.Mpart, mch.data(), (int)mch.size(), w.batch_chunk_off, K, B, d,
-                              w.M, st));
+    HB_TRY(launch_accum<S, T, TA>(R, P->ldr, X, d, cell_index, w.m_chunks, (int)mch.size(), K, d,
+                                  (TA*)w.Mpart, st));
+    HB_TRY(launch_m_reduce<TA>((TA*)w.Mpart, mch.data(), (int)mch.size(), w.batch_chunk_off, K, B, d,
+                               w.M, st));
     CorrArgs ca{w.M, ring.state(), w.Pr, w.Nb, p.alpha, p.ridge_lambda, p.batch_prune_threshold,
                 p.prune, p.dynamic_lambda, K, B, d};
     HB_TRY(launch_ridge_solve<T>(ca, (T*)w.W, st));
-    HB_TRY(launch_apply_t<T, T, T>(X, d, R, P->ldr, (T*)w.W, cell_index, w.apply_tiles,
+    HB_TRY(launch_apply_t<T, S, S>(X, d, R, P->ldr, (T*)w.W, cell_index, w.apply_tiles,
                                    (int)tiles.size(), K, d, Zhat, d, Zn, P->ldz, st));
     // outer convergence (_harmony/__init__.py:722-734)
     const size_t m = objs.size();
@@ -354,6 +438,17 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
     }
   }
   HB_CUDA(cudaStreamSynchronize(st));
+  if (prof) {
+    *prof = hb_profile{};
+    for (const Span& sp : spans) {
+      float ms = 0.f;
+      if (sp.e1 < 0) continue;
+      HB_CUDA(cudaEventElapsedTime(&ms, P->events[sp.e0], P->events[sp.e1]));
+      if (sp.cat == 0) { prof->block_launches++; prof->block_ms += ms; prof->block_bytes += sp.bytes; }
+      else { prof->centroid_launches++; prof->centroid_ms += ms; prof->centroid_bytes += sp.bytes; }
+    }
+    prof->kernel_launches = g_launches - launches0;
+  }
   if (out) {
     if (out->objectives)
       for (size_t i = 0; i < objs.size(); ++i) out->objectives[i] = objs[i];
@@ -375,11 +470,21 @@ int hb_harmonize(hb_plan* plan, const void* X, const int32_t* cats, const int32_
     return HB_ERR_INVALID;
   }
   cudaStream_t st = (cudaStream_t)stream;
-  if (plan->p.precision == HB_FP64)
-    return run_impl<double>(plan, (const double*)X, cats, cell_index, batch_offsets, theta,
-                            (const double*)Y0, workspace, workspace_bytes, (double*)Z_hat, out, st);
-  return run_impl<float>(plan, (const float*)X, cats, cell_index, batch_offsets, theta,
-                         (const float*)Y0, workspace, workspace_bytes, (float*)Z_hat, out, st);
+  switch (plan->p.precision) {
+    case HB_FP64:
+      return run_impl<double, double>(plan, (const double*)X, cats, cell_index, batch_offsets, theta,
+                                      (const double*)Y0, workspace, workspace_bytes, (double*)Z_hat, out, st);
+    case HB_FP16:
+      return run_impl<float, __half>(plan, (const float*)X, cats, cell_index, batch_offsets, theta,
+                                     (const float*)Y0, workspace, workspace_bytes, (float*)Z_hat, out, st);
+    case HB_BF16:
+      return run_impl<float, __nv_bfloat16>(plan, (const float*)X, cats, cell_index, batch_offsets, theta,
+                                            (const float*)Y0, workspace, workspace_bytes, (float*)Z_hat, out,
+                                            st);
+    default:
+      return run_impl<float, float>(plan, (const float*)X, cats, cell_index, batch_offsets, theta,
+                                    (const float*)Y0, workspace, workspace_bytes, (float*)Z_hat, out, st);
+  }
 }
 
 int hb_l2_normalize(const void* src, void* dst, int64_t rows, int32_t cols, int32_t dtype, void* stream) {
@@ -391,29 +496,33 @@ int hb_l2_normalize(const void* src, void* dst, int64_t rows, int32_t cols, int3
   return HB_ERR_INVALID;
 }
 
-size_t hb_block_lists_workspace_bytes(int64_t n, int64_t block_size) {
+size_t hb_block_lists_workspace_bytes(int64_t n, int64_t block_size, int32_t n_batches) {
   if (n < 1 || block_size < 1) return 0;
-  MembershipLayout L = membership_layout(n, block_size);
+  MembershipLayout L = membership_layout(n, block_size, n_batches);
   Carver cv(nullptr, 0);
   MembershipBufs B;
   membership_carve(cv, L, B);
   return cv.off + 256;
 }
 
-int hb_block_lists(int64_t n, int64_t block_size, const uint32_t* seeds, int32_t n_iters, int32_t* idx,
-                   void* workspace, size_t workspace_bytes, void* stream) {
+int hb_block_lists(int64_t n, int64_t block_size, const uint32_t* seeds, int32_t n_iters,
+                   const int32_t* cats, int32_t n_batches, int32_t* idx, void* workspace,
+                   size_t workspace_bytes, void* stream) {
   if (n < 1 || block_size < 1 || !seeds || !idx) { set_error("hb_block_lists: bad argument"); return HB_ERR_INVALID; }
-  MembershipLayout L = membership_layout(n, block_size);
+  MembershipLayout L = membership_layout(n, block_size, cats ? n_batches : 1);
   if (L.nblk > kMaxBlocks) { set_error("too many blocks"); return HB_ERR_UNSUPPORTED; }
   if (L.cap > 16384) { set_error("n too large"); return HB_ERR_UNSUPPORTED; }
-  if (workspace_bytes < hb_block_lists_workspace_bytes(n, block_size)) { set_error("workspace too small"); return HB_ERR_WORKSPACE; }
+  if (workspace_bytes < hb_block_lists_workspace_bytes(n, block_size, cats ? n_batches : 1)) {
+    set_error("workspace too small");
+    return HB_ERR_WORKSPACE;
+  }
   Carver cv((void*)align_up((size_t)workspace, 256), workspace_bytes - 256);
   MembershipBufs B;
   membership_carve(cv, L, B);
   cudaStream_t st = (cudaStream_t)stream;
   for (int c0 = 0; c0 < n_iters; c0 += kMaxIterChunk) {
     const int C = std::min(kMaxIterChunk, n_iters - c0);
-    HB_TRY(membership_build(L, B, seeds + c0, C, idx + (size_t)c0 * n, st));
+    HB_TRY(membership_build(L, B, seeds + c0, C, cats, idx + (size_t)c0 * n, st));
   }
   int err = 0;
   HB_CUDA(cudaMemcpyAsync(&err, B.err, sizeof(int), cudaMemcpyDeviceToHost, st));

@@ -11,6 +11,7 @@ namespace hb {
 struct MembershipLayout {
   int64_t n, bs;
   int nblk, ntiles, cap, max_slots;
+  int nsub;  // batch codes per block bucket (1 = order by cell index only)
 };
 struct MembershipBufs {
   uint32_t* seeds;
@@ -25,15 +26,16 @@ struct MembershipBufs {
   uint32_t* split;
   uint32_t* counts;
   uint32_t* offsets;
+  uint32_t* totals;
   int* err;
 };
-MembershipLayout membership_layout(int64_t n, int64_t bs);
+MembershipLayout membership_layout(int64_t n, int64_t bs, int nsub);
 void membership_carve(Carver& cv, const MembershipLayout& L, MembershipBufs& B);
 int membership_build(const MembershipLayout& L, const MembershipBufs& B, const uint32_t* h_seeds,
-                     int n_iters, int32_t* idx, cudaStream_t st);
-int membership_build_dev(const MembershipLayout& L, const MembershipBufs& B, int n_iters,
-                         int32_t* idx, cudaStream_t st);
-__global__ void k_iota(int32_t* out, int64_t n);
+                     int n_iters, const int32_t* cats, int32_t* idx, cudaStream_t st);
+int membership_build_dev(const MembershipLayout& L, const MembershipBufs& B, const uint32_t* seeds,
+                         uint32_t seed0, int n_iters, const int32_t* cats, int32_t* idx,
+                         cudaStream_t st);
 
 // ---- SIMT kernels of the plain (fp32 / fp64) path ----------------------------
 // Row L2 normalisation, inverse norm clamped to 1e12 (reference semantics).
@@ -87,6 +89,15 @@ int launch_block_update_f64(const BlockArgs& a, const double* O_in, double* O_ou
 int launch_objective_finalize(const double* O, const double* Pr, const double* theta, double sigma,
                               int B, int K, int stabilized, double* obj_acc, double* obj_out,
                               cudaStream_t st);
+
+// ---- tensor-core kernels of the 16-bit path ------------------------------------
+template <typename H>
+int launch_tc_block_update(const BlockArgs& a, const double* O_in, double* O_out, double* O_zero,
+                           int* err, cudaStream_t st);
+template <typename H>
+int launch_tc_similarity(const H* Zn, int ldz, const H* Yn, int ldy, const int32_t* idx,
+                         const int32_t* cats, int64_t n, int d, int K, float* S, int* err,
+                         cudaStream_t st);
 
 struct CorrArgs {
   const double* M;      // [K][B+1][d]

@@ -15,13 +15,18 @@
 
 namespace hb {
 
+// seed of iteration c of the chunk: an explicit list, or consecutive from seed0
+__device__ __forceinline__ uint32_t seed_of(const uint32_t* seeds, uint32_t seed0, int c) {
+  return seeds ? seeds[c] : seed0 + (uint32_t)c;
+}
+
 // ---------------------------------------------------------------------------
 // 1) 12-bit key histogram, one per iteration.
 __global__ void k_key_hist(int64_t n, const uint32_t* __restrict__ seeds,
-                           uint32_t* __restrict__ hist) {
+                           uint32_t seed0, uint32_t* __restrict__ hist) {
   __shared__ uint32_t sh[kNumBins];
   const int c = blockIdx.y;
-  const uint32_t seed = seeds[c];
+  const uint32_t seed = seed_of(seeds, seed0, c);
   for (int b = threadIdx.x; b < kNumBins; b += blockDim.x) sh[b] = 0;
   __syncthreads();
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -104,14 +109,14 @@ __global__ void k_boundary_bins(int64_t bs, int nb, const uint32_t* __restrict__
 }
 
 // 3) Collect the keys that fall in a boundary bin.
-__global__ void k_collect_candidates(int64_t n, const uint32_t* __restrict__ seeds,
+__global__ void k_collect_candidates(int64_t n, const uint32_t* __restrict__ seeds, uint32_t seed0,
                                      const int16_t* __restrict__ lut,
                                      uint32_t* __restrict__ cand_cnt,
                                      uint32_t* __restrict__ cand, int max_slots, int cap,
                                      int* __restrict__ err) {
   __shared__ int16_t sl[kNumBins];
   const int c = blockIdx.y;
-  const uint32_t seed = seeds[c];
+  const uint32_t seed = seed_of(seeds, seed0, c);
   for (int b = threadIdx.x; b < kNumBins; b += blockDim.x) sl[b] = lut[(size_t)c * kNumBins + b];
   __syncthreads();
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -176,40 +181,46 @@ __device__ __forceinline__ int block_of(uint32_t key, const uint32_t* sp, int nb
   return lo;
 }
 
-// 5) Per-tile block counts.
-__global__ void k_part_count(int64_t n, int nblk, const uint32_t* __restrict__ seeds,
-                             const uint32_t* __restrict__ split, uint32_t* __restrict__ counts,
-                             int ntiles) {
+// 5) Per-tile bucket counts.  A bucket is (block, batch): within a block the
+//    cells are ordered by batch code, then by cell index, so every tile of a
+//    block holds long runs of one batch (used by the O accumulation).
+__global__ void k_part_count(int64_t n, int nblk, int nsub, const int32_t* __restrict__ cats,
+                             const uint32_t* __restrict__ seeds, uint32_t seed0,
+                             const uint32_t* __restrict__ split, uint32_t* __restrict__ counts, int ntiles) {
+  extern __shared__ uint32_t cnt[];   // [nblk * nsub]
   __shared__ uint32_t sp[kMaxBlocks];
-  __shared__ uint32_t cnt[kMaxBlocks];
   const int c = blockIdx.y, tile = blockIdx.x;
-  const uint32_t seed = seeds[c];
-  const int nb = nblk - 1;
+  const uint32_t seed = seed_of(seeds, seed0, c);
+  const int nb = nblk - 1, nbk = nblk * nsub;
   for (int j = threadIdx.x; j < nb; j += blockDim.x) sp[j] = split[(size_t)c * kMaxBlocks + j];
-  for (int j = threadIdx.x; j < nblk; j += blockDim.x) cnt[j] = 0;
+  for (int j = threadIdx.x; j < nbk; j += blockDim.x) cnt[j] = 0;
   __syncthreads();
   const int64_t base = (int64_t)tile * kPartTile;
   for (int q = threadIdx.x; q < kPartTile; q += blockDim.x) {
     int64_t i = base + q;
-    if (i < n) atomicAdd(&cnt[block_of(pcg_key((uint32_t)i, seed), sp, nb)], 1u);
+    if (i < n) {
+      const int bucket = block_of(pcg_key((uint32_t)i, seed), sp, nb) * nsub + (cats ? cats[i] : 0);
+      atomicAdd(&cnt[bucket], 1u);
+    }
   }
   __syncthreads();
-  uint32_t* out = counts + ((size_t)c * ntiles + tile) * nblk;
-  for (int j = threadIdx.x; j < nblk; j += blockDim.x) out[j] = cnt[j];
+  uint32_t* out = counts + ((size_t)c * ntiles + tile) * nbk;
+  for (int j = threadIdx.x; j < nbk; j += blockDim.x) out[j] = cnt[j];
 }
 
-// 6) Column scan over tiles: offsets[tile][blk] = blk*bs + sum_{t'<tile} counts[t'][blk].
-__global__ void k_part_scan(int64_t bs, int nblk, int ntiles, const uint32_t* __restrict__ counts,
-                            uint32_t* __restrict__ offsets) {
+// 6) Column scan over tiles: offsets[tile][bucket] = sum_{t'<tile} counts[t'][bucket];
+//    totals[bucket] = the column total.
+__global__ void k_part_scan(int nbk, int ntiles, const uint32_t* __restrict__ counts,
+                            uint32_t* __restrict__ offsets, uint32_t* __restrict__ totals) {
   __shared__ uint32_t wsum[32];
   __shared__ uint32_t carry_s;
-  const int blk = blockIdx.x, c = blockIdx.y;
+  const int bk = blockIdx.x, c = blockIdx.y;
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-  if (t == 0) carry_s = (uint32_t)((int64_t)blk * bs);
+  if (t == 0) carry_s = 0;
   __syncthreads();
   for (int t0 = 0; t0 < ntiles; t0 += blockDim.x) {
     const int tile = t0 + t;
-    const size_t at = ((size_t)c * ntiles + tile) * nblk + blk;
+    const size_t at = ((size_t)c * ntiles + tile) * nbk + bk;
     uint32_t v = (tile < ntiles) ? counts[at] : 0u;
     uint32_t incl = v;
 #pragma unroll
@@ -236,49 +247,64 @@ __global__ void k_part_scan(int64_t bs, int nblk, int ntiles, const uint32_t* __
     if (t == blockDim.x - 1) carry_s = carry + wsum[w] + incl;
     __syncthreads();
   }
+  if (t == 0) totals[(size_t)c * nbk + bk] = carry_s;
 }
 
-// 7) Stable scatter: cell i lands at offsets[tile][blk] + (rank of i among the
-//    tile's cells of the same block, in ascending cell order).
-__global__ void __launch_bounds__(256) k_part_scatter(int64_t n, int nblk,
-                                                      const uint32_t* __restrict__ seeds,
+// 7) Stable scatter: cell i lands at base(bucket) + offsets[tile][bucket] + (rank
+//    of i among the tile's cells of the same bucket, ascending), where base =
+//    blk*bs + cells of lower batches in the same block.
+__global__ void __launch_bounds__(256) k_part_scatter(int64_t n, int64_t bs, int nblk, int nsub,
+                                                      const int32_t* __restrict__ cats,
+                                                      const uint32_t* __restrict__ seeds, uint32_t seed0,
                                                       const uint32_t* __restrict__ split,
                                                       const uint32_t* __restrict__ offsets,
+                                                      const uint32_t* __restrict__ totals,
                                                       int ntiles, int32_t* __restrict__ idx) {
+  extern __shared__ uint32_t dyn[];
+  const int nbk = nblk * nsub;
+  uint32_t* base = dyn;               // [nbk]
+  uint32_t* wc = dyn + nbk;           // [8][nbk]
   __shared__ uint32_t sp[kMaxBlocks];
-  __shared__ uint32_t base[kMaxBlocks];
-  __shared__ uint32_t wc[8][kMaxBlocks];
   const int c = blockIdx.y, tile = blockIdx.x;
-  const uint32_t seed = seeds[c];
+  const uint32_t seed = seed_of(seeds, seed0, c);
   const int nb = nblk - 1;
-  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  const int t = threadIdx.x, w = t >> 5;
   for (int j = t; j < nb; j += 256) sp[j] = split[(size_t)c * kMaxBlocks + j];
-  const uint32_t* off = offsets + ((size_t)c * ntiles + tile) * nblk;
-  for (int j = t; j < nblk; j += 256) base[j] = off[j];
-  for (int j = t; j < 8 * kMaxBlocks; j += 256) (&wc[0][0])[j] = 0;
+  const uint32_t* off = offsets + ((size_t)c * ntiles + tile) * nbk;
+  const uint32_t* tot = totals + (size_t)c * nbk;
+  for (int blk = t; blk < nblk; blk += 256) {
+    uint32_t run = (uint32_t)((int64_t)blk * bs);
+    for (int q = 0; q < nsub; ++q) {
+      const int bk = blk * nsub + q;
+      base[bk] = run + off[bk];
+      run += tot[bk];
+    }
+  }
+  for (int j = t; j < 8 * nbk; j += 256) wc[j] = 0;
   __syncthreads();
   int32_t* out = idx + (size_t)c * n;
   const int64_t tbase = (int64_t)tile * kPartTile;
   for (int r = 0; r < kPartTile / 256; ++r) {
     const int64_t i = tbase + r * 256 + t;
     const bool valid = i < n;
-    const int blk = valid ? block_of(pcg_key((uint32_t)i, seed), sp, nb) : nblk;
-    const unsigned peers = __match_any_sync(0xffffffffu, blk);
+    const int bk = valid ? block_of(pcg_key((uint32_t)i, seed), sp, nb) * nsub + (cats ? cats[i] : 0)
+                         : nbk;
+    const unsigned peers = __match_any_sync(0xffffffffu, bk);
     const unsigned lrank = __popc(peers & lanemask_lt());
-    if (valid && lrank == 0) wc[w][blk] = __popc(peers);
+    if (valid && lrank == 0) wc[w * nbk + bk] = __popc(peers);
     __syncthreads();
-    for (int j = t; j < nblk; j += 256) {
+    for (int j = t; j < nbk; j += 256) {
       uint32_t run = base[j];
 #pragma unroll
-      for (int q = 0; q < 8; ++q) { uint32_t x = wc[q][j]; wc[q][j] = run; run += x; }
+      for (int q = 0; q < 8; ++q) { uint32_t x = wc[q * nbk + j]; wc[q * nbk + j] = run; run += x; }
       base[j] = run;
     }
     __syncthreads();
-    if (valid) out[wc[w][blk] + lrank] = (int32_t)i;
+    if (valid) out[wc[w * nbk + bk] + lrank] = (int32_t)i;
     __syncthreads();
-    for (int j = t; j < nblk; j += 256) {
+    for (int j = t; j < nbk; j += 256) {
 #pragma unroll
-      for (int q = 0; q < 8; ++q) wc[q][j] = 0;
+      for (int q = 0; q < 8; ++q) wc[q * nbk + j] = 0;
     }
     __syncthreads();
   }
@@ -286,10 +312,11 @@ __global__ void __launch_bounds__(256) k_part_scatter(int64_t n, int nblk,
 
 // ---------------------------------------------------------------------------
 
-MembershipLayout membership_layout(int64_t n, int64_t bs) {
+MembershipLayout membership_layout(int64_t n, int64_t bs, int nsub) {
   MembershipLayout L{};
   L.n = n;
   L.bs = bs;
+  L.nsub = nsub < 1 ? 1 : nsub;
   L.nblk = (int)((n + bs - 1) / bs);
   L.ntiles = div_up(n, kPartTile);
   const double mu = (double)n / kNumBins;
@@ -298,6 +325,7 @@ MembershipLayout membership_layout(int64_t n, int64_t bs) {
   while (p < cap) p <<= 1;
   L.cap = p;
   L.max_slots = L.nblk > 1 ? L.nblk - 1 : 1;
+  if ((int64_t)L.nblk * L.nsub > kMaxBuckets) L.nsub = 1;  // too many (block, batch) buckets
   return L;
 }
 
@@ -313,45 +341,44 @@ void membership_carve(Carver& cv, const MembershipLayout& L, MembershipBufs& B) 
   B.cand_cnt = cv.take<uint32_t>((size_t)C * L.max_slots);
   B.cand = cv.take<uint32_t>((size_t)C * L.max_slots * L.cap);
   B.split = cv.take<uint32_t>((size_t)C * kMaxBlocks);
-  B.counts = cv.take<uint32_t>((size_t)C * L.ntiles * L.nblk);
-  B.offsets = cv.take<uint32_t>((size_t)C * L.ntiles * L.nblk);
+  B.counts = cv.take<uint32_t>((size_t)C * L.ntiles * L.nblk * L.nsub);
+  B.offsets = cv.take<uint32_t>((size_t)C * L.ntiles * L.nblk * L.nsub);
+  B.totals = cv.take<uint32_t>((size_t)C * L.nblk * L.nsub);
   B.err = cv.take<int>(4);
 }
 
 // Writes, for each of `n_iters` (<= kMaxIterChunk) seeds, the cell list of every
 // block: idx[c*n + j*bs + r] is the r-th cell (ascending) of block j.
 int membership_build(const MembershipLayout& L, const MembershipBufs& B, const uint32_t* h_seeds,
-                     int n_iters, int32_t* idx, cudaStream_t st) {
+                     int n_iters, const int32_t* cats, int32_t* idx, cudaStream_t st) {
   if (n_iters < 1 || n_iters > kMaxIterChunk) {
     set_error("membership_build: n_iters out of range");
     return HB_ERR_INVALID;
   }
   HB_CUDA(cudaMemcpyAsync(B.seeds, h_seeds, sizeof(uint32_t) * n_iters, cudaMemcpyHostToDevice, st));
-  return membership_build_dev(L, B, n_iters, idx, st);
+  return membership_build_dev(L, B, B.seeds, 0, n_iters, cats, idx, st);
 }
 
-int membership_build_dev(const MembershipLayout& L, const MembershipBufs& B, int n_iters,
-                         int32_t* idx, cudaStream_t st) {
+// Block lists for the consecutive seeds seed0 .. seed0+n_iters-1 (no host copy),
+// or for the device list `seeds` when it is not null.
+int membership_build_dev(const MembershipLayout& L, const MembershipBufs& B, const uint32_t* seeds,
+                         uint32_t seed0, int n_iters, const int32_t* cats, int32_t* idx,
+                         cudaStream_t st) {
   const int nb = L.nblk - 1;
   const int sms = num_sms();
-  if (nb == 0) {
-    // a single block: cells in order
-    for (int c = 0; c < n_iters; ++c) {
-      k_iota<<<div_up(L.n, 256) < 4 * sms ? div_up(L.n, 256) : 4 * sms, 256, 0, st>>>(idx + (size_t)c * L.n, L.n);
-      HB_LAUNCH_CHECK();
-    }
-    return HB_OK;
-  }
+  const int nsub = cats ? L.nsub : 1;
+  const int nbk = L.nblk * nsub;
   HB_CUDA(cudaMemsetAsync(B.hist, 0, sizeof(uint32_t) * (size_t)n_iters * kNumBins, st));
   HB_CUDA(cudaMemsetAsync(B.err, 0, sizeof(int), st));
   int g = std::min(div_up(L.n, 256 * 8), 2 * sms);
   if (g < 1) g = 1;
-  k_key_hist<<<dim3(g, n_iters), 256, 0, st>>>(L.n, B.seeds, B.hist);
+  if (nb > 0) {
+  k_key_hist<<<dim3(g, n_iters), 256, 0, st>>>(L.n, seeds, seed0, B.hist);
   HB_LAUNCH_CHECK();
   k_boundary_bins<<<n_iters, 1024, 0, st>>>(L.bs, nb, B.hist, B.bnd_slot, B.bnd_q, B.slot_bin,
                                             B.nslots, B.lut, B.cand_cnt, L.max_slots);
   HB_LAUNCH_CHECK();
-  k_collect_candidates<<<dim3(g, n_iters), 256, 0, st>>>(L.n, B.seeds, B.lut, B.cand_cnt, B.cand,
+  k_collect_candidates<<<dim3(g, n_iters), 256, 0, st>>>(L.n, seeds, seed0, B.lut, B.cand_cnt, B.cand,
                                                          L.max_slots, L.cap, B.err);
   HB_LAUNCH_CHECK();
   const size_t smem = sizeof(uint32_t) * (size_t)L.cap;
@@ -360,20 +387,22 @@ int membership_build_dev(const MembershipLayout& L, const MembershipBufs& B, int
   k_select_splitters<<<dim3(L.max_slots, n_iters), 512, smem, st>>>(
       nb, L.cap, B.nslots, B.cand_cnt, B.cand, B.bnd_slot, B.bnd_q, B.split, L.max_slots, L.cap);
   HB_LAUNCH_CHECK();
-  k_part_count<<<dim3(L.ntiles, n_iters), 256, 0, st>>>(L.n, L.nblk, B.seeds, B.split, B.counts, L.ntiles);
+  }
+  if (sizeof(uint32_t) * nbk > 48 * 1024)
+    HB_CUDA(cudaFuncSetAttribute(k_part_count, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(sizeof(uint32_t) * nbk)));
+  k_part_count<<<dim3(L.ntiles, n_iters), 256, sizeof(uint32_t) * nbk, st>>>(
+      L.n, L.nblk, nsub, cats, seeds, seed0, B.split, B.counts, L.ntiles);
   HB_LAUNCH_CHECK();
-  k_part_scan<<<dim3(L.nblk, n_iters), 1024, 0, st>>>(L.bs, L.nblk, L.ntiles, B.counts, B.offsets);
+  k_part_scan<<<dim3(nbk, n_iters), 1024, 0, st>>>(nbk, L.ntiles, B.counts, B.offsets, B.totals);
   HB_LAUNCH_CHECK();
-  k_part_scatter<<<dim3(L.ntiles, n_iters), 256, 0, st>>>(L.n, L.nblk, B.seeds, B.split, B.offsets,
-                                                         L.ntiles, idx);
+  const size_t ssm = sizeof(uint32_t) * 9 * (size_t)nbk;
+  if (ssm > 48 * 1024)
+    HB_CUDA(cudaFuncSetAttribute(k_part_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm));
+  k_part_scatter<<<dim3(L.ntiles, n_iters), 256, ssm, st>>>(L.n, L.bs, L.nblk, nsub, cats, seeds, seed0,
+                                                           B.split, B.offsets, B.totals, L.ntiles, idx);
   HB_LAUNCH_CHECK();
   return HB_OK;
-}
-
-__global__ void k_iota(int32_t* out, int64_t n) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x)
-    out[i] = (int32_t)i;
 }
 
 }  // namespace hb

@@ -63,10 +63,11 @@ __global__ void __launch_bounds__(256) k_accum(const TS* __restrict__ W, int ldw
                                                const int32_t* __restrict__ cell_index,
                                                const AccumChunk* __restrict__ chunks, int K,
                                                int d, int ktiles, TA* __restrict__ P) {
-  constexpr int ACC_ROWS = sizeof(TA) == 8 ? 16 : 32;
-  __shared__ TA ws[ACC_ROWS][ACC_BK];
-  __shared__ TA vs[ACC_ROWS][ACC_BD];
-  __shared__ int64_t cid[ACC_ROWS];
+  constexpr int ROWS = sizeof(TA) == 8 ? 16 : 32;
+  constexpr int NW = ROWS * ACC_BK / 256;  // W elements per thread per step
+  constexpr int NV = ROWS * ACC_BD / 256;  // V elements per thread per step
+  __shared__ TA ws[ROWS][ACC_BK];
+  __shared__ TA vs[ROWS][ACC_BD];
   const AccumChunk ch = chunks[blockIdx.x];
   const int kt = blockIdx.y % ktiles, dt = blockIdx.y / ktiles;
   const int k0 = kt * ACC_BK, d0 = dt * ACC_BD;
@@ -77,27 +78,42 @@ __global__ void __launch_bounds__(256) k_accum(const TS* __restrict__ W, int ldw
 #pragma unroll
     for (int b = 0; b < 4; ++b) acc[a][b] = TA(0);
 
-  for (int pos = 0; pos < ch.len; pos += ACC_ROWS) {
-    const int nrow = min(ACC_ROWS, ch.len - pos);
-    __syncthreads();
-    if (tid < ACC_ROWS) {
-      int64_t q = ch.start + pos + tid;
-      cid[tid] = (tid < nrow) ? (cell_index ? (int64_t)cell_index[q] : q) : -1;
+  TA rw[NW], rv[NV];
+  auto load = [&](int pos) {
+#pragma unroll
+    for (int q = 0; q < NW; ++q) {
+      const int e = tid + q * 256, r = e / ACC_BK, kk = e % ACC_BK;
+      TA v = TA(0);
+      if (pos + r < ch.len && k0 + kk < K) {
+        const int64_t qq = ch.start + pos + r;
+        const int64_t cell = cell_index ? (int64_t)__ldg(cell_index + qq) : qq;
+        v = (TA)to_f(W[cell * ldw + k0 + kk]);
+      }
+      rw[q] = v;
     }
-    __syncthreads();
-    for (int e = tid; e < ACC_ROWS * ACC_BK; e += 256) {
-      const int r = e / ACC_BK, kk = e % ACC_BK;
-      const int64_t cell = cid[r];
-      ws[r][kk] = (cell >= 0 && k0 + kk < K) ? (TA)to_f(W[cell * ldw + k0 + kk]) : TA(0);
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+      const int e = tid + q * 256, r = e / ACC_BD, cc = e % ACC_BD;
+      TA v = TA(0);
+      if (pos + r < ch.len && d0 + cc < d) {
+        const int64_t qq = ch.start + pos + r;
+        const int64_t cell = cell_index ? (int64_t)__ldg(cell_index + qq) : qq;
+        v = (TA)to_f(V[cell * ldv + d0 + cc]);
+      }
+      rv[q] = v;
     }
-    for (int e = tid; e < ACC_ROWS * ACC_BD; e += 256) {
-      const int r = e / ACC_BD, cc = e % ACC_BD;
-      const int64_t cell = cid[r];
-      vs[r][cc] = (cell >= 0 && d0 + cc < d) ? (TA)to_f(V[cell * ldv + d0 + cc]) : TA(0);
-    }
+  };
+  load(0);
+  for (int pos = 0; pos < ch.len; pos += ROWS) {
     __syncthreads();
+#pragma unroll
+    for (int q = 0; q < NW; ++q) { const int e = tid + q * 256; ws[e / ACC_BK][e % ACC_BK] = rw[q]; }
+#pragma unroll
+    for (int q = 0; q < NV; ++q) { const int e = tid + q * 256; vs[e / ACC_BD][e % ACC_BD] = rv[q]; }
+    __syncthreads();
+    if (pos + ROWS < ch.len) load(pos + ROWS);  // next step's loads overlap this step's math
 #pragma unroll 4
-    for (int r = 0; r < ACC_ROWS; ++r) {
+    for (int r = 0; r < ROWS; ++r) {
       TA wv[8], vv[4];
 #pragma unroll
       for (int a = 0; a < 8; ++a) wv[a] = ws[r][tk * 8 + a];
@@ -149,30 +165,53 @@ template int launch_accum<__nv_bfloat16, __nv_bfloat16, float>(const __nv_bfloat
                                                                cudaStream_t);
 
 // Y_norm[k] = l2normalise(sum over chunks of P[chunk][k]) -- fixed summation
-// order (deterministic), float64 accumulation.
+// order (deterministic), float64 accumulation.  One CTA per centroid row; 8
+// warps split the chunks, lanes split the PCs.
+constexpr int RED_Y = 8;
+
+template <typename TA>
+__device__ __forceinline__ void reduce_rows_into(const TA* __restrict__ P, int q0, int q1,
+                                                 size_t stride, size_t off, int d,
+                                                 double* __restrict__ part, double* __restrict__ out) {
+  // part: [RED_Y][d] scratch, out: [d]
+  for (int c = threadIdx.x; c < d; c += 32) {
+    double s = 0;
+    for (int q = q0 + (int)threadIdx.y; q < q1; q += RED_Y) s += (double)P[(size_t)q * stride + off + c];
+    part[threadIdx.y * d + c] = s;
+  }
+  __syncthreads();
+  const int t = threadIdx.y * 32 + threadIdx.x;
+  for (int c = t; c < d; c += 32 * RED_Y) {
+    double s = 0;
+#pragma unroll
+    for (int y = 0; y < RED_Y; ++y) s += part[y * d + c];
+    out[c] = s;
+  }
+  __syncthreads();
+}
+
 template <typename TA, typename TY>
 __global__ void k_centroid_reduce(const TA* __restrict__ P, int n_chunks, int K, int d,
                                   TY* __restrict__ Yn, int ldy) {
-  extern __shared__ double ys[];
+  extern __shared__ double sm[];
+  double* part = sm;              // [RED_Y][d]
+  double* ys = sm + RED_Y * d;    // [d]
   __shared__ double red[32];
   const int k = blockIdx.x;
+  reduce_rows_into(P, 0, n_chunks, (size_t)K * d, (size_t)k * d, d, part, ys);
+  const int t = threadIdx.y * 32 + threadIdx.x;
   double ss = 0;
-  for (int c = threadIdx.x; c < d; c += blockDim.x) {
-    double s = 0;
-    for (int q = 0; q < n_chunks; ++q) s += (double)P[((size_t)q * K + k) * d + c];
-    ys[c] = s;
-    ss += s * s;
-  }
+  for (int c = t; c < d; c += 32 * RED_Y) ss += ys[c] * ys[c];
   ss = block_sum(ss, red);
   double inv = rsqrt(ss);
   if (inv > 1e12) inv = 1e12;
-  for (int c = threadIdx.x; c < ldy; c += blockDim.x)
+  for (int c = t; c < ldy; c += 32 * RED_Y)
     Yn[(size_t)k * ldy + c] = (c < d) ? from_f<TY>((compute_t<TY>)(ys[c] * inv)) : from_f<TY>(compute_t<TY>(0));
 }
 
 template <typename TA, typename TY>
 int launch_centroid_reduce(const TA* P, int n_chunks, int K, int d, TY* Yn, int ldy, cudaStream_t st) {
-  k_centroid_reduce<TA, TY><<<K, 128, sizeof(double) * d, st>>>(P, n_chunks, K, d, Yn, ldy);
+  k_centroid_reduce<TA, TY><<<K, dim3(32, RED_Y), sizeof(double) * (RED_Y + 1) * d, st>>>(P, n_chunks, K, d, Yn, ldy);
   HB_LAUNCH_CHECK();
   return HB_OK;
 }
@@ -200,7 +239,8 @@ template int launch_centroid_reduce<float, __nv_bfloat16>(const float*, int, int
 // O_in + delta into O_out (zeroed beforehand), and zeroes O_zero (the buffer
 // the previous launch read), so no CTA ever reads a buffer another CTA of the
 // same launch is writing.
-constexpr int BU_TM = 64, BU_DC = 16, BU_THREADS = 256;
+constexpr int BU_TM = 64, BU_THREADS = 256;
+template <typename T> constexpr int bu_dc() { return sizeof(T) == 8 ? 16 : 32; }
 
 struct BlockArgsDev {
   BlockArgs a;
@@ -211,15 +251,18 @@ struct BlockArgsDev {
 
 template <typename T, int KPT>
 __global__ void __launch_bounds__(BU_THREADS) k_block_update(BlockArgsDev p) {
+  constexpr int DC = bu_dc<T>();
+  constexpr int K16 = 16 * KPT;
+  constexpr int NZ = BU_TM * DC / BU_THREADS;   // Z elements per thread per chunk
+  constexpr int NY = K16 * DC / BU_THREADS;     // Y elements per thread per chunk
   const BlockArgs& a = p.a;
   const int K = a.K, B = a.B, d = a.d;
-  const int K16 = 16 * KPT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* pen = (T*)smem_raw;                       // [B][K]
   T* osm = pen + (size_t)B * K;                // [B][K]
   T* zt = osm + (size_t)B * K;                 // [TM][DC+1]
-  T* yt = zt + BU_TM * (BU_DC + 1);            // [K16][DC+1]
-  int64_t* cid = (int64_t*)(yt + (size_t)K16 * (BU_DC + 1));  // [TM]
+  T* yt = zt + BU_TM * (DC + 1);               // [K16][DC+1]
+  int64_t* cid = (int64_t*)(yt + (size_t)K16 * (DC + 1));  // [TM]
   int* ccat = (int*)(cid + BU_TM);             // [TM]
   __shared__ double red[32];
 
@@ -234,7 +277,7 @@ __global__ void __launch_bounds__(BU_THREADS) k_block_update(BlockArgsDev p) {
 
   // penalty table from the current state (kernels_pen.cuh:8-21)
   if (a.n_new > 0 && !a.init_mode) {
-    double* ocol = (double*)zt;  // scratch (K doubles fit in zt+yt)
+    double* ocol = (double*)zt;  // scratch: K doubles fit in zt + yt
     for (int k = tid; k < K; k += BU_THREADS) {
       double s = 0;
       for (int b = 0; b < B; ++b) s += p.O_in[(size_t)b * K + k];
@@ -255,9 +298,25 @@ __global__ void __launch_bounds__(BU_THREADS) k_block_update(BlockArgsDev p) {
   const T term = T(-2) / (T)a.sigma;
   const T sig = (T)a.sigma;
   double obj_local = 0.0;
+  const int nchunk = (d + DC - 1) / DC;
   const int64_t ntiles_new = (a.n_new + BU_TM - 1) / BU_TM;
+  T rz[NZ], ry[NY];
+  auto load_chunk = [&](int d0) {
+#pragma unroll
+    for (int q = 0; q < NZ; ++q) {
+      const int e = tid + q * BU_THREADS, r = e / DC, c = e % DC;
+      const int64_t cell = cid[r];
+      rz[q] = (cell >= 0 && d0 + c < d) ? Zn[cell * a.ldz + d0 + c] : T(0);
+    }
+#pragma unroll
+    for (int q = 0; q < NY; ++q) {
+      const int e = tid + q * BU_THREADS, k = e / DC, c = e % DC;
+      ry[q] = (k < K && d0 + c < d) ? Yn[(size_t)k * a.ldy + d0 + c] : T(0);
+    }
+  };
   for (int64_t tile = blockIdx.x; tile < ntiles_new; tile += gridDim.x) {
     const int64_t r0 = tile * BU_TM;
+    __syncthreads();
     if (tid < BU_TM) {
       const int64_t q = r0 + tid;
       int64_t cell = -1;
@@ -265,30 +324,28 @@ __global__ void __launch_bounds__(BU_THREADS) k_block_update(BlockArgsDev p) {
       cid[tid] = cell;
       ccat[tid] = cell >= 0 ? a.cats[cell] : 0;
     }
+    __syncthreads();
+    load_chunk(0);
     T s[4][KPT];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
       for (int j = 0; j < KPT; ++j) s[i][j] = T(0);
-    for (int d0 = 0; d0 < d; d0 += BU_DC) {
+    for (int ck = 0; ck < nchunk; ++ck) {
       __syncthreads();
-      for (int e = tid; e < BU_TM * BU_DC; e += BU_THREADS) {
-        const int r = e / BU_DC, c = e % BU_DC;
-        const int64_t cell = cid[r];
-        zt[r * (BU_DC + 1) + c] = (cell >= 0 && d0 + c < d) ? Zn[cell * a.ldz + d0 + c] : T(0);
-      }
-      for (int e = tid; e < K16 * BU_DC; e += BU_THREADS) {
-        const int k = e / BU_DC, c = e % BU_DC;
-        yt[k * (BU_DC + 1) + c] = (k < K && d0 + c < d) ? Yn[(size_t)k * a.ldy + d0 + c] : T(0);
-      }
+#pragma unroll
+      for (int q = 0; q < NZ; ++q) { const int e = tid + q * BU_THREADS; zt[(e / DC) * (DC + 1) + e % DC] = rz[q]; }
+#pragma unroll
+      for (int q = 0; q < NY; ++q) { const int e = tid + q * BU_THREADS; yt[(e / DC) * (DC + 1) + e % DC] = ry[q]; }
       __syncthreads();
+      if (ck + 1 < nchunk) load_chunk((ck + 1) * DC);
 #pragma unroll 4
-      for (int c = 0; c < BU_DC; ++c) {
+      for (int c = 0; c < DC; ++c) {
         T z[4], y[KPT];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) z[i] = zt[(cg * 4 + i) * (BU_DC + 1) + c];
+        for (int i = 0; i < 4; ++i) z[i] = zt[(cg * 4 + i) * (DC + 1) + c];
 #pragma unroll
-        for (int j = 0; j < KPT; ++j) y[j] = yt[(kg + 16 * j) * (BU_DC + 1) + c];
+        for (int j = 0; j < KPT; ++j) y[j] = yt[(kg + 16 * j) * (DC + 1) + c];
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -364,15 +421,33 @@ __global__ void __launch_bounds__(BU_THREADS) k_block_update(BlockArgsDev p) {
     }
   }
 
-  // remove the current rows of the next block's cells
+  // remove the current rows of the next block's cells (two rows per warp step,
+  // all loads issued before the shared-memory atomics)
   {
+    constexpr int KL = (K16 + 31) / 32;
     const int lane = tid & 31, w = tid >> 5;
-    for (int64_t q = (int64_t)blockIdx.x * (BU_THREADS / 32) + w; q < a.n_old;
-         q += (int64_t)gridDim.x * (BU_THREADS / 32)) {
-      const int64_t cell = a.idx_old[q];
-      const int cat = a.cats[cell];
-      const T* Rrow = R + cell * a.ldr;
-      for (int k = lane; k < K; k += 32) atomicAdd(&osm[cat * K + k], -Rrow[k]);
+    const int64_t nw = (int64_t)gridDim.x * (BU_THREADS / 32);
+    for (int64_t q = (int64_t)blockIdx.x * (BU_THREADS / 32) + w; q < a.n_old; q += 2 * nw) {
+      const int64_t q2 = q + nw;
+      const int64_t c1 = a.idx_old[q];
+      const int64_t c2 = q2 < a.n_old ? (int64_t)a.idx_old[q2] : -1;
+      const int cat1 = a.cats[c1];
+      const int cat2 = c2 >= 0 ? a.cats[c2] : 0;
+      T v1[KL], v2[KL];
+#pragma unroll
+      for (int u = 0; u < KL; ++u) {
+        const int k = lane + 32 * u;
+        v1[u] = k < K ? R[c1 * a.ldr + k] : T(0);
+        v2[u] = (k < K && c2 >= 0) ? R[c2 * a.ldr + k] : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < KL; ++u) {
+        const int k = lane + 32 * u;
+        if (k < K) {
+          atomicAdd(&osm[cat1 * K + k], -v1[u]);
+          if (c2 >= 0) atomicAdd(&osm[cat2 * K + k], -v2[u]);
+        }
+      }
     }
   }
   __syncthreads();
@@ -388,8 +463,9 @@ __global__ void __launch_bounds__(BU_THREADS) k_block_update(BlockArgsDev p) {
 template <typename T, int KPT>
 static int launch_block_kpt(const BlockArgsDev& p, cudaStream_t st) {
   const BlockArgs& a = p.a;
-  const size_t smem = sizeof(T) * ((size_t)2 * a.B * a.K + BU_TM * (BU_DC + 1) +
-                                    (size_t)16 * KPT * (BU_DC + 1)) +
+  constexpr int DC = bu_dc<T>();
+  const size_t smem = sizeof(T) * ((size_t)2 * a.B * a.K + BU_TM * (DC + 1) +
+                                    (size_t)16 * KPT * (DC + 1)) +
                       BU_TM * (sizeof(int64_t) + sizeof(int)) + 64;
   if (smem > 227 * 1024) {
     set_error("block update: B*K too large for shared memory (B=%d K=%d)", a.B, a.K);
@@ -464,31 +540,33 @@ int launch_objective_finalize(const double* O, const double* Pr, const double* t
 
 // ---------------------------------------------------------------------------
 // Ridge moments: M[k][b+1][c] = sum over batch-b chunks of P, M[k][0] = sum_b.
-__global__ void k_m_reduce(const float* __restrict__ Pf, const double* __restrict__ Pd,
-                           const int32_t* __restrict__ batch_chunk_off, int K, int B, int d,
-                           double* __restrict__ M) {
+template <typename TA>
+__global__ void k_m_reduce(const TA* __restrict__ P, const int32_t* __restrict__ batch_chunk_off,
+                           int K, int B, int d, double* __restrict__ M) {
+  extern __shared__ double sm[];
+  double* part = sm;              // [RED_Y][d]
+  double* row = sm + RED_Y * d;   // [d]
+  double* row0 = row + d;         // [d]
   const int k = blockIdx.x;
-  for (int c = threadIdx.x; c < d; c += blockDim.x) {
-    double row0 = 0;
-    for (int b = 0; b < B; ++b) {
-      double s = 0;
-      for (int q = batch_chunk_off[b]; q < batch_chunk_off[b + 1]; ++q) {
-        const size_t at = ((size_t)q * K + k) * d + c;
-        s += Pf ? (double)Pf[at] : Pd[at];
-      }
-      M[((size_t)k * (B + 1) + b + 1) * d + c] = s;
-      row0 += s;
+  const int t = threadIdx.y * 32 + threadIdx.x;
+  for (int c = t; c < d; c += 32 * RED_Y) row0[c] = 0;
+  for (int b = 0; b < B; ++b) {
+    reduce_rows_into(P, batch_chunk_off[b], batch_chunk_off[b + 1], (size_t)K * d, (size_t)k * d, d,
+                     part, row);
+    for (int c = t; c < d; c += 32 * RED_Y) {
+      M[((size_t)k * (B + 1) + b + 1) * d + c] = row[c];
+      row0[c] += row[c];
     }
-    M[((size_t)k * (B + 1)) * d + c] = row0;
+    __syncthreads();
   }
+  for (int c = t; c < d; c += 32 * RED_Y) M[((size_t)k * (B + 1)) * d + c] = row0[c];
 }
 
 template <typename TA>
 int launch_m_reduce(const TA* P, const AccumChunk*, int, const int32_t* d_batch_chunk_off, int K,
                     int B, int d, double* M, cudaStream_t st) {
-  const float* Pf = std::is_same<TA, float>::value ? (const float*)P : nullptr;
-  const double* Pd = std::is_same<TA, double>::value ? (const double*)P : nullptr;
-  k_m_reduce<<<K, 128, 0, st>>>(Pf, Pd, d_batch_chunk_off, K, B, d, M);
+  k_m_reduce<TA><<<K, dim3(32, RED_Y), sizeof(double) * (RED_Y + 2) * d, st>>>(P, d_batch_chunk_off,
+                                                                              K, B, d, M);
   HB_LAUNCH_CHECK();
   return HB_OK;
 }

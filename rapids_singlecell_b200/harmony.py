@@ -17,7 +17,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import HbOutputs, HbParams, PRECISIONS
+from ._lib import HbOutputs, HbParams, PRECISIONS  # noqa: F401
 
 SUPPRESS_PENALTY = 1e30
 
@@ -30,6 +30,116 @@ class HarmonyInfo:
     n_outer: int = 0
     n_clusters: int = 0
     precision: str = "fp32"
+    profile: dict | None = None
+
+
+class HarmonyProblem:
+    """One Harmony problem resident on the GPU: the engine plan, its workspace and
+    the device inputs.  ``run()`` integrates it (and can be called again, e.g. to
+    time it); nothing is copied between host and device inside ``run()`` except
+    the small per-batch tables and the objective values.
+
+    ``X`` is a CUDA tensor (float32, or float64 for precision "fp64"), ``cats``
+    the int32 batch code per cell (host array), ``theta`` the per-batch theta
+    (tau discount applied), ``Y0`` the initial centroids on the device.
+    """
+
+    def __init__(self, X, cats, n_batches, Y0, theta, *, precision="fp32", n_clusters,
+                 max_iter_harmony=10, max_iter_clustering=200, tol_harmony=1e-4,
+                 tol_clustering=1e-5, ridge_lambda=1.0, sigma=0.1, block_proportion=0.05,
+                 random_state=0, stabilized_penalty=True, dynamic_lambda=True, alpha=0.2,
+                 batch_prune_threshold=1e-5, stream=None):
+        self.lib = _lib.load()
+        self.device = X.device
+        self.X = X.contiguous()
+        n_cells, n_pcs = self.X.shape
+        cats = np.asarray(cats, dtype=np.int32)
+        self.n_batches = int(n_batches)
+        N_b = np.bincount(cats, minlength=self.n_batches).astype(np.int64)
+        self.cats = torch.as_tensor(cats, device=self.device)
+        self.cell_index = torch.as_tensor(np.argsort(cats, kind="stable").astype(np.int32),
+                                          device=self.device)
+        self.offsets = np.zeros(self.n_batches + 1, dtype=np.int64)
+        self.offsets[1:] = np.cumsum(N_b)
+        self.theta = np.asarray(theta, dtype=np.float64)
+        self.Y0 = torch.as_tensor(Y0, device=self.device).to(self.X.dtype).contiguous()
+        self.max_iter_harmony = max_iter_harmony
+        self.max_iter_clustering = max_iter_clustering
+        self.n_clusters = n_clusters
+        self.precision = precision
+        p = HbParams()
+        p.n_cells = n_cells
+        p.n_pcs = n_pcs
+        p.n_clusters = n_clusters
+        p.n_batches = self.n_batches
+        p.precision = PRECISIONS[precision]
+        p.block_size = int(n_cells * block_proportion)
+        p.max_iter_harmony = max_iter_harmony
+        p.max_iter_clustering = max_iter_clustering
+        p.tol_harmony = tol_harmony
+        p.tol_clustering = tol_clustering
+        p.sigma = sigma
+        p.ridge_lambda = ridge_lambda
+        p.alpha = alpha
+        p.batch_prune_threshold = 0.0 if batch_prune_threshold is None else batch_prune_threshold
+        p.prune = 0 if batch_prune_threshold is None else 1
+        p.stabilized_penalty = int(bool(stabilized_penalty))
+        p.dynamic_lambda = int(bool(dynamic_lambda))
+        p.random_state = int(random_state) & 0xFFFFFFFFFFFFFFFF
+        self.params = p
+        self.plan = ctypes.c_void_p()
+        _lib.check(self.lib.hb_plan_create(ctypes.byref(p), ctypes.byref(self.plan)))
+        self.ws_bytes = self.lib.hb_plan_workspace_bytes(self.plan)
+        self.ws = torch.empty(self.ws_bytes, dtype=torch.uint8, device=self.device)
+        self.Z_hat = torch.empty_like(self.X)
+        self._off_c = (ctypes.c_int64 * (self.n_batches + 1))(*self.offsets.tolist())
+        self._th_c = (ctypes.c_double * self.n_batches)(*self.theta.tolist())
+        self.stream = stream
+
+    @staticmethod
+    def workspace_bytes(params: HbParams) -> int:
+        lib = _lib.load()
+        plan = ctypes.c_void_p()
+        _lib.check(lib.hb_plan_create(ctypes.byref(params), ctypes.byref(plan)))
+        try:
+            return int(lib.hb_plan_workspace_bytes(plan))
+        finally:
+            lib.hb_plan_destroy(plan)
+
+    def run(self, profile: bool = False):
+        mih, mic = self.max_iter_harmony, self.max_iter_clustering
+        objs = (ctypes.c_double * (mih + 1))()
+        n_obj = ctypes.c_int32(0)
+        kobjs = (ctypes.c_double * max(1, mih * mic))()
+        kits = (ctypes.c_int32 * mih)()
+        conv = ctypes.c_int32(0)
+        prof = _lib.HbProfile()
+        out = HbOutputs(objs, ctypes.pointer(n_obj), kobjs, kits, ctypes.pointer(conv),
+                        ctypes.pointer(prof) if profile else None)
+        st = self.stream if self.stream is not None else torch.cuda.current_stream(self.device)
+        _lib.check(self.lib.hb_harmonize(
+            self.plan, self.X.data_ptr(), self.cats.data_ptr(), self.cell_index.data_ptr(),
+            self._off_c, self._th_c, self.Y0.data_ptr(), self.ws.data_ptr(), self.ws_bytes,
+            self.Z_hat.data_ptr(), ctypes.byref(out), ctypes.c_void_p(st.cuda_stream)))
+        n_outer = n_obj.value - 1
+        info = HarmonyInfo(
+            objectives_harmony=[objs[i] for i in range(n_obj.value)],
+            kmeans_objectives=[[kobjs[o * mic + i] for i in range(kits[o])] for o in range(n_outer)],
+            converged=bool(conv.value), n_outer=n_outer, n_clusters=self.n_clusters,
+            precision=self.precision,
+            profile={f: getattr(prof, f) for f, _ in _lib.HbProfile._fields_} if profile else None)
+        return self.Z_hat, info
+
+    def close(self):
+        if self.plan:
+            self.lib.hb_plan_destroy(self.plan)
+            self.plan = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass
 
 
 def get_batch_codes(batch_mat, batch_key):
@@ -187,12 +297,6 @@ def harmonize(
     prec = _resolve_precision(precision, X.dtype)
     X = X.to(torch.float64 if prec == "fp64" else torch.float32).contiguous()
 
-    cats = torch.as_tensor(cats_np, device=device)
-    order = np.argsort(cats_np, kind="stable").astype(np.int32)
-    cell_index = torch.as_tensor(order, device=device)
-    offsets = np.zeros(n_batches + 1, dtype=np.int64)
-    offsets[1:] = np.cumsum(N_b)
-
     if init_centroids is None:
         Y0 = seeded_centroids(X, n_clusters, random_state)
     else:
@@ -201,58 +305,17 @@ def harmonize(
             raise ValueError(
                 f"init_centroids must have shape ({n_clusters}, {n_pcs}), got {tuple(Y0.shape)}"
             )
-    Y0 = Y0.to(X.dtype).contiguous()
-
-    p = HbParams()
-    p.n_cells = n_cells
-    p.n_pcs = n_pcs
-    p.n_clusters = n_clusters
-    p.n_batches = n_batches
-    p.precision = PRECISIONS[prec]
-    p.block_size = int(n_cells * block_proportion)
-    p.max_iter_harmony = max_iter_harmony
-    p.max_iter_clustering = max_iter_clustering
-    p.tol_harmony = tol_harmony
-    p.tol_clustering = tol_clustering
-    p.sigma = sigma
-    p.ridge_lambda = ridge_lambda
-    p.alpha = alpha
-    p.batch_prune_threshold = 0.0 if batch_prune_threshold is None else batch_prune_threshold
-    p.prune = 0 if batch_prune_threshold is None else 1
-    p.stabilized_penalty = int(bool(stabilized_penalty))
-    p.dynamic_lambda = int(bool(dynamic_lambda))
-    p.random_state = int(random_state) & 0xFFFFFFFFFFFFFFFF
-
-    plan = ctypes.c_void_p()
-    _lib.check(lib.hb_plan_create(ctypes.byref(p), ctypes.byref(plan)))
-    try:
-        ws_bytes = lib.hb_plan_workspace_bytes(plan)
-        ws = torch.empty(ws_bytes, dtype=torch.uint8, device=device)
-        Z_hat = torch.empty_like(X)
-        objs = (ctypes.c_double * (max_iter_harmony + 1))()
-        n_obj = ctypes.c_int32(0)
-        kobjs = (ctypes.c_double * max(1, max_iter_harmony * max_iter_clustering))()
-        kits = (ctypes.c_int32 * max_iter_harmony)()
-        conv = ctypes.c_int32(0)
-        out = HbOutputs(objs, ctypes.pointer(n_obj), kobjs, kits, ctypes.pointer(conv))
-        off_c = (ctypes.c_int64 * (n_batches + 1))(*offsets.tolist())
-        th_c = (ctypes.c_double * n_batches)(*th.tolist())
-        stream = torch.cuda.current_stream(device).cuda_stream
-        _lib.check(lib.hb_harmonize(plan, X.data_ptr(), cats.data_ptr(), cell_index.data_ptr(),
-                                    off_c, th_c, Y0.data_ptr(), ws.data_ptr(), ws_bytes,
-                                    Z_hat.data_ptr(), ctypes.byref(out), ctypes.c_void_p(stream)))
-    finally:
-        lib.hb_plan_destroy(plan)
-
-    n_outer = n_obj.value - 1
-    info = HarmonyInfo(
-        objectives_harmony=[objs[i] for i in range(n_obj.value)],
-        kmeans_objectives=[[kobjs[o * max_iter_clustering + i] for i in range(kits[o])]
-                           for o in range(n_outer)],
-        converged=bool(conv.value), n_outer=n_outer, n_clusters=n_clusters, precision=prec,
-    )
+    problem = HarmonyProblem(
+        X, cats_np, n_batches, Y0, th, precision=prec, n_clusters=n_clusters,
+        max_iter_harmony=max_iter_harmony, max_iter_clustering=max_iter_clustering,
+        tol_harmony=tol_harmony, tol_clustering=tol_clustering, ridge_lambda=ridge_lambda,
+        sigma=sigma, block_proportion=block_proportion, random_state=random_state,
+        stabilized_penalty=stabilized_penalty, dynamic_lambda=dynamic_lambda, alpha=alpha,
+        batch_prune_threshold=batch_prune_threshold)
+    Z_hat, info = problem.run()
+    problem.close()
     if info.converged and verbose:
-        print(f"Harmony converged in {n_outer} iterations")
+        print(f"Harmony converged in {info.n_outer} iterations")
     if not info.converged:
         warnings.warn("Harmony did not converge. Consider increasing the number of iterations")
     return (Z_hat, info) if return_info else Z_hat

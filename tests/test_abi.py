@@ -50,4 +50,5 @@ def test_plan_validation_without_gpu():
 def test_struct_layout():
     # hb_params: 8+4*4+8+4*2+8*6+4*4+8 = 112 bytes
     assert ctypes.sizeof(_lib.HbParams) == 112
-    assert ctypes.sizeof(_lib.HbOutputs) == 5 * ctypes.sizeof(ctypes.c_void_p)
+    assert ctypes.sizeof(_lib.HbOutputs) == 6 * ctypes.sizeof(ctypes.c_void_p)
+    assert ctypes.sizeof(_lib.HbProfile) == 56

@@ -40,18 +40,26 @@ def test_l2_normalize_zero_row():
 
 @pytest.mark.parametrize("n,bs", [(20_000, 1000), (1000, 50), (1003, 50), (777, 777), (100_000, 5000),
                                   (2_000_000, 100_000), (50, 1), (4099, 2048)])
-def test_block_lists_match_sorted_permutation(n, bs):
+@pytest.mark.parametrize("B", [0, 3, 32])
+def test_block_lists_match_sorted_permutation(n, bs, B):
     seeds = [0, 12345, 1000003, 0xFFFFFFFF, 7, 99, 5, 31337, 42]
-    ws_bytes = lib().hb_block_lists_workspace_bytes(n, bs)
+    cats = np.random.default_rng(n).integers(0, max(B, 1), n).astype(np.int32)
+    ws_bytes = lib().hb_block_lists_workspace_bytes(n, bs, B)
     ws = torch.empty(ws_bytes, dtype=torch.uint8, device="cuda")
     idx = torch.empty(len(seeds) * n, dtype=torch.int32, device="cuda")
     arr = (ctypes.c_uint32 * len(seeds))(*seeds)
-    _lib.check(lib().hb_block_lists(n, bs, arr, len(seeds), ptr(idx), ptr(ws), ws_bytes, stream()))
+    dcats = dev(cats)
+    _lib.check(lib().hb_block_lists(n, bs, arr, len(seeds), ptr(dcats) if B else None, B, ptr(idx),
+                                    ptr(ws), ws_bytes, stream()))
     got = idx.cpu().numpy().reshape(len(seeds), n)
     for c, s in enumerate(seeds):
         perm = ho.block_permutation(n, s)
         for j, p0 in enumerate(range(0, n, bs)):
-            exp = np.sort(perm[p0:p0 + bs])
+            blk = perm[p0:p0 + bs]
+            if B:  # within a block: ordered by (batch, cell)
+                exp = blk[np.lexsort((blk, cats[blk]))]
+            else:
+                exp = np.sort(blk)
             np.testing.assert_array_equal(got[c, p0:p0 + bs], exp, err_msg=f"seed {s} block {j}")
 
 
@@ -64,8 +72,8 @@ def test_penalty(stabilized, B, K):
     O[0, 0] = 0
     th = rng.random(B) * 2 + 0.5
     pen = torch.empty((B, K), dtype=torch.float64, device="cuda")
-    _lib.check(lib().hb_penalty(ptr(dev(E)), ptr(dev(O)), ptr(dev(th)), ptr(pen), B, K,
-                                int(stabilized), stream()))
+    dE, dO, dth = dev(E), dev(O), dev(th)  # keep the inputs alive across the launch
+    _lib.check(lib().hb_penalty(ptr(dE), ptr(dO), ptr(dth), ptr(pen), B, K, int(stabilized), stream()))
     np.testing.assert_allclose(pen.cpu().numpy(), ho.penalty(E, O, th, stabilized), rtol=1e-12)
 
 
@@ -73,7 +81,8 @@ def _lambda(E, O, Nb, **kw):
     B, K = E.shape
     out = torch.empty((B, K), dtype=torch.float64, device="cuda")
     thr = kw["threshold"]
-    _lib.check(lib().hb_lambda_kb(ptr(dev(E)), ptr(dev(O)), ptr(dev(Nb)), ptr(out), B, K, kw["alpha"],
+    dE, dO, dNb = dev(E), dev(O), dev(Nb)
+    _lib.check(lib().hb_lambda_kb(ptr(dE), ptr(dO), ptr(dNb), ptr(out), B, K, kw["alpha"],
                                   0.0 if thr is None else thr, int(thr is not None),
                                   kw["ridge_lambda"], int(kw["dynamic_lambda"]), stream()))
     return out.cpu().numpy()
@@ -104,7 +113,8 @@ def test_ridge_inverse(B):
     lam = rng.random((B, K)) * 5 + 0.1
     lam[0, 0] = 1e30
     inv = torch.empty((K, B + 1, B + 1), dtype=torch.float64, device="cuda")
-    _lib.check(lib().hb_ridge_inverse(ptr(dev(O)), ptr(dev(lam)), ptr(inv), B, K, stream()))
+    dO, dlam = dev(O), dev(lam)
+    _lib.check(lib().hb_ridge_inverse(ptr(dO), ptr(dlam), ptr(inv), B, K, stream()))
     got = inv.cpu().numpy()
     for k in range(K):
         np.testing.assert_allclose(got[k], ho.arrowhead_inverse(O[:, k], lam[:, k]), atol=1e-12,

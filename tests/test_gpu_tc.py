@@ -1,0 +1,74 @@
+"""Tensor-core (tcgen05) path: the similarity tile against a plain PyTorch fp32
+reference of the same op, and full 16-bit Harmony runs against the float64
+oracle (error budget of the 16-bit path: 1e-3 relative max-abs on Z_hat)."""
+
+import numpy as np
+import pandas as pd
+import pytest
+import torch
+
+from oracle import harmony_oracle as ho
+from rapids_singlecell_b200 import _lib, harmonize
+from rapids_singlecell_b200.synthetic import MixtureSpec, initial_centroids, make_config, make_mixture
+from tests._gpu import dev, lib, ptr, rel_maxabs, stream
+
+pytestmark = pytest.mark.gpu
+HT = {"fp16": (torch.float16, _lib.HB_FP16), "bf16": (torch.bfloat16, _lib.HB_BF16)}
+
+
+def _pad(t, ld):
+    out = torch.zeros((t.shape[0], ld), dtype=t.dtype, device=t.device)
+    out[:, : t.shape[1]] = t
+    return out
+
+
+@pytest.mark.parametrize("prec", ["fp16", "bf16"])
+@pytest.mark.parametrize("n,d,K", [(128, 64, 16), (300, 50, 100), (1000, 100, 200), (257, 3, 7),
+                                   (5000, 128, 256), (129, 65, 129)])
+def test_similarity_tile(prec, n, d, K):
+    dt, code = HT[prec]
+    g = torch.Generator(device="cuda").manual_seed(n + d + K)
+    Z = torch.nn.functional.normalize(torch.randn(2 * n, d, device="cuda", generator=g), dim=1)
+    Y = torch.nn.functional.normalize(torch.randn(K, d, device="cuda", generator=g), dim=1)
+    ld = (d + 7) // 8 * 8
+    Zh, Yh = _pad(Z.to(dt), ld), _pad(Y.to(dt), ld)
+    idx = torch.randperm(2 * n, device="cuda", generator=g)[:n].to(torch.int32)
+    S = torch.full((n, K), float("nan"), device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    _lib.check(lib().hb_similarity(ptr(Zh), ld, ptr(Yh), ld, ptr(idx), n, d, K, code, ptr(S), ptr(err),
+                                   stream()))
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    ref = Zh[idx.long(), :d].float() @ Yh[:, :d].float().T   # fp32 reference of the same op
+    torch.testing.assert_close(S, ref, rtol=1e-5, atol=1e-5)
+
+
+@pytest.mark.parametrize("prec", ["fp16", "bf16"])
+def test_c1_small_16bit_vs_fp64_oracle(prec):
+    cfg = make_config("C1", seed=1, n_cells=4000)
+    Y0 = cfg["Y0"][:40]
+    labels = pd.Categorical.from_codes(cfg["cats"], categories=["a", "b", "c"])
+    kw = dict(n_clusters=40, max_iter_harmony=3, max_iter_clustering=8, tol_harmony=-np.inf,
+              tol_clustering=-np.inf)
+    out, info = harmonize(torch.as_tensor(cfg["Z"], device="cuda"), labels, None, init_centroids=Y0,
+                          precision=prec, return_info=True, **kw)
+    ref = ho.harmonize(cfg["Z"], cfg["cats"], 3, Y0, dtype=np.float64, **kw)
+    err = rel_maxabs(out.cpu().numpy(), ref.Z_hat)
+    print(f"{prec}: rel max-abs vs fp64 oracle = {err:.3e}; objectives {info.objectives_harmony} vs "
+          f"{ref.objectives_harmony}")
+    np.testing.assert_allclose(info.objectives_harmony, ref.objectives_harmony, rtol=5e-3)
+    assert err < (1e-3 if prec == "fp16" else 5e-3)
+
+
+@pytest.mark.parametrize("n,d,K,B", [(3001, 5, 17, 4), (6000, 100, 200, 12), (2000, 64, 129, 1)])
+def test_16bit_odd_shapes_fp16(n, d, K, B):
+    spec = MixtureSpec(n, d, 5, B, "dirichlet", (), 0.5, (0.8, 1.2))
+    Z, cats, _ = make_mixture(spec, 21)
+    Y0 = initial_centroids(Z, K, 22)
+    labels = pd.Categorical.from_codes(cats, categories=[f"b{i}" for i in range(B)])
+    kw = dict(n_clusters=K, max_iter_harmony=2, max_iter_clustering=4, tol_harmony=-np.inf,
+              tol_clustering=-np.inf)
+    out = harmonize(torch.as_tensor(Z, device="cuda"), labels, None, init_centroids=Y0,
+                    precision="fp16", **kw)
+    ref = ho.harmonize(Z, cats, B, Y0, dtype=np.float64, **kw)
+    assert rel_maxabs(out.cpu().numpy(), ref.Z_hat) < 2e-3

@@ -67,6 +67,7 @@ struct Work {
   double* obj_acc;
   double* obj_out;
   double* M;
+  double* Omin;  // [nblk][B][K] old contribution of each block of the current iteration
   int32_t* idx;
   int* err;
   AccumChunk* cen_chunks;
@@ -93,6 +94,7 @@ void carve(const hb_plan& P, Carver& cv, Work& w) {
   w.obj_acc = cv.take<double>(1);
   w.obj_out = cv.take<double>(std::max(p.max_iter_clustering, 1) + 1);
   w.M = cv.take<double>((size_t)K * (B + 1) * d);
+  w.Omin = cv.take<double>((size_t)P.ml.nblk * B * K);
   w.idx = cv.take<int32_t>((size_t)kMaxIterChunk * n);
   w.err = cv.take<int>(4);
   w.cen_chunks = cv.take<AccumChunk>(P.cen_chunks);
@@ -300,7 +302,7 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
   HB_TRY(launch_l2_normalize<T, S>(Y0, K, d, d, Yn, P->ldy, st));
   {
     BlockArgs a = base;
-    a.idx_new = nullptr; a.new_start = 0; a.n_new = n; a.idx_old = nullptr; a.n_old = 0;
+    a.idx_new = nullptr; a.new_start = 0; a.n_new = n; a.Om_cur = nullptr; a.Om_next = nullptr;
     a.init_mode = 1;
     HB_TRY(ring.step<S>(a, st));
   }
@@ -355,32 +357,25 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
       for (int c = 0; c < C && !stop; ++c) {
         const int it = it0 + c;
         const int32_t* idx = w.idx + (size_t)c * n;
-        // centroids Y = R^T Z_norm, L2-normalised (clustering.cu:272-281)
-        int sp = span_begin(1, (double)n * (zb + rb));
-        HB_TRY(launch_accum<S, S, TA>(R, P->ldr, Zn, P->ldz, nullptr, w.cen_chunks, P->cen_chunks, K, d,
-                                      (TA*)w.Ypart, st));
+        // centroids Y = R^T Z_norm, L2-normalised (clustering.cu:272-281).  The pass walks
+        // the block-ordered cell list, so it also sums every block's current rows per
+        // batch: the "remove old contribution" terms of the sweep (clustering.cu:321-332).
+        const size_t omsz = (size_t)B * K;
+        HB_CUDA(cudaMemsetAsync(w.Omin, 0, sizeof(double) * nblk * omsz, st));
+        int sp = span_begin(1, (double)n * (zb + rb + 8));
+        HB_TRY(launch_accum<S, S, TA>(R, P->ldr, Zn, P->ldz, idx, w.cen_chunks, P->cen_chunks, K, d,
+                                      (TA*)w.Ypart, st, OminArgs{w.Omin, cats, ml.bs, B}));
         HB_TRY(launch_centroid_reduce<TA, S>((TA*)w.Ypart, P->cen_chunks, K, d, Yn, P->ldy, st));
         span_end(sp);
-        // remove block 0's current rows, then sweep the blocks (clustering.cu:308-372)
-        {
-          BlockArgs a = base;
-          a.n_new = 0; a.idx_new = nullptr;
-          a.idx_old = idx; a.n_old = std::min<int64_t>(ml.bs, n);
-          sp = span_begin(0, (double)a.n_old * (rb + 8));
-          HB_TRY(ring.step<S>(a, st));
-          span_end(sp);
-        }
+        // sweep the blocks (clustering.cu:308-372)
         for (int j = 0; j < nblk; ++j) {
           BlockArgs a = base;
           const int64_t s0 = (int64_t)j * ml.bs;
           a.idx_new = idx + s0;
           a.n_new = std::min<int64_t>(ml.bs, n - s0);
-          if (j + 1 < nblk) {
-            const int64_t s1 = s0 + ml.bs;
-            a.idx_old = idx + s1;
-            a.n_old = std::min<int64_t>(ml.bs, n - s1);
-          }
-          sp = span_begin(0, (double)a.n_new * (zb + rb + 8) + (double)a.n_old * (rb + 8));
+          a.Om_cur = j == 0 ? w.Omin : nullptr;
+          a.Om_next = j + 1 < nblk ? w.Omin + (size_t)(j + 1) * omsz : nullptr;
+          sp = span_begin(0, (double)a.n_new * (zb + rb + 8));
           HB_TRY(ring.step<S>(a, st));
           span_end(sp);
         }

@@ -165,9 +165,13 @@ __global__ void __launch_bounds__(256, 1) k_tc_block_update(TcArgs p, TcLayout L
   if (a.n_new > 0 && !a.init_mode) {
     for (int k = tid; k < K; k += 256) {
       double col = 0;
-      for (int b = 0; b < B; ++b) col += p.O_in[(size_t)b * K + k];
       for (int b = 0; b < B; ++b) {
-        const float o = (float)p.O_in[(size_t)b * K + k];
+        const size_t e = (size_t)b * K + k;
+        col += p.O_in[e] - (a.Om_cur ? a.Om_cur[e] : 0.0);
+      }
+      for (int b = 0; b < B; ++b) {
+        const size_t e = (size_t)b * K + k;
+        const float o = (float)(p.O_in[e] - (a.Om_cur ? a.Om_cur[e] : 0.0));
         const float E = (float)(a.Pr[b] * col);
         const float denom = a.stabilized ? (o + E + 1.f) : (o + 1.f);
         pen[b * K + k] = powf((E + 1.f) / denom, (float)a.theta[b]);
@@ -280,39 +284,14 @@ __global__ void __launch_bounds__(256, 1) k_tc_block_update(TcArgs p, TcLayout L
     }
   }
 
-  // remove the current rows of the next block's cells
-  const int64_t ntiles_old = (a.n_old + 127) / 128;
-  for (int64_t tile = blockIdx.x; tile < ntiles_old; tile += gridDim.x) {
-    __syncthreads();
-    const int nvalid = (int)(a.n_old - tile * 128 < 128 ? a.n_old - tile * 128 : 128);
-    const uint32_t sR = tc::smem_u32(Rst);
-    for (int e = tid; e < nvalid * L.ldr_chunks; e += 256) {
-      const int r = e / L.ldr_chunks, ch = e % L.ldr_chunks;
-      const int64_t cl = __ldg(a.idx_old + tile * 128 + r);
-      tc::cp_async16(sR + (uint32_t)(r * L.ldst + ch * 8) * 2u, R + cl * a.ldr + ch * 8, 16u);
-      if (ch == 0) ccat[r] = __ldg(a.cats + cl);
-    }
-    tc::cp_async_wait_all();
-    __syncthreads();
-    if (tid < K) {
-      float acc = 0.f;
-      int cur = ccat[0];
-      for (int r = 0; r < nvalid; ++r) {
-        const int c = ccat[r];
-        if (c != cur) {
-          osm[cur * K + tid] -= acc;
-          acc = 0.f;
-          cur = c;
-        }
-        acc += h2f(Rst[r * L.ldst + tid]);
-      }
-      osm[cur * K + tid] -= acc;
-    }
-  }
   __syncthreads();
   for (int e = tid; e < B * K; e += 256) {
     double v = (double)osm[e];
-    if (blockIdx.x == 0 && p.O_in) v += p.O_in[e];
+    if (blockIdx.x == 0) {
+      if (p.O_in) v += p.O_in[e];
+      if (a.Om_cur) v -= a.Om_cur[e];
+      if (a.Om_next) v -= a.Om_next[e];
+    }
     if (v != 0.0) atomicAdd(&p.O_out[e], v);
   }
   const double tot = block_sum(obj_local, red);
@@ -413,7 +392,7 @@ int launch_tc_block_update(const BlockArgs& a, const double* O_in, double* O_out
   const TcLayout L = tc_layout(a.d, a.K, a.B, a.ldr, 4);
   int occ = 1;
   HB_TRY(prepare<H>((const void*)k_tc_block_update<H>, L, &occ));
-  const int64_t tiles = std::max<int64_t>((a.n_new + 127) / 128, (a.n_old + 127) / 128);
+  const int64_t tiles = (a.n_new + 127) / 128;
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)num_sms() * occ));
   // keep residency at `occ` CTAs per SM (TMEM budget) by padding the shared-memory request
   size_t smem = L.bytes;

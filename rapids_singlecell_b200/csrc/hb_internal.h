@@ -49,10 +49,20 @@ struct AccumChunk {  // a run of cells that all belong to batch `batch`
   int32_t batch;
 };
 
+// Optional by-product of the centroid pass over a block-ordered cell list:
+// Omin[(pos / bs) * B + cats[cell]][k] += W[cell][k]  (float64, zeroed by the caller)
+struct OminArgs {
+  double* Omin;
+  const int32_t* cats;
+  int64_t bs;
+  int B;
+};
+
 // P[chunk][k][c] = sum over the chunk's cells i of W[i][k] * V[i][c]
 template <typename TS, typename TV, typename TA>
 int launch_accum(const TS* W, int ldw, const TV* V, int ldv, const int32_t* cell_index,
-                 const AccumChunk* chunks, int n_chunks, int K, int d, TA* P, cudaStream_t st);
+                 const AccumChunk* chunks, int n_chunks, int K, int d, TA* P, cudaStream_t st,
+                 OminArgs om = OminArgs{nullptr, nullptr, 1, 1});
 
 // Y_norm[k] = l2norm(sum_chunks P[chunk][k]); optional 16-bit copy.
 template <typename TA, typename TY>
@@ -73,8 +83,8 @@ struct BlockArgs {
   const int32_t* idx_new;  // nullptr -> identity (start at new_start)
   int64_t new_start;
   int64_t n_new;
-  const int32_t* idx_old;
-  int64_t n_old;
+  const double* Om_cur;   // [B][K] old contribution of this block (nullptr = none)
+  const double* Om_next;  // [B][K] old contribution of the next block (nullptr = none)
   double* obj_acc;      // kmeans error + entropy of the new rows
   double sigma;
   int d, K, B;

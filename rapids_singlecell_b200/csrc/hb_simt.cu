@@ -62,12 +62,13 @@ __global__ void __launch_bounds__(256) k_accum(const TS* __restrict__ W, int ldw
                                                const TV* __restrict__ V, int ldv,
                                                const int32_t* __restrict__ cell_index,
                                                const AccumChunk* __restrict__ chunks, int K,
-                                               int d, int ktiles, TA* __restrict__ P) {
+                                               int d, int ktiles, TA* __restrict__ P, OminArgs om) {
   constexpr int ROWS = sizeof(TA) == 8 ? 16 : 32;
   constexpr int NW = ROWS * ACC_BK / 256;  // W elements per thread per step
   constexpr int NV = ROWS * ACC_BD / 256;  // V elements per thread per step
   __shared__ TA ws[ROWS][ACC_BK];
   __shared__ TA vs[ROWS][ACC_BD];
+  __shared__ int rkey_s[ROWS];
   const AccumChunk ch = chunks[blockIdx.x];
   const int kt = blockIdx.y % ktiles, dt = blockIdx.y / ktiles;
   const int k0 = kt * ACC_BK, d0 = dt * ACC_BD;
@@ -79,7 +80,21 @@ __global__ void __launch_bounds__(256) k_accum(const TS* __restrict__ W, int ldw
     for (int b = 0; b < 4; ++b) acc[a][b] = TA(0);
 
   TA rw[NW], rv[NV];
+  int rkey = -1;
+  // per-(block, batch) sums of the W rows (the "old contribution" of each block),
+  // only by the CTAs of the first PC tile; rows arrive ordered by (block, batch)
+  const bool do_om = om.Omin != nullptr && dt == 0;
+  double om_acc = 0.0;
+  int om_key = -1;
   auto load = [&](int pos) {
+    if (do_om && tid < ROWS) {
+      rkey = -1;
+      if (pos + tid < ch.len) {
+        const int64_t qq = ch.start + pos + tid;
+        const int64_t cell = cell_index ? (int64_t)__ldg(cell_index + qq) : qq;
+        rkey = (int)(qq / om.bs) * om.B + __ldg(om.cats + cell);
+      }
+    }
 #pragma unroll
     for (int q = 0; q < NW; ++q) {
       const int e = tid + q * 256, r = e / ACC_BK, kk = e % ACC_BK;
@@ -110,8 +125,21 @@ __global__ void __launch_bounds__(256) k_accum(const TS* __restrict__ W, int ldw
     for (int q = 0; q < NW; ++q) { const int e = tid + q * 256; ws[e / ACC_BK][e % ACC_BK] = rw[q]; }
 #pragma unroll
     for (int q = 0; q < NV; ++q) { const int e = tid + q * 256; vs[e / ACC_BD][e % ACC_BD] = rv[q]; }
+    if (do_om && tid < ROWS) rkey_s[tid] = rkey;
     __syncthreads();
     if (pos + ROWS < ch.len) load(pos + ROWS);  // next step's loads overlap this step's math
+    if (do_om && tid < ACC_BK && k0 + tid < K) {
+      const int nrow = min(ROWS, ch.len - pos);
+      for (int r = 0; r < nrow; ++r) {
+        const int key = rkey_s[r];
+        if (key != om_key) {
+          if (om_key >= 0) atomicAdd(&om.Omin[(size_t)om_key * K + k0 + tid], om_acc);
+          om_key = key;
+          om_acc = 0.0;
+        }
+        om_acc += (double)ws[r][tid];
+      }
+    }
 #pragma unroll 4
     for (int r = 0; r < ROWS; ++r) {
       TA wv[8], vv[4];
@@ -125,6 +153,8 @@ __global__ void __launch_bounds__(256) k_accum(const TS* __restrict__ W, int ldw
         for (int b = 0; b < 4; ++b) acc[a][b] += wv[a] * vv[b];
     }
   }
+  if (do_om && om_key >= 0 && tid < ACC_BK && k0 + tid < K)
+    atomicAdd(&om.Omin[(size_t)om_key * K + k0 + tid], om_acc);
   TA* out = P + (size_t)blockIdx.x * K * d;
 #pragma unroll
   for (int a = 0; a < 8; ++a) {
@@ -140,29 +170,30 @@ __global__ void __launch_bounds__(256) k_accum(const TS* __restrict__ W, int ldw
 
 template <typename TS, typename TV, typename TA>
 int launch_accum(const TS* W, int ldw, const TV* V, int ldv, const int32_t* cell_index,
-                 const AccumChunk* chunks, int n_chunks, int K, int d, TA* P, cudaStream_t st) {
+                 const AccumChunk* chunks, int n_chunks, int K, int d, TA* P, cudaStream_t st,
+                 OminArgs om) {
   if (n_chunks == 0) return HB_OK;
   const int ktiles = div_up(K, ACC_BK), dtiles = div_up(d, ACC_BD);
   k_accum<TS, TV, TA><<<dim3(n_chunks, ktiles * dtiles), 256, 0, st>>>(W, ldw, V, ldv, cell_index,
-                                                                       chunks, K, d, ktiles, P);
+                                                                       chunks, K, d, ktiles, P, om);
   HB_LAUNCH_CHECK();
   return HB_OK;
 }
 template int launch_accum<float, float, float>(const float*, int, const float*, int, const int32_t*,
-                                               const AccumChunk*, int, int, int, float*, cudaStream_t);
+                                               const AccumChunk*, int, int, int, float*, cudaStream_t, OminArgs);
 template int launch_accum<double, double, double>(const double*, int, const double*, int, const int32_t*,
-                                                  const AccumChunk*, int, int, int, double*, cudaStream_t);
+                                                  const AccumChunk*, int, int, int, double*, cudaStream_t, OminArgs);
 template int launch_accum<__half, float, float>(const __half*, int, const float*, int, const int32_t*,
-                                                const AccumChunk*, int, int, int, float*, cudaStream_t);
+                                                const AccumChunk*, int, int, int, float*, cudaStream_t, OminArgs);
 template int launch_accum<__nv_bfloat16, float, float>(const __nv_bfloat16*, int, const float*, int,
                                                        const int32_t*, const AccumChunk*, int, int, int,
-                                                       float*, cudaStream_t);
+                                                       float*, cudaStream_t, OminArgs);
 template int launch_accum<__half, __half, float>(const __half*, int, const __half*, int, const int32_t*,
-                                                 const AccumChunk*, int, int, int, float*, cudaStream_t);
+                                                 const AccumChunk*, int, int, int, float*, cudaStream_t, OminArgs);
 template int launch_accum<__nv_bfloat16, __nv_bfloat16, float>(const __nv_bfloat16*, int,
                                                                const __nv_bfloat16*, int, const int32_t*,
                                                                const AccumChunk*, int, int, int, float*,
-                                                               cudaStream_t);
+                                                               cudaStream_t, OminArgs);
 
 // Y_norm[k] = l2normalise(sum over chunks of P[chunk][k]) -- fixed summation
 // order (deterministic), float64 accumulation.  One CTA per centroid row; 8
@@ -280,13 +311,16 @@ __global__ void __launch_bounds__(BU_THREADS) k_block_update(BlockArgsDev p) {
     double* ocol = (double*)zt;  // scratch: K doubles fit in zt + yt
     for (int k = tid; k < K; k += BU_THREADS) {
       double s = 0;
-      for (int b = 0; b < B; ++b) s += p.O_in[(size_t)b * K + k];
+      for (int b = 0; b < B; ++b) {
+        const size_t e = (size_t)b * K + k;
+        s += p.O_in[e] - (a.Om_cur ? a.Om_cur[e] : 0.0);
+      }
       ocol[k] = s;
     }
     __syncthreads();
     for (int e = tid; e < B * K; e += BU_THREADS) {
       const int b = e / K, k = e % K;
-      const T o = (T)p.O_in[e];
+      const T o = (T)(p.O_in[e] - (a.Om_cur ? a.Om_cur[e] : 0.0));
       const T E = (T)(a.Pr[b] * ocol[k]);
       const T denom = a.stabilized ? (o + E + T(1)) : (o + T(1));
       pen[e] = num<T>::pow_((E + T(1)) / denom, (T)a.theta[b]);
@@ -421,39 +455,15 @@ __global__ void __launch_bounds__(BU_THREADS) k_block_update(BlockArgsDev p) {
     }
   }
 
-  // remove the current rows of the next block's cells (two rows per warp step,
-  // all loads issued before the shared-memory atomics)
-  {
-    constexpr int KL = (K16 + 31) / 32;
-    const int lane = tid & 31, w = tid >> 5;
-    const int64_t nw = (int64_t)gridDim.x * (BU_THREADS / 32);
-    for (int64_t q = (int64_t)blockIdx.x * (BU_THREADS / 32) + w; q < a.n_old; q += 2 * nw) {
-      const int64_t q2 = q + nw;
-      const int64_t c1 = a.idx_old[q];
-      const int64_t c2 = q2 < a.n_old ? (int64_t)a.idx_old[q2] : -1;
-      const int cat1 = a.cats[c1];
-      const int cat2 = c2 >= 0 ? a.cats[c2] : 0;
-      T v1[KL], v2[KL];
-#pragma unroll
-      for (int u = 0; u < KL; ++u) {
-        const int k = lane + 32 * u;
-        v1[u] = k < K ? R[c1 * a.ldr + k] : T(0);
-        v2[u] = (k < K && c2 >= 0) ? R[c2 * a.ldr + k] : T(0);
-      }
-#pragma unroll
-      for (int u = 0; u < KL; ++u) {
-        const int k = lane + 32 * u;
-        if (k < K) {
-          atomicAdd(&osm[cat1 * K + k], -v1[u]);
-          if (c2 >= 0) atomicAdd(&osm[cat2 * K + k], -v2[u]);
-        }
-      }
-    }
-  }
   __syncthreads();
   for (int e = tid; e < B * K; e += BU_THREADS) {
     double v = (double)osm[e];
-    if (blockIdx.x == 0) v += p.O_in ? p.O_in[e] : 0.0;
+    if (blockIdx.x == 0) {
+      // this CTA also carries the state forward: O_in - old(this block) - old(next block)
+      if (p.O_in) v += p.O_in[e];
+      if (a.Om_cur) v -= a.Om_cur[e];
+      if (a.Om_next) v -= a.Om_next[e];
+    }
     if (v != 0.0) atomicAdd(&p.O_out[e], v);
   }
   const double tot = block_sum(obj_local, red);
@@ -476,8 +486,7 @@ static int launch_block_kpt(const BlockArgsDev& p, cudaStream_t st) {
   int occ = 1;
   HB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_block_update<T, KPT>, BU_THREADS, smem));
   if (occ < 1) occ = 1;
-  const int64_t tiles = std::max<int64_t>((a.n_new + BU_TM - 1) / BU_TM,
-                                          (a.n_old + 7) / 8 / 4);
+  const int64_t tiles = (a.n_new + BU_TM - 1) / BU_TM;
   int grid = (int)std::min<int64_t>(std::max<int64_t>(tiles, 1), (int64_t)num_sms() * occ);
   k_block_update<T, KPT><<<grid, BU_THREADS, smem, st>>>(p);
   HB_LAUNCH_CHECK();

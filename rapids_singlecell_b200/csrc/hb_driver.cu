@@ -67,7 +67,8 @@ struct Work {
   double* obj_acc;
   double* obj_out;
   double* M;
-  double* Omin;  // [nblk][B][K] old contribution of each block of the current iteration
+  double* Omin;  // [nblk][B+1][K] old contribution of each block of the current iteration
+  unsigned* barrier;  // grid-barrier counter of the persistent sweep
   int32_t* idx;
   int* err;
   AccumChunk* cen_chunks;
@@ -87,14 +88,16 @@ void carve(const hb_plan& P, Carver& cv, Work& w) {
   w.Ypart = cv.take<char>((size_t)P.cen_chunks * K * d * P.asz);
   w.Mpart = cv.take<char>((size_t)P.max_m_chunks * K * d * P.asz);
   w.W = cv.take<char>((size_t)B * K * d * P.esz);
-  for (int i = 0; i < 3; ++i) w.O[i] = cv.take<double>((size_t)B * K);
+  // observed counts: [B][K] plus a column-sum row (kept by the 16-bit sweep)
+  for (int i = 0; i < 3; ++i) w.O[i] = cv.take<double>((size_t)(B + 1) * K);
   w.Pr = cv.take<double>(B);
   w.theta = cv.take<double>(B);
   w.Nb = cv.take<double>(B);
   w.obj_acc = cv.take<double>(1);
   w.obj_out = cv.take<double>(std::max(p.max_iter_clustering, 1) + 1);
   w.M = cv.take<double>((size_t)K * (B + 1) * d);
-  w.Omin = cv.take<double>((size_t)P.ml.nblk * B * K);
+  w.Omin = cv.take<double>((size_t)P.ml.nblk * (B + 1) * K);
+  w.barrier = cv.take<unsigned>(4);
   w.idx = cv.take<int32_t>((size_t)kMaxIterChunk * n);
   w.err = cv.take<int>(4);
   w.cen_chunks = cv.take<AccumChunk>(P.cen_chunks);
@@ -166,6 +169,7 @@ int hb_plan_create(const hb_params* params, hb_plan** plan) {
   P->cen_tiles = div_up(p.n_clusters, 128) * div_up(p.n_pcs, 64);
   const int64_t target = std::max(1, 2 * sms / P->cen_tiles);
   P->cen_chunks = (int)std::max<int64_t>(1, std::min<int64_t>(target, (p.n_cells + 255) / 256));
+  if (P->ssz == 2) P->cen_chunks = tc_centroid_grid(p.n_clusters);  // one partial per resident CTA
   P->m_chunk_len = std::max<int64_t>(256, (p.n_cells + target - 1) / target);
   P->max_m_chunks = (int)((p.n_cells + P->m_chunk_len - 1) / P->m_chunk_len) + p.n_batches;
   P->max_apply_tiles = (int)((p.n_cells + 31) / 32) + p.n_batches;
@@ -283,7 +287,7 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
   HB_CUDA(cudaMemcpyAsync(w.batch_chunk_off, bco.data(), sizeof(int32_t) * (B + 1), cudaMemcpyHostToDevice, st));
   if (!tiles.empty())
     HB_CUDA(cudaMemcpyAsync(w.apply_tiles, tiles.data(), sizeof(ApplyTile) * tiles.size(), cudaMemcpyHostToDevice, st));
-  for (int i = 0; i < 3; ++i) HB_CUDA(cudaMemsetAsync(w.O[i], 0, sizeof(double) * B * K, st));
+  for (int i = 0; i < 3; ++i) HB_CUDA(cudaMemsetAsync(w.O[i], 0, sizeof(double) * (B + 1) * K, st));
   HB_CUDA(cudaMemsetAsync(w.obj_acc, 0, sizeof(double), st));
   HB_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
 
@@ -300,15 +304,39 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
   // ---- initial state (_harmony/__init__.py:292-353) ------------------------
   HB_TRY(launch_l2_normalize<T, S>(X, n, d, d, Zn, P->ldz, st));
   HB_TRY(launch_l2_normalize<T, S>(Y0, K, d, d, Yn, P->ldy, st));
-  {
+  double* obj_init = w.obj_out + std::max(p.max_iter_clustering, 1);
+  constexpr bool tc_path = !std::is_same<S, float>::value && !std::is_same<S, double>::value;
+  // one persistent sweep (16-bit path) over `nblk` blocks of `idx`, objective into obj_dst
+  auto sweep = [&](const int32_t* idx, int64_t bs, int nb, const double* Omin, int init,
+                   double* obj_dst) -> int {
+    if constexpr (tc_path) {
+      SweepArgs sa{};
+      sa.Zn = Zn; sa.ldz = P->ldz; sa.R = R; sa.ldr = P->ldr; sa.cats = cats; sa.Yn = Yn; sa.ldy = P->ldy;
+      sa.idx = idx; sa.n = n; sa.bs = bs; sa.nblk = nb;
+      sa.Obuf[0] = w.O[0]; sa.Obuf[1] = w.O[1]; sa.Obuf[2] = w.O[2]; sa.b0 = ring.cur;
+      sa.Omin = Omin; sa.Pr = w.Pr; sa.theta = w.theta; sa.obj_acc = w.obj_acc; sa.obj_out = obj_dst;
+      sa.sigma = p.sigma; sa.d = d; sa.K = K; sa.B = B; sa.stabilized = p.stabilized_penalty;
+      sa.init_mode = init; sa.barrier = w.barrier; sa.err = w.err;
+      HB_CUDA(cudaMemsetAsync(w.barrier, 0, sizeof(unsigned), st));
+      HB_TRY(launch_tc_sweep<S>(sa, st));
+      ring.cur = (ring.cur + nb) % 3;
+      return HB_OK;
+    } else {
+      (void)idx; (void)bs; (void)nb; (void)Omin; (void)init; (void)obj_dst;
+      set_error("internal: sweep on the plain path");
+      return HB_ERR_INTERNAL;
+    }
+  };
+  if constexpr (tc_path) {
+    HB_TRY(sweep(nullptr, n, 1, nullptr, 1, obj_init));
+  } else {
     BlockArgs a = base;
     a.idx_new = nullptr; a.new_start = 0; a.n_new = n; a.Om_cur = nullptr; a.Om_next = nullptr;
     a.init_mode = 1;
     HB_TRY(ring.step<S>(a, st));
+    HB_TRY(launch_objective_finalize(ring.state(), w.Pr, w.theta, p.sigma, B, K, p.stabilized_penalty,
+                                     w.obj_acc, obj_init, st));
   }
-  double* obj_init = w.obj_out + std::max(p.max_iter_clustering, 1);
-  HB_TRY(launch_objective_finalize(ring.state(), w.Pr, w.theta, p.sigma, B, K, p.stabilized_penalty,
-                                   w.obj_acc, obj_init, st));
   double h_obj = 0;
   HB_CUDA(cudaMemcpyAsync(&h_obj, obj_init, sizeof(double), cudaMemcpyDeviceToHost, st));
   HB_CUDA(cudaStreamSynchronize(st));
@@ -360,14 +388,24 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
         // centroids Y = R^T Z_norm, L2-normalised (clustering.cu:272-281).  The pass walks
         // the block-ordered cell list, so it also sums every block's current rows per
         // batch: the "remove old contribution" terms of the sweep (clustering.cu:321-332).
-        const size_t omsz = (size_t)B * K;
+        const size_t omsz = (size_t)(B + 1) * K;
         HB_CUDA(cudaMemsetAsync(w.Omin, 0, sizeof(double) * nblk * omsz, st));
         int sp = span_begin(1, (double)n * (zb + rb + 8));
-        HB_TRY(launch_accum<S, S, TA>(R, P->ldr, Zn, P->ldz, idx, w.cen_chunks, P->cen_chunks, K, d,
-                                      (TA*)w.Ypart, st, OminArgs{w.Omin, cats, ml.bs, B}));
+        if constexpr (tc_path) {
+          CenArgs ca{Zn, P->ldz, R, P->ldr, cats, idx, n, ml.bs, d, K, B, (float*)w.Ypart, w.Omin, w.err};
+          HB_TRY(launch_tc_centroid<S>(ca, P->cen_chunks, st));
+        } else {
+          HB_TRY(launch_accum<S, S, TA>(R, P->ldr, Zn, P->ldz, idx, w.cen_chunks, P->cen_chunks, K, d,
+                                        (TA*)w.Ypart, st, OminArgs{w.Omin, cats, ml.bs, B}));
+        }
         HB_TRY(launch_centroid_reduce<TA, S>((TA*)w.Ypart, P->cen_chunks, K, d, Yn, P->ldy, st));
         span_end(sp);
         // sweep the blocks (clustering.cu:308-372)
+        if constexpr (tc_path) {
+          sp = span_begin(0, (double)n * (zb + rb + 8));
+          HB_TRY(sweep(idx, ml.bs, nblk, w.Omin, 0, w.obj_out + it));
+          span_end(sp);
+        } else {
         for (int j = 0; j < nblk; ++j) {
           BlockArgs a = base;
           const int64_t s0 = (int64_t)j * ml.bs;
@@ -381,6 +419,7 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
         }
         HB_TRY(launch_objective_finalize(ring.state(), w.Pr, w.theta, p.sigma, B, K,
                                          p.stabilized_penalty, w.obj_acc, w.obj_out + it, st));
+        }
         if (early_stop) {
           HB_CUDA(cudaMemcpyAsync(&h_obj, w.obj_out + it, sizeof(double), cudaMemcpyDeviceToHost, st));
           HB_CUDA(cudaStreamSynchronize(st));

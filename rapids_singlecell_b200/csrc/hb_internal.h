@@ -50,7 +50,8 @@ struct AccumChunk {  // a run of cells that all belong to batch `batch`
 };
 
 // Optional by-product of the centroid pass over a block-ordered cell list:
-// Omin[(pos / bs) * B + cats[cell]][k] += W[cell][k]  (float64, zeroed by the caller)
+// Omin[pos / bs][cats[cell]][k] += W[cell][k] and Omin[pos / bs][B][k] += W[cell][k]
+// (layout [nblk][B+1][K], float64, zeroed by the caller)
 struct OminArgs {
   double* Omin;
   const int32_t* cats;
@@ -108,6 +109,53 @@ template <typename H>
 int launch_tc_similarity(const H* Zn, int ldz, const H* Yn, int ldy, const int32_t* idx,
                          const int32_t* cats, int64_t n, int d, int K, float* S, int* err,
                          cudaStream_t st);
+
+struct SweepArgs {
+  const void* Zn;
+  int ldz;
+  void* R;
+  int ldr;
+  const int32_t* cats;
+  const void* Yn;
+  int ldy;
+  const int32_t* idx;      // block-ordered cell list (nullptr: identity, one block)
+  int64_t n, bs;
+  int nblk;
+  double* Obuf[3];
+  int b0;
+  const double* Omin;      // [nblk][B+1][K] old contribution per block (nullptr: none)
+  const double* Pr;
+  const double* theta;
+  double* obj_acc;         // running kmeans-error + entropy (zero on entry, zero on exit)
+  double* obj_out;         // objective of this iteration (written by CTA 0)
+  double sigma;
+  int d, K, B;
+  int stabilized;
+  int init_mode;
+  unsigned* barrier;       // zero on entry
+  int* err;
+};
+
+template <typename H>
+int launch_tc_sweep(const SweepArgs& a, cudaStream_t st);
+
+struct CenArgs {
+  const void* Zn;
+  int ldz;
+  const void* R;
+  int ldr;
+  const int32_t* cats;
+  const int32_t* idx;   // block-ordered cell list
+  int64_t n, bs;
+  int d, K, B;
+  float* P;             // [G][K][d] partial sums
+  double* Omin;         // [nblk][B+1][K]
+  int* err;
+};
+
+template <typename H>
+int launch_tc_centroid(const CenArgs& a, int grid, cudaStream_t st);
+int tc_centroid_grid(int K);
 
 struct CorrArgs {
   const double* M;      // [K][B+1][d]

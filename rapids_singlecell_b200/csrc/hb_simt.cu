@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(256) k_accum(const TS* __restrict__ W, int ldw
       if (pos + tid < ch.len) {
         const int64_t qq = ch.start + pos + tid;
         const int64_t cell = cell_index ? (int64_t)__ldg(cell_index + qq) : qq;
-        rkey = (int)(qq / om.bs) * om.B + __ldg(om.cats + cell);
+        rkey = (int)(qq / om.bs) * (om.B + 1) + __ldg(om.cats + cell);
       }
     }
 #pragma unroll
@@ -133,7 +133,11 @@ __global__ void __launch_bounds__(256) k_accum(const TS* __restrict__ W, int ldw
       for (int r = 0; r < nrow; ++r) {
         const int key = rkey_s[r];
         if (key != om_key) {
-          if (om_key >= 0) atomicAdd(&om.Omin[(size_t)om_key * K + k0 + tid], om_acc);
+          if (om_key >= 0) {
+            atomicAdd(&om.Omin[(size_t)om_key * K + k0 + tid], om_acc);
+            const int sum_row = om_key - om_key % (om.B + 1) + om.B;
+            atomicAdd(&om.Omin[(size_t)sum_row * K + k0 + tid], om_acc);
+          }
           om_key = key;
           om_acc = 0.0;
         }
@@ -153,8 +157,11 @@ __global__ void __launch_bounds__(256) k_accum(const TS* __restrict__ W, int ldw
         for (int b = 0; b < 4; ++b) acc[a][b] += wv[a] * vv[b];
     }
   }
-  if (do_om && om_key >= 0 && tid < ACC_BK && k0 + tid < K)
+  if (do_om && om_key >= 0 && tid < ACC_BK && k0 + tid < K) {
     atomicAdd(&om.Omin[(size_t)om_key * K + k0 + tid], om_acc);
+    const int sum_row = om_key - om_key % (om.B + 1) + om.B;
+    atomicAdd(&om.Omin[(size_t)sum_row * K + k0 + tid], om_acc);
+  }
   TA* out = P + (size_t)blockIdx.x * K * d;
 #pragma unroll
   for (int a = 0; a < 8; ++a) {

@@ -19,8 +19,8 @@
 namespace hb {
 
 struct CenLayout {
-  int npad, nbB, tcols;
-  uint32_t offA[2], offB[2], offCid, offCat, offMisc, bytes;
+  int npad, nbB, tcols, stages;
+  uint32_t offA[3], offB[3], offCid, offCat, offMisc, bytes;
 };
 
 inline CenLayout cen_layout(int K) {
@@ -28,15 +28,19 @@ inline CenLayout cen_layout(int K) {
   L.npad = (K + 15) / 16 * 16;
   L.nbB = (L.npad + 63) / 64;
   L.tcols = L.npad <= 128 ? 128 : 256;
-  uint32_t o = 0;
-  for (int s = 0; s < 2; ++s) { L.offA[s] = o; o += 2u * 16384u; }
-  for (int s = 0; s < 2; ++s) { L.offB[s] = o; o += (uint32_t)L.nbB * 16384u; }
-  L.offCid = o; o += 2u * 128u * 4u;
-  L.offCat = o; o += 2u * 128u * 4u;
-  L.offMisc = o; o += 16u;
-  // 8 KB of slack: reads stay inside the allocation under either reading of the
-  // descriptor's leading / stride offsets (see the layout note above)
-  L.bytes = o + 8192u + 1024u;
+  for (int st = 3; st >= 2; --st) {  // as many stages as fit: st-1 gathers in flight
+    uint32_t o = 0;
+    for (int s = 0; s < 3; ++s) { L.offA[s] = o; if (s < st) o += 2u * 16384u; }
+    for (int s = 0; s < 3; ++s) { L.offB[s] = o; if (s < st) o += (uint32_t)L.nbB * 16384u; }
+    L.offCid = o; o += 4u * 128u * 4u;   // id ring: stages + 1 slots
+    L.offCat = o; o += 4u * 128u * 4u;
+    L.offMisc = o; o += 16u;
+    // 8 KB of slack: reads stay inside the allocation under either reading of the
+    // descriptor's leading / stride offsets (see the layout note above)
+    L.bytes = o + 8192u + 1024u;
+    L.stages = st;
+    if (L.bytes <= 227u * 1024u) break;
+  }
   return L;
 }
 
@@ -45,32 +49,37 @@ __device__ __forceinline__ uint32_t mn_off(uint32_t r, uint32_t nb, uint32_t c8,
   return (r >> 3) * (nblocks * 1024u) + nb * 1024u + (r & 7u) * 128u + ((c8 ^ (r & 7u)) << 4);
 }
 
+// Cell ids and (block, batch) keys of one tile: one coalesced list read.
+__device__ __forceinline__ void cen_load_ids(const CenArgs& a, int64_t pos, int nr, int* cid, int* key) {
+  const int r = threadIdx.x;
+  if (r < 128) {
+    const int64_t cell = r < nr ? (int64_t)__ldg(a.idx + pos + r) : -1;
+    cid[r] = (int)cell;
+    key[r] = cell >= 0 ? (int)((pos + r) / a.bs) * (a.B + 1) + __ldg(a.cats + cell) : -1;
+  }
+}
+
+// Copies of one tile from ids already in shared memory; consecutive lanes copy
+// consecutive 16-byte chunks of the same rows.
 template <typename H>
-__device__ __forceinline__ void cen_gather(const CenArgs& a, const CenLayout& L, int64_t pos, int nr,
-                                           uint32_t sA, uint32_t sB, int* cid, int* ccat) {
-  // thread t owns row t % 128 and every other chunk of it (one cell-id load per thread)
+__device__ __forceinline__ void cen_copy(const CenArgs& a, const CenLayout& L, uint32_t sA, uint32_t sB,
+                                         const int* cid) {
   const H* Zn = (const H*)a.Zn;
   const H* R = (const H*)a.R;
   const int zch = 16;             // 128 PCs (zero-padded) = 16 chunks, 2 blocks
-  const int rch = L.nbB * 8;      // cluster chunks
-  const int r = threadIdx.x & 127, part = threadIdx.x >> 7, nparts = blockDim.x >> 7;
-  const int64_t cell = r < nr ? (int64_t)__ldg(a.idx + pos + r) : -1;
-  if (part == 0) {
-    cid[r] = (int)cell;
-    ccat[r] = cell >= 0 ? __ldg(a.cats + cell) : 0;
-  }
-  const H* zs = cell >= 0 ? Zn + cell * a.ldz : Zn;
-  const H* rs = cell >= 0 ? R + cell * a.ldr : R;
-  for (int ch = part; ch < zch + rch; ch += nparts) {
+  const int nch = zch + L.nbB * 8;
+  for (int e = threadIdx.x; e < 128 * nch; e += blockDim.x) {
+    const int r = e / nch, ch = e % nch;
+    const int64_t cell = cid[r];
     if (ch < zch) {
       const bool ok = cell >= 0 && ch * 8 < a.ldz;
-      tc::cp_async16(sA + mn_off(r, ch >> 3, ch & 7, 2), ok ? (const void*)(zs + ch * 8) : (const void*)Zn,
-                     ok ? 16u : 0u);
+      tc::cp_async16(sA + mn_off(r, ch >> 3, ch & 7, 2),
+                     ok ? (const void*)(Zn + cell * a.ldz + ch * 8) : (const void*)Zn, ok ? 16u : 0u);
     } else {
       const int c = ch - zch;
       const bool ok = cell >= 0 && c * 8 < a.ldr;
-      tc::cp_async16(sB + mn_off(r, c >> 3, c & 7, L.nbB), ok ? (const void*)(rs + c * 8) : (const void*)R,
-                     ok ? 16u : 0u);
+      tc::cp_async16(sB + mn_off(r, c >> 3, c & 7, L.nbB),
+                     ok ? (const void*)(R + cell * a.ldr + c * 8) : (const void*)R, ok ? 16u : 0u);
     }
   }
 }
@@ -85,8 +94,11 @@ __global__ void __launch_bounds__(256, 1) k_tc_centroid(CenArgs a, CenLayout L) 
   int* ccat = (int*)(sm + L.offCat);
   uint64_t* mbar = (uint64_t*)(sm + L.offMisc);
   uint32_t* tmem_slot = (uint32_t*)(sm + L.offMisc + 8);
-  const uint32_t sA[2] = {tc::smem_u32(sm + L.offA[0]), tc::smem_u32(sm + L.offA[1])};
-  const uint32_t sB[2] = {tc::smem_u32(sm + L.offB[0]), tc::smem_u32(sm + L.offB[1])};
+  const uint32_t sA[3] = {tc::smem_u32(sm + L.offA[0]), tc::smem_u32(sm + L.offA[1]),
+                          tc::smem_u32(sm + L.offA[2])};
+  const uint32_t sB[3] = {tc::smem_u32(sm + L.offB[0]), tc::smem_u32(sm + L.offB[1]),
+                          tc::smem_u32(sm + L.offB[2])};
+  const int S = L.stages;
   const int64_t lo = a.n * blockIdx.x / gridDim.x, hi = a.n * (blockIdx.x + 1) / gridDim.x;
   const int ntiles = (int)((hi - lo + 127) / 128);
 
@@ -99,8 +111,16 @@ __global__ void __launch_bounds__(256, 1) k_tc_centroid(CenArgs a, CenLayout L) 
     tc::mbar_init(mbar, 1);
     tc::fence_mbar_init();
   }
-  if (ntiles > 0) cen_gather<H>(a, L, lo, (int)(hi - lo < 128 ? hi - lo : 128), sA[0], sB[0], cid, ccat);
+  const int SI = S + 1;  // id ring slots
+  auto tile_rows = [&](int t) { const int64_t p = lo + (int64_t)t * 128; return (int)(hi - p < 128 ? hi - p : 128); };
+  // prologue: ids of the first S tiles, copies of the first S-1 (one cp.async group each)
+  for (int t = 0; t < S; ++t)
+    if (t < ntiles) cen_load_ids(a, lo + (int64_t)t * 128, tile_rows(t), cid + t * 128, ccat + t * 128);
   __syncthreads();
+  for (int t = 0; t < S - 1; ++t) {
+    if (t < ntiles) cen_copy<H>(a, L, sA[t], sB[t], cid + t * 128);
+    tc::cp_async_commit();
+  }
   tc::fence_after_sync();
   const uint32_t tmem = *tmem_slot;
   const uint32_t idesc = tc::idesc_f16(128, L.npad, is_bf16<H>::value, true, true);
@@ -110,15 +130,16 @@ __global__ void __launch_bounds__(256, 1) k_tc_centroid(CenArgs a, CenLayout L) 
   const int kcol = tid % ncol, rhalf = tid / ncol;
   const int nhalves = 256 / ncol;
   const bool owner = kcol < K;
-  double om_acc = 0.0;
+  float om_acc = 0.f;   // current run, this 8-row group
+  double om_tot = 0.0;  // current run, earlier groups (float64 keeps long runs exact enough)
   int om_key = -1;
   uint32_t phase = 0;
 
   for (int t = 0; t < ntiles; ++t) {
-    const int buf = t & 1;
+    const int buf = t % S;
     const int64_t pos = lo + (int64_t)t * 128;
     const int nr = (int)(hi - pos < 128 ? hi - pos : 128);
-    tc::cp_async_wait_all();
+    if (S == 3) tc::cp_async_wait_group<1>(); else tc::cp_async_wait_group<0>();
     tc::fence_proxy_async_smem();
     tc::fence_before_sync();
     __syncthreads();
@@ -132,43 +153,57 @@ __global__ void __launch_bounds__(256, 1) k_tc_centroid(CenArgs a, CenLayout L) 
       }
       tc::mma_commit(mbar);
     }
-    if (t + 1 < ntiles)
-      cen_gather<H>(a, L, pos + 128, (int)(hi - pos - 128 < 128 ? hi - pos - 128 : 128), sA[buf ^ 1], sB[buf ^ 1],
-                    cid + (buf ^ 1) * 128, ccat + (buf ^ 1) * 128);
-    // per-(block, batch) row sums of R from the staged tile (the block changes at
-    // most where the list position crosses a multiple of bs)
+    {
+      const int tn = t + S - 1, bn = tn % S;  // refill the stage freed by tile t-1
+      if (tn < ntiles) cen_copy<H>(a, L, sA[bn], sB[bn], cid + (tn % SI) * 128);
+      tc::cp_async_commit();
+      const int ti = t + S;  // ids two steps ahead, into the slot tile t-1 used
+      if (ti < ntiles) cen_load_ids(a, lo + (int64_t)ti * 128, tile_rows(ti), cid + (ti % SI) * 128,
+                                    ccat + (ti % SI) * 128);
+    }
+    // per-(block, batch) row sums of R from the staged tile; the row keys were
+    // stored by the gather, swizzle offsets of the 8 rows of a group are fixed
     if (owner) {
-      const unsigned char* tb = sm + L.offB[buf];
-      const int nb = kcol >> 6, c8 = (kcol & 63) >> 3, w8 = kcol & 7;
-      const int r0 = rhalf * (128 / nhalves), r1 = min(nr, r0 + 128 / nhalves);
-      if (r0 < r1) {
-        int blk = (int)((pos + r0) / a.bs);
-        int64_t next_edge = (int64_t)(blk + 1) * a.bs;
-        for (int r = r0; r < r1; ++r) {
-          if (pos + r >= next_edge) {
-            ++blk;
-            next_edge += a.bs;
-          }
-          const int key = blk * (a.B + 1) + ccat[buf * 128 + r];
-          if (key != om_key) {
-            if (om_key >= 0) {
-              atomicAdd(&a.Omin[(size_t)om_key * K + kcol], om_acc);
-              atomicAdd(&a.Omin[(size_t)(om_key - om_key % (a.B + 1) + a.B) * K + kcol], om_acc);
+      const int* keys = ccat + (t % SI) * 128;
+      const unsigned char* tb = sm + L.offB[buf] + (kcol >> 6) * 1024 + (kcol & 7) * 2;
+      const uint32_t gstride = (uint32_t)L.nbB * 1024u;
+      const int c8 = (kcol & 63) >> 3;
+      uint32_t tab[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) tab[i] = (uint32_t)i * 128u + ((uint32_t)(c8 ^ i) << 4);
+      const int rows_per = 128 / nhalves;
+      const int r0 = rhalf * rows_per, r1 = min(nr, r0 + rows_per);
+      for (int g = r0; g < r1; g += 8) {
+        const unsigned char* gb = tb + (uint32_t)(g >> 3) * gstride;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const int r = g + i;
+          if (r < r1) {
+            const int key = keys[r];
+            if (key != om_key) {
+              if (om_key >= 0) {
+                const double v = om_tot + (double)om_acc;
+                atomicAdd(&a.Omin[(size_t)om_key * K + kcol], v);
+                atomicAdd(&a.Omin[(size_t)(om_key - om_key % (a.B + 1) + a.B) * K + kcol], v);
+              }
+              om_key = key;
+              om_acc = 0.f;
+              om_tot = 0.0;
             }
-            om_key = key;
-            om_acc = 0.0;
+            om_acc += h2f(*(const H*)(gb + tab[i]));
           }
-          const H* p = (const H*)(tb + mn_off(r, nb, c8, L.nbB)) + w8;
-          om_acc += (double)h2f(*p);
         }
+        om_tot += (double)om_acc;
+        om_acc = 0.f;
       }
     }
     if (!tc::mbar_wait(mbar, phase, kMaxPolls)) atomicExch(a.err, 4);
     phase ^= 1u;
   }
   if (owner && om_key >= 0) {
-    atomicAdd(&a.Omin[(size_t)om_key * K + kcol], om_acc);
-    atomicAdd(&a.Omin[(size_t)(om_key - om_key % (a.B + 1) + a.B) * K + kcol], om_acc);
+    const double v = om_tot + (double)om_acc;
+    atomicAdd(&a.Omin[(size_t)om_key * K + kcol], v);
+    atomicAdd(&a.Omin[(size_t)(om_key - om_key % (a.B + 1) + a.B) * K + kcol], v);
   }
   tc::fence_after_sync();
   // partial D[pc][cluster] -> P[cta][cluster][pc]; lane = PC, warps 0-3 / 4-7 split the columns

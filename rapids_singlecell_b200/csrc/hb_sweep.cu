@@ -93,8 +93,11 @@ __device__ __forceinline__ void gather_item(const SweepArgs& a, const Cursor& cu
                        cid, ccat, a.cats);
 }
 
-template <typename H>
-__global__ void __launch_bounds__(256, 1) k_tc_sweep(SweepArgs a, TcLayout L) {
+// NT = 256: warps 0-3 and 4-7 take the two column halves of the same 128 rows
+// (one CTA per SM).  NT = 128: each thread owns a full row; used when two CTAs
+// fit on an SM so that one CTA's latency chain overlaps the other's.
+template <typename H, int NT>
+__global__ void __launch_bounds__(NT, 1) k_tc_sweep(SweepArgs a, TcLayout L) {
   extern __shared__ __align__(1024) unsigned char smem_dyn[];
   unsigned char* sm = (unsigned char*)(((uintptr_t)smem_dyn + 1023) & ~(uintptr_t)1023);
   const int K = a.K, B = a.B;
@@ -110,7 +113,7 @@ __global__ void __launch_bounds__(256, 1) k_tc_sweep(SweepArgs a, TcLayout L) {
   double* red = (double*)(sm + L.offMisc + 16);
   __shared__ float dsum[256];             // column sums of the delta (row B)
   __shared__ double ocol[256];            // column sums of the state
-  __shared__ int crange[2];
+  __shared__ int2 crange[kMaxBlocks];    // batch range of this CTA's slice, per block
   __shared__ int runs[130];               // tile run starts (batch changes), terminated by nrows
   __shared__ int nruns;
   H* R = (H*)a.R;
@@ -138,14 +141,26 @@ __global__ void __launch_bounds__(256, 1) k_tc_sweep(SweepArgs a, TcLayout L) {
   const uint32_t idesc = tc::idesc_f16(128, L.npad, is_bf16<H>::value, false, false);
   const float c2 = (float)(-2.0 / a.sigma * 1.4426950408889634);  // exp(x) = exp2(x log2 e)
   const float sig = (float)a.sigma;
-  const int half = warp >> 2;
+  const int half = NT == 256 ? warp >> 2 : 0;
   const int row = (warp & 3) * 32 + lane;
   const uint32_t tl = tmem + ((uint32_t)((warp & 3) * 32) << 16);
-  const int nh = (L.npad / 2 + 7) / 8 * 8;
+  const int nh = NT == 256 ? (L.npad / 2 + 7) / 8 * 8 : L.npad;
   const int c_lo = half * nh, c_hi = min(L.npad, c_lo + nh);
   double obj_local = 0.0;
   uint32_t phase = 0;
   int buf = 0;
+  bool pre_issued = false;  // the MMA of the current tile was issued before the last barrier
+  // batch range of every block's slice (the list is ordered by batch within a block)
+  for (int j = tid; j < a.nblk; j += NT) {
+    int64_t lo, hi;
+    slice_of(a, j, blockIdx.x, gridDim.x, lo, hi);
+    int cmin = 0, cmax = B - 1;
+    if (a.idx && lo < hi) {
+      cmin = __ldg(a.cats + __ldg(a.idx + lo));
+      cmax = __ldg(a.cats + __ldg(a.idx + hi - 1));
+    }
+    crange[j] = make_int2(cmin, lo < hi ? cmax : cmin - 1);
+  }
 
   for (int j = 0; j < a.nblk; ++j) {
     const double* Oin = a.Obuf[(a.b0 + j) % 3];
@@ -155,27 +170,17 @@ __global__ void __launch_bounds__(256, 1) k_tc_sweep(SweepArgs a, TcLayout L) {
     const double* Omn = (a.Omin && j + 1 < a.nblk) ? a.Omin + (size_t)(j + 1) * ldo : nullptr;  // next
     int64_t lo, hi;
     slice_of(a, j, blockIdx.x, gridDim.x, lo, hi);
-    for (size_t e = (size_t)blockIdx.x * 256 + tid; e < ldo; e += (size_t)gridDim.x * 256) Ozero[e] = 0.0;
-    // batch range of this CTA's slice (the list is ordered by batch within a block)
-    if (tid == 0) {
-      int cmin = 0, cmax = B - 1;
-      if (a.idx && lo < hi) {
-        cmin = __ldg(a.cats + __ldg(a.idx + lo));
-        cmax = __ldg(a.cats + __ldg(a.idx + hi - 1));
-      }
-      crange[0] = cmin;
-      crange[1] = lo < hi ? cmax : cmin - 1;
-    }
-    for (int k = tid; k < K; k += 256) {
+    for (size_t e = (size_t)blockIdx.x * NT + tid; e < ldo; e += (size_t)gridDim.x * NT) Ozero[e] = 0.0;
+    for (int k = tid; k < K; k += NT) {
       double s = Oin[(size_t)B * K + k];
       if (Omc) s -= Omc[(size_t)B * K + k];
       ocol[k] = s;
       dsum[k] = 0.f;
     }
     __syncthreads();
-    const int cmin = crange[0], cmax = crange[1];
+    const int cmin = crange[j].x, cmax = crange[j].y;
     // penalty rows of the batches present (kernels_pen.cuh:8-21); zero the delta rows
-    for (int e = tid; e < (cmax - cmin + 1) * K; e += 256) {
+    for (int e = tid; e < (cmax - cmin + 1) * K; e += NT) {
       const int b = cmin + e / K, k = e % K;
       const size_t o_at = (size_t)b * K + k;
       osm[o_at] = 0.f;
@@ -188,11 +193,16 @@ __global__ void __launch_bounds__(256, 1) k_tc_sweep(SweepArgs a, TcLayout L) {
     }
     // ---- tiles of this block ------------------------------------------------
     while (have && cu.j == j) {
-      tc::cp_async_wait_all();
-      tc::fence_proxy_async_smem();
-      tc::fence_before_sync();
-      __syncthreads();
-      if (tid == 0) issue_similarity_mma(tmem, sA[buf], sB, L, idesc, mbar);
+      if (!pre_issued) {
+        tc::cp_async_wait_all();
+        tc::fence_proxy_async_smem();
+        tc::fence_before_sync();
+        __syncthreads();
+        if (tid == 0) issue_similarity_mma(tmem, sA[buf], sB, L, idesc, mbar);
+      } else {
+        __syncthreads();  // penalty rows of this block are complete
+      }
+      pre_issued = false;
       Cursor nx;
       const bool have_nx = cursor_next(a, cu, nx);
       if (have_nx) gather_item<H>(a, nx, sA[buf ^ 1], L, cid + (buf ^ 1) * 128, ccat + (buf ^ 1) * 128);
@@ -232,7 +242,7 @@ __global__ void __launch_bounds__(256, 1) k_tc_sweep(SweepArgs a, TcLayout L) {
       }
       km *= 2.f;
       tc::tmem_st_wait();
-      rsp[half * 128 + row] = rs;
+      if (NT == 256) rsp[half * 128 + row] = rs;
       // run starts of equal batch inside the tile (rows are ordered by batch)
       if (warp == 0) {
         int cnt = 0;
@@ -249,7 +259,7 @@ __global__ void __launch_bounds__(256, 1) k_tc_sweep(SweepArgs a, TcLayout L) {
         }
       }
       __syncthreads();
-      const float rsum = rsp[row] + rsp[128 + row];
+      const float rsum = NT == 256 ? rsp[row] + rsp[128 + row] : rs;
       const float inv = a.init_mode ? 1.f / fmaxf(rsum, 1e-12f) : 1.f / rsum;
       // pass 2: normalise, round to 16 bits, stage the row, entropy term (lg2 on the SFU)
       float ent = 0.f;
@@ -275,27 +285,27 @@ __global__ void __launch_bounds__(256, 1) k_tc_sweep(SweepArgs a, TcLayout L) {
       if (cell >= 0) obj_local += (double)(inv * km) + (double)(sig * ent);
       __syncthreads();
       // observed-count delta: one thread per cluster column, summed per batch run
-      if (tid < K) {
+      for (int kc = tid; kc < K; kc += NT) {
         float tot = 0.f;
         for (int q = 0; q < nruns; ++q) {
           const int r0 = runs[q], r1 = runs[q + 1];
           float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
           int r = r0;
           for (; r + 4 <= r1; r += 4) {
-            s0 += h2f(Rst[(r + 0) * L.ldst + tid]);
-            s1 += h2f(Rst[(r + 1) * L.ldst + tid]);
-            s2 += h2f(Rst[(r + 2) * L.ldst + tid]);
-            s3 += h2f(Rst[(r + 3) * L.ldst + tid]);
+            s0 += h2f(Rst[(r + 0) * L.ldst + kc]);
+            s1 += h2f(Rst[(r + 1) * L.ldst + kc]);
+            s2 += h2f(Rst[(r + 2) * L.ldst + kc]);
+            s3 += h2f(Rst[(r + 3) * L.ldst + kc]);
           }
-          for (; r < r1; ++r) s0 += h2f(Rst[r * L.ldst + tid]);
+          for (; r < r1; ++r) s0 += h2f(Rst[r * L.ldst + kc]);
           const float srun = (s0 + s1) + (s2 + s3);
-          osm[ccat[buf * 128 + r0] * K + tid] += srun;
+          osm[ccat[buf * 128 + r0] * K + kc] += srun;
           tot += srun;
         }
-        dsum[tid] += tot;
+        dsum[kc] += tot;
       }
       // write the new assignment rows
-      for (int e = tid; e < nvalid * L.ldr_chunks; e += 256) {
+      for (int e = tid; e < nvalid * L.ldr_chunks; e += NT) {
         const int r = e / L.ldr_chunks, ch = e % L.ldr_chunks;
         const int64_t cl = cid[buf * 128 + r];
         *(uint4*)(R + cl * a.ldr + ch * 8) = *(const uint4*)(Rst + r * L.ldst + ch * 8);
@@ -306,20 +316,29 @@ __global__ void __launch_bounds__(256, 1) k_tc_sweep(SweepArgs a, TcLayout L) {
     }
     // ---- flush this CTA's delta and carry the state (CTA 0) ----------------------
     __syncthreads();
-    for (int e = tid; e < (cmax - cmin + 1) * K; e += 256) {
+    for (int e = tid; e < (cmax - cmin + 1) * K; e += NT) {
       const size_t o_at = (size_t)cmin * K + e;
       const double v = (double)osm[o_at];
       if (v != 0.0) atomicAdd(&Oout[o_at], v);
     }
-    for (int k = tid; k < K; k += 256)
+    for (int k = tid; k < K; k += NT)
       if (dsum[k] != 0.f) atomicAdd(&Oout[(size_t)B * K + k], (double)dsum[k]);
-    if (blockIdx.x == 0) {
-      for (size_t e = tid; e < ldo; e += 256) {
-        double v = Oin[e];
-        if (Omc) v -= Omc[e];
-        if (Omn) v -= Omn[e];
-        if (v != 0.0) atomicAdd(&Oout[e], v);
-      }
+    // carry the state forward (O_in - old(this block) - old(next block)), spread over the CTAs
+    for (size_t e = ldo * blockIdx.x / gridDim.x + tid; e < ldo * (blockIdx.x + 1) / gridDim.x; e += NT) {
+      double v = Oin[e];
+      if (Omc) v -= Omc[e];
+      if (Omn) v -= Omn[e];
+      if (v != 0.0) atomicAdd(&Oout[e], v);
+    }
+    // the similarity of the next block's first tile does not depend on the counts:
+    // start it before the barrier
+    if (have && cu.j == j + 1) {
+      tc::cp_async_wait_all();
+      tc::fence_proxy_async_smem();
+      tc::fence_before_sync();
+      __syncthreads();
+      if (tid == 0) issue_similarity_mma(tmem, sA[buf], sB, L, idesc, mbar);
+      pre_issued = true;
     }
     if (j == a.nblk - 1) {
       const double tot = block_sum(obj_local, red);
@@ -332,7 +351,7 @@ __global__ void __launch_bounds__(256, 1) k_tc_sweep(SweepArgs a, TcLayout L) {
   if (blockIdx.x == 0) {
     const double* Of = a.Obuf[(a.b0 + a.nblk) % 3];
     double acc = 0.0;
-    for (int e = tid; e < B * K; e += 256) {
+    for (int e = tid; e < B * K; e += NT) {
       const int b = e / K, k = e % K;
       const double o = Of[e];
       const double E = a.Pr[b] * Of[(size_t)B * K + k];
@@ -353,23 +372,22 @@ __global__ void __launch_bounds__(256, 1) k_tc_sweep(SweepArgs a, TcLayout L) {
   }
 }
 
-template <typename H>
-int launch_tc_sweep(const SweepArgs& a, cudaStream_t st) {
-  const TcLayout L = tc_layout(a.d, a.K, a.B, a.ldr, 4);
-  if (L.bytes > 227u * 1024u) {
-    set_error("tensor-core sweep: shared-memory tables too large (B=%d K=%d d=%d)", a.B, a.K, a.d);
-    return HB_ERR_UNSUPPORTED;
-  }
-  const void* fn = (const void*)k_tc_sweep<H>;
-  // residency: limited by shared memory and by the 512 TMEM columns of an SM
-  const int occ_tmem = std::max(1, 512 / L.tcols);
+template <typename H, int NT>
+static int launch_sweep_nt(const SweepArgs& a, const TcLayout& L, int occ_target, cudaStream_t st) {
+  const void* fn = (const void*)k_tc_sweep<H, NT>;
+  cudaFuncAttributes fa;
+  HB_CUDA(cudaFuncGetAttributes(&fa, fn));
+  const size_t stat = fa.sharedSizeBytes;  // static shared memory of the kernel
   size_t smem = L.bytes;
   const size_t per_sm = 228u * 1024u;
-  if (per_sm / (smem + 1024) > (size_t)occ_tmem) smem = std::min<size_t>(227u * 1024u, per_sm / occ_tmem - 2048);
+  // pad the request so that no more than occ_target CTAs share an SM (TMEM budget)
+  if (per_sm / (smem + stat + 1024) > (size_t)occ_target)
+    smem = std::min<size_t>(227u * 1024u - stat, per_sm / occ_target - stat - 2048);
+  if (smem < L.bytes) smem = L.bytes;
   HB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int occ = 0;
-  HB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 256, smem));
-  occ = std::min(occ, occ_tmem);
+  HB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, NT, smem));
+  occ = std::min(occ, occ_target);
   if (occ < 1) {
     set_error("tensor-core sweep: kernel does not fit on an SM");
     return HB_ERR_UNSUPPORTED;
@@ -379,9 +397,19 @@ int launch_tc_sweep(const SweepArgs& a, cudaStream_t st) {
   SweepArgs args = a;
   TcLayout lay = L;
   void* kargs[] = {(void*)&args, (void*)&lay};
-  HB_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(256), kargs, smem, st));
+  HB_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(NT), kargs, smem, st));
   ++g_launches;
   return HB_OK;
+}
+
+template <typename H>
+int launch_tc_sweep(const SweepArgs& a, cudaStream_t st) {
+  const TcLayout L = tc_layout(a.d, a.K, a.B, a.ldr, 4);
+  if (L.bytes > 227u * 1024u) {
+    set_error("tensor-core sweep: shared-memory tables too large (B=%d K=%d d=%d)", a.B, a.K, a.d);
+    return HB_ERR_UNSUPPORTED;
+  }
+  return launch_sweep_nt<H, 256>(a, L, std::max(1, 512 / L.tcols), st);
 }
 template int launch_tc_sweep<__half>(const SweepArgs&, cudaStream_t);
 template int launch_tc_sweep<__nv_bfloat16>(const SweepArgs&, cudaStream_t);

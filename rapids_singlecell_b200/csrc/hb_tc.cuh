@@ -142,6 +142,11 @@ __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32
                : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
 // byte offset of 16-byte chunk `ch` (0..7) of row `r` inside 128B-swizzled 8-row atoms
 __host__ __device__ __forceinline__ uint32_t sw128_off(uint32_t r, uint32_t ch) {

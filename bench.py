@@ -46,7 +46,27 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="bf16", choices=["bf16", "fp16", "fp32"])
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="one short run for ncu: 200,000 cells of the same workload, 1 outer x 2 "
+                         "k-means iterations, then exit")
     return ap.parse_args()
+
+
+def run_profile_case(args):
+    import torch
+
+    from rapids_singlecell_b200.harmony import HarmonyProblem
+    from rapids_singlecell_b200.synthetic import make_config
+
+    cfg = make_config(WORKLOAD, seed=0, n_cells=200_000)
+    X = torch.as_tensor(cfg["Z"], device="cuda")
+    prob = HarmonyProblem(X, cfg["cats"], cfg["n_batches"], torch.as_tensor(cfg["Y0"], device="cuda"),
+                          np.full(cfg["n_batches"], 2.0), precision=args.precision,
+                          n_clusters=cfg["n_clusters"], max_iter_harmony=1, max_iter_clustering=2,
+                          tol_harmony=-np.inf, tol_clustering=-np.inf)
+    _, info = prob.run(profile=True)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_case": info.profile}))
 
 
 def dist_env():
@@ -323,7 +343,9 @@ def run_ours(args):
 
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.profile_case:
+        run_profile_case(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

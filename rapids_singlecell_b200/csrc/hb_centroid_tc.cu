@@ -49,58 +49,141 @@ __device__ __forceinline__ uint32_t mn_off(uint32_t r, uint32_t nb, uint32_t c8,
   return (r >> 3) * (nblocks * 1024u) + nb * 1024u + (r & 7u) * 128u + ((c8 ^ (r & 7u)) << 4);
 }
 
-// Cell ids and (block, batch) keys of one tile: one coalesced list read.
-__device__ __forceinline__ void cen_load_ids(const CenArgs& a, int64_t pos, int nr, int* cid, int* key) {
-  const int r = threadIdx.x;
-  if (r < 128) {
-    const int64_t cell = r < nr ? (int64_t)__ldg(a.idx + pos + r) : -1;
-    cid[r] = (int)cell;
-    key[r] = cell >= 0 ? (int)((pos + r) / a.bs) * (a.B + 1) + __ldg(a.cats + cell) : -1;
+// Producer (warp 0): gather tile `t` into stage `s`.  Lane q takes rows 4q..4q+3:
+// it reads their cell ids and batches, records the (block, batch) key of each row,
+// and issues one TMA gather of 4 rows per 64-element block of Z_norm and of R.
+// Rows past the slice use row index n (out of range: zero fill).
+__device__ __forceinline__ void cen_produce(const CenArgs& a, const CenLayout& L, const CUtensorMap* tmZ,
+                                            const CUtensorMap* tmR, int64_t pos, int nr, uint32_t sA,
+                                            uint32_t sB, uint64_t* full, int* key, int* runs) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t bytes = 32u * (uint32_t)(2 + L.nbB) * 512u;
+  int rows[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = lane * 4 + i;
+    int cell = (int)a.n;  // out of range -> zeros
+    int k = -1;
+    if (r < nr) {
+      cell = __ldg(a.idx + pos + r);
+      k = (int)((pos + r) / a.bs) * (a.B + 1) + __ldg(a.cats + cell);
+    }
+    rows[i] = cell;
+    key[r] = k;
   }
+  // run starts (rows whose key differs from the previous row's), compacted in
+  // ascending row order: round i looks at rows 32 i + lane.
+  // runs[0] = count, runs[1..count] = starts, runs[count+1] = nr
+  __syncwarp();
+  int cnt = 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = i * 32 + lane;
+    const bool start = r < nr && (r == 0 || key[r] != key[r - 1]);
+    const unsigned m = __ballot_sync(0xffffffffu, start);
+    if (start) runs[1 + cnt + __popc(m & ((1u << lane) - 1u))] = r;
+    cnt += __popc(m);
+  }
+  if (lane == 0) {
+    runs[0] = cnt;
+    runs[1 + cnt] = nr;
+  }
+  // keys and runs are published by the arrive (release) that follows them
+  __syncwarp();
+  if (lane == 0) tc::mbar_arrive_expect_tx(full, bytes);
+  __syncwarp();
+  tc::fence_proxy_async_smem();
+  const uint32_t g = (uint32_t)(lane >> 1), ro = (uint32_t)(lane & 1) * 512u;  // 8-row group, half
+#pragma unroll
+  for (int nb = 0; nb < 2; ++nb)
+    tc::tma_gather4(sA + g * 2048u + (uint32_t)nb * 1024u + ro, tmZ, nb * 64, rows[0], rows[1], rows[2],
+                    rows[3], full);
+  for (int nb = 0; nb < L.nbB; ++nb)
+    tc::tma_gather4(sB + g * (uint32_t)L.nbB * 1024u + (uint32_t)nb * 1024u + ro, tmR, nb * 64, rows[0],
+                    rows[1], rows[2], rows[3], full);
 }
 
-// Copies of one tile from ids already in shared memory; consecutive lanes copy
-// consecutive 16-byte chunks of the same rows.
-template <typename H>
-__device__ __forceinline__ void cen_copy(const CenArgs& a, const CenLayout& L, uint32_t sA, uint32_t sB,
-                                         const int* cid) {
-  const H* Zn = (const H*)a.Zn;
-  const H* R = (const H*)a.R;
-  const int zch = 16;             // 128 PCs (zero-padded) = 16 chunks, 2 blocks
-  const int nch = zch + L.nbB * 8;
-  for (int e = threadIdx.x; e < 128 * nch; e += blockDim.x) {
-    const int r = e / nch, ch = e % nch;
-    const int64_t cell = cid[r];
-    if (ch < zch) {
-      const bool ok = cell >= 0 && ch * 8 < a.ldz;
-      tc::cp_async16(sA + mn_off(r, ch >> 3, ch & 7, 2),
-                     ok ? (const void*)(Zn + cell * a.ldz + ch * 8) : (const void*)Zn, ok ? 16u : 0u);
-    } else {
-      const int c = ch - zch;
-      const bool ok = cell >= 0 && c * 8 < a.ldr;
-      tc::cp_async16(sB + mn_off(r, c >> 3, c & 7, L.nbB),
-                     ok ? (const void*)(R + cell * a.ldr + c * 8) : (const void*)R, ok ? 16u : 0u);
+// Warp roles: warp 0 produces (ids, keys, TMA gathers), lane 0 of warp 1 issues the
+// MMAs, warps 2-7 (192 threads) consume the staged R rows for the per-(block,
+// batch) sums.  Stages pass between roles through mbarriers only:
+//   full[s]  : producer arrive + TMA bytes          -> MMA issuer, consumers
+//   empty[s] : 6 consumer-warp arrivals + MMA commit -> producer (stage reuse)
+//   acc      : final MMA commit                      -> epilogue (TMEM read)
+constexpr int CEN_CONSUMER_WARPS = 6;
+
+// One consumer column: sums of R[.., kcol] over runs of equal (block, batch) key.
+struct CenColumn {
+  int kcol;
+  int key;
+  double tot;
+  const unsigned char* base;  // shared-memory base of the column
+  uint32_t c8;
+  __device__ __forceinline__ void init(unsigned char* sm, const CenLayout& L, int k) {
+    kcol = k;
+    key = -1;
+    tot = 0.0;
+    base = sm + (k >> 6) * 1024 + (k & 7) * 2;
+    c8 = (uint32_t)((k & 63) >> 3);
+  }
+  __device__ __forceinline__ void flush(const CenArgs& a) {
+    if (key < 0) return;
+    atomicAdd(&a.Omin[(size_t)key * a.K + kcol], tot);
+    atomicAdd(&a.Omin[(size_t)(key - key % (a.B + 1) + a.B) * a.K + kcol], tot);
+  }
+  template <typename H>
+  __device__ __forceinline__ void tile(const CenArgs& a, const CenLayout& L, int s, const int* kr,
+                                       const int* rl) {
+    const unsigned char* tb = base + L.offB[0] + (uint32_t)s * (uint32_t)L.nbB * 16384u;
+    const uint32_t gstride = (uint32_t)L.nbB * 1024u;
+    const int nrun = rl[0];
+    for (int u = 0; u < nrun; ++u) {
+      const int r0 = rl[1 + u], r1 = rl[2 + u];
+      const int kk = kr[r0];
+      if (kk != key) {
+        flush(a);
+        key = kk;
+        tot = 0.0;
+      }
+      float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+      int r = r0;
+#define HB_CEN_VAL(rw)                                                                  \
+  h2f(*(const H*)(tb + ((uint32_t)(rw) >> 3) * gstride + ((uint32_t)(rw) & 7u) * 128u + \
+                  ((c8 ^ ((uint32_t)(rw) & 7u)) << 4)))
+      for (; r + 4 <= r1; r += 4) {
+        s0 += HB_CEN_VAL(r);
+        s1 += HB_CEN_VAL(r + 1);
+        s2 += HB_CEN_VAL(r + 2);
+        s3 += HB_CEN_VAL(r + 3);
+      }
+      for (; r < r1; ++r) s0 += HB_CEN_VAL(r);
+#undef HB_CEN_VAL
+      tot += (double)((s0 + s1) + (s2 + s3));
     }
   }
-}
+};
 
 template <typename H>
-__global__ void __launch_bounds__(256, 1) k_tc_centroid(CenArgs a, CenLayout L) {
+__global__ void __launch_bounds__(256, 1) k_tc_centroid(CenArgs a, CenLayout L,
+                                                        const __grid_constant__ CUtensorMap tmZ,
+                                                        const __grid_constant__ CUtensorMap tmR) {
   extern __shared__ __align__(1024) unsigned char smem_dyn[];
   unsigned char* sm = (unsigned char*)(((uintptr_t)smem_dyn + 1023) & ~(uintptr_t)1023);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int K = a.K;
-  int* cid = (int*)(sm + L.offCid);
-  int* ccat = (int*)(sm + L.offCat);
-  uint64_t* mbar = (uint64_t*)(sm + L.offMisc);
+  int* keys = (int*)(sm + L.offCat);            // [S][128] (block, batch) key per row
+  uint64_t* bars = (uint64_t*)(sm + L.offCid);  // full[3], empty[3], acc
+  uint64_t* full = bars;
+  uint64_t* empty = bars + 3;
+  uint64_t* acc_bar = bars + 6;
+  int* runs = (int*)(sm + L.offCid + 64);         // [3][130] per-stage run lists
   uint32_t* tmem_slot = (uint32_t*)(sm + L.offMisc + 8);
-  const uint32_t sA[3] = {tc::smem_u32(sm + L.offA[0]), tc::smem_u32(sm + L.offA[1]),
-                          tc::smem_u32(sm + L.offA[2])};
-  const uint32_t sB[3] = {tc::smem_u32(sm + L.offB[0]), tc::smem_u32(sm + L.offB[1]),
-                          tc::smem_u32(sm + L.offB[2])};
+  // stage s: A tile at offA[0] + s * 32 KB, B tile at offB[0] + s * nbB * 16 KB
+  const uint32_t sm32 = tc::smem_u32(sm);
+  const uint32_t aStride = 2u * 16384u, bStride = (uint32_t)L.nbB * 16384u;
   const int S = L.stages;
   const int64_t lo = a.n * blockIdx.x / gridDim.x, hi = a.n * (blockIdx.x + 1) / gridDim.x;
   const int ntiles = (int)((hi - lo + 127) / 128);
+  auto tile_rows = [&](int t) { const int64_t p = lo + (int64_t)t * 128; return (int)(hi - p < 128 ? hi - p : 128); };
 
   if (warp == 0) {
     tc::tmem_alloc(tmem_slot, (uint32_t)L.tcols);
@@ -108,105 +191,65 @@ __global__ void __launch_bounds__(256, 1) k_tc_centroid(CenArgs a, CenLayout L) 
     tc::fence_before_sync();
   }
   if (tid == 0) {
-    tc::mbar_init(mbar, 1);
+    for (int s = 0; s < S; ++s) {
+      tc::mbar_init(full + s, 1);
+      tc::mbar_init(empty + s, CEN_CONSUMER_WARPS + 1);
+    }
+    tc::mbar_init(acc_bar, 1);
     tc::fence_mbar_init();
   }
-  const int SI = S + 1;  // id ring slots
-  auto tile_rows = [&](int t) { const int64_t p = lo + (int64_t)t * 128; return (int)(hi - p < 128 ? hi - p : 128); };
-  // prologue: ids of the first S tiles, copies of the first S-1 (one cp.async group each)
-  for (int t = 0; t < S; ++t)
-    if (t < ntiles) cen_load_ids(a, lo + (int64_t)t * 128, tile_rows(t), cid + t * 128, ccat + t * 128);
   __syncthreads();
-  for (int t = 0; t < S - 1; ++t) {
-    if (t < ntiles) cen_copy<H>(a, L, sA[t], sB[t], cid + t * 128);
-    tc::cp_async_commit();
-  }
   tc::fence_after_sync();
   const uint32_t tmem = *tmem_slot;
-  const uint32_t idesc = tc::idesc_f16(128, L.npad, is_bf16<H>::value, true, true);
 
-  // O_minus column owners: (column k, row half h); K <= 128 uses both halves
-  const int ncol = K > 128 ? 256 : 128;
-  const int kcol = tid % ncol, rhalf = tid / ncol;
-  const int nhalves = 256 / ncol;
-  const bool owner = kcol < K;
-  float om_acc = 0.f;   // current run, this 8-row group
-  double om_tot = 0.0;  // current run, earlier groups (float64 keeps long runs exact enough)
-  int om_key = -1;
-  uint32_t phase = 0;
-
-  for (int t = 0; t < ntiles; ++t) {
-    const int buf = t % S;
-    const int64_t pos = lo + (int64_t)t * 128;
-    const int nr = (int)(hi - pos < 128 ? hi - pos : 128);
-    if (S == 3) tc::cp_async_wait_group<1>(); else tc::cp_async_wait_group<0>();
-    tc::fence_proxy_async_smem();
-    tc::fence_before_sync();
-    __syncthreads();
-    if (tid == 0) {
-      tc::fence_after_sync();
-      for (int s = 0; s < 8; ++s) {  // 8 steps of 16 cells
-        const uint64_t ad = tc::sdesc_sw128(sA[buf] + (uint32_t)s * 2u * 2048u, 1024, 2048);
-        const uint64_t bd = tc::sdesc_sw128(sB[buf] + (uint32_t)s * 2u * (uint32_t)L.nbB * 1024u, 1024,
-                                            (uint32_t)L.nbB * 1024u);
-        tc::mma_f16(tmem, ad, bd, idesc, (t > 0 || s > 0) ? 1u : 0u);
-      }
-      tc::mma_commit(mbar);
+  if (warp == 0) {
+    // ---- producer ----------------------------------------------------------------
+    for (int t = 0; t < ntiles; ++t) {
+      const int s = t % S;
+      if (t >= S && !tc::mbar_wait(empty + s, (uint32_t)((t / S - 1) & 1), kMaxPolls)) atomicExch(a.err, 6);
+      cen_produce(a, L, &tmZ, &tmR, lo + (int64_t)t * 128, tile_rows(t), sm32 + L.offA[0] + s * aStride,
+                  sm32 + L.offB[0] + s * bStride, full + s, keys + s * 128, runs + s * 130);
     }
-    {
-      const int tn = t + S - 1, bn = tn % S;  // refill the stage freed by tile t-1
-      if (tn < ntiles) cen_copy<H>(a, L, sA[bn], sB[bn], cid + (tn % SI) * 128);
-      tc::cp_async_commit();
-      const int ti = t + S;  // ids two steps ahead, into the slot tile t-1 used
-      if (ti < ntiles) cen_load_ids(a, lo + (int64_t)ti * 128, tile_rows(ti), cid + (ti % SI) * 128,
-                                    ccat + (ti % SI) * 128);
-    }
-    // per-(block, batch) row sums of R from the staged tile; the row keys were
-    // stored by the gather, swizzle offsets of the 8 rows of a group are fixed
-    if (owner) {
-      const int* keys = ccat + (t % SI) * 128;
-      const unsigned char* tb = sm + L.offB[buf] + (kcol >> 6) * 1024 + (kcol & 7) * 2;
-      const uint32_t gstride = (uint32_t)L.nbB * 1024u;
-      const int c8 = (kcol & 63) >> 3;
-      uint32_t tab[8];
-#pragma unroll
-      for (int i = 0; i < 8; ++i) tab[i] = (uint32_t)i * 128u + ((uint32_t)(c8 ^ i) << 4);
-      const int rows_per = 128 / nhalves;
-      const int r0 = rhalf * rows_per, r1 = min(nr, r0 + rows_per);
-      for (int g = r0; g < r1; g += 8) {
-        const unsigned char* gb = tb + (uint32_t)(g >> 3) * gstride;
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          const int r = g + i;
-          if (r < r1) {
-            const int key = keys[r];
-            if (key != om_key) {
-              if (om_key >= 0) {
-                const double v = om_tot + (double)om_acc;
-                atomicAdd(&a.Omin[(size_t)om_key * K + kcol], v);
-                atomicAdd(&a.Omin[(size_t)(om_key - om_key % (a.B + 1) + a.B) * K + kcol], v);
-              }
-              om_key = key;
-              om_acc = 0.f;
-              om_tot = 0.0;
-            }
-            om_acc += h2f(*(const H*)(gb + tab[i]));
-          }
+  } else if (warp == 1) {
+    // ---- MMA issuer ------------------------------------------------------------------
+    if (lane == 0) {
+      const uint32_t idesc = tc::idesc_f16(128, L.npad, is_bf16<H>::value, true, true);
+      for (int t = 0; t < ntiles; ++t) {
+        const int s = t % S;
+        if (!tc::mbar_wait(full + s, (uint32_t)((t / S) & 1), kMaxPolls)) atomicExch(a.err, 5);
+        tc::fence_after_sync();
+        for (int k = 0; k < 8; ++k) {  // 8 steps of 16 cells
+          const uint64_t ad = tc::sdesc_sw128(sm32 + L.offA[0] + s * aStride + (uint32_t)k * 2u * 2048u, 1024, 2048);
+          const uint64_t bd = tc::sdesc_sw128(sm32 + L.offB[0] + s * bStride + (uint32_t)k * 2u * (uint32_t)L.nbB * 1024u,
+                                              1024, (uint32_t)L.nbB * 1024u);
+          tc::mma_f16(tmem, ad, bd, idesc, (t > 0 || k > 0) ? 1u : 0u);
         }
-        om_tot += (double)om_acc;
-        om_acc = 0.f;
+        tc::mma_commit(empty + s);
       }
+      if (ntiles > 0) tc::mma_commit(acc_bar);
     }
-    if (!tc::mbar_wait(mbar, phase, kMaxPolls)) atomicExch(a.err, 4);
-    phase ^= 1u;
+  } else {
+    // ---- consumers: per-(block, batch) row sums of R ------------------------------
+    const int c = tid - 64;
+    CenColumn colA, colB;  // columns c and c + 192
+    colA.init(sm, L, c);
+    colB.init(sm, L, c + 192);
+    for (int t = 0; t < ntiles; ++t) {
+      const int s = t % S;
+      if (!tc::mbar_wait(full + s, (uint32_t)((t / S) & 1), kMaxPolls)) atomicExch(a.err, 5);
+      const int* kr = keys + s * 128;
+      const int* rl = runs + s * 130;
+      if (colA.kcol < K) colA.tile<H>(a, L, s, kr, rl);
+      if (colB.kcol < K) colB.tile<H>(a, L, s, kr, rl);
+      __syncwarp();
+      if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc::smem_u32(empty + s)) : "memory");
+    }
+    if (colA.kcol < K) colA.flush(a);
+    if (colB.kcol < K) colB.flush(a);
   }
-  if (owner && om_key >= 0) {
-    const double v = om_tot + (double)om_acc;
-    atomicAdd(&a.Omin[(size_t)om_key * K + kcol], v);
-    atomicAdd(&a.Omin[(size_t)(om_key - om_key % (a.B + 1) + a.B) * K + kcol], v);
-  }
+  // ---- epilogue: partial D[pc][cluster] -> P[cta][cluster][pc] -------------------------
+  if (ntiles > 0 && !tc::mbar_wait(acc_bar, 0, kMaxPolls)) atomicExch(a.err, 4);
   tc::fence_after_sync();
-  // partial D[pc][cluster] -> P[cta][cluster][pc]; lane = PC, warps 0-3 / 4-7 split the columns
   {
     const int half = warp >> 2, c = (warp & 3) * 32 + lane;
     const uint32_t tl = tmem + ((uint32_t)((warp & 3) * 32) << 16);
@@ -244,7 +287,10 @@ int launch_tc_centroid(const CenArgs& a, int grid, cudaStream_t st) {
   if ((228u * 1024u) / (smem + 1024) > (size_t)occ_tmem)
     smem = std::min<size_t>(227u * 1024u, 228u * 1024u / occ_tmem - 2048);
   HB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_tc_centroid<H><<<grid, 256, smem, st>>>(a, L);
+  CUtensorMap tmZ, tmR;
+  HB_TRY(make_row_gather_map(&tmZ, a.Zn, a.n, a.ldz, is_bf16<H>::value));
+  HB_TRY(make_row_gather_map(&tmR, a.R, a.n, a.ldr, is_bf16<H>::value));
+  k_tc_centroid<H><<<grid, 256, smem, st>>>(a, L, tmZ, tmR);
   HB_LAUNCH_CHECK();
   return HB_OK;
 }

@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <vector>
+#include <cudaTypedefs.h>
 #include "hb_internal.h"
 
 namespace hb {
@@ -20,6 +21,36 @@ void set_error(const char* fmt, ...) {
   va_start(ap, fmt);
   vsnprintf(g_err, sizeof(g_err), fmt, ap);
   va_end(ap);
+}
+
+int make_row_gather_map(CUtensorMap* tm, const void* base, int64_t rows, int ld, bool bf16) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", (void**)&encode, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !encode) {
+      encode = nullptr;
+      set_error("cuTensorMapEncodeTiled is not available from the driver");
+      return HB_ERR_CUDA;
+    }
+  }
+  if (((uintptr_t)base & 15) || (ld * 2) % 16) {
+    set_error("row gather map: base must be 16-byte aligned and rows a multiple of 16 bytes");
+    return HB_ERR_INVALID;
+  }
+  cuuint64_t gdim[2] = {(cuuint64_t)ld, (cuuint64_t)rows};
+  cuuint64_t gstride[1] = {(cuuint64_t)ld * 2};
+  cuuint32_t box[2] = {64, 1};
+  cuuint32_t estr[2] = {1, 1};
+  const CUresult r = encode(tm, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2,
+                            const_cast<void*>(base), gdim, gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                            CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed (%d) for rows=%lld ld=%d", (int)r, (long long)rows, ld);
+    return HB_ERR_CUDA;
+  }
+  return HB_OK;
 }
 
 int num_sms() {

@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cuda.h>
 #include "hb_common.cuh"
 
 namespace hb {
@@ -102,6 +103,9 @@ int launch_objective_finalize(const double* O, const double* Pr, const double* t
                               cudaStream_t st);
 
 // ---- tensor-core kernels of the 16-bit path ------------------------------------
+// 2-D tensor map over a row-major 16-bit matrix [rows][ld] for row gathers:
+// box = 64 elements x 1 row, 128-byte swizzle, zero fill out of bounds.
+int make_row_gather_map(CUtensorMap* tm, const void* base, int64_t rows, int ld, bool bf16);
 template <typename H>
 int launch_tc_block_update(const BlockArgs& a, const double* O_in, double* O_out, double* O_zero,
                            int* err, cudaStream_t st);

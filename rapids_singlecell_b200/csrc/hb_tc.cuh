@@ -5,6 +5,7 @@
 #pragma once
 
 #include <stdint.h>
+#include <cuda.h>
 #include <cuda_fp16.h>
 #include <cuda_bf16.h>
 
@@ -64,6 +65,24 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* m, uint32_t parity, uint32_t
   for (uint32_t i = 0; i < max_tries; ++i)
     if (mbar_try_wait(m, parity)) return true;
   return false;
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* m, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(m)), "r"(bytes)
+               : "memory");
+}
+
+// ---- TMA row gather (no multicast): 4 rows x one 64-element box of a 2-D
+// tensor map (box one row high) into 512 contiguous bytes of shared memory; the
+// tensor map's 128B swizzle is applied from the destination address.  Rows at or
+// beyond the tensor's height read the zero fill.  Completion is counted on mbar.
+__device__ __forceinline__ void tma_gather4(uint32_t dst, const CUtensorMap* tm, int x, int r0, int r1,
+                                            int r2, int r3, uint64_t* mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(dst),
+      "l"((uint64_t)tm), "r"(x), "r"(r0), "r"(r1), "r"(r2), "r"(r3), "r"(smem_u32(mbar))
+      : "memory");
 }
 
 // ---- MMA ---------------------------------------------------------------------

@@ -179,17 +179,20 @@ __global__ void __launch_bounds__(NT, 1) k_tc_sweep(SweepArgs a, TcLayout L) {
     }
     __syncthreads();
     const int cmin = crange[j].x, cmax = crange[j].y;
-    // penalty rows of the batches present (kernels_pen.cuh:8-21); zero the delta rows
+    // log2 of the penalty rows of the batches present (kernels_pen.cuh:8-21):
+    // log2 pen = theta_b * log2((E+1)/(O[+E]+1)); zero the delta rows
     for (int e = tid; e < (cmax - cmin + 1) * K; e += NT) {
       const int b = cmin + e / K, k = e % K;
       const size_t o_at = (size_t)b * K + k;
       osm[o_at] = 0.f;
+      float lp = 0.f;
       if (!a.init_mode) {
         const float o = (float)(Oin[o_at] - (Omc ? Omc[o_at] : 0.0));
         const float E = (float)(a.Pr[b] * ocol[k]);
         const float denom = a.stabilized ? (o + E + 1.f) : (o + 1.f);
-        pen[o_at] = powf((E + 1.f) / denom, (float)a.theta[b]);
+        lp = (float)a.theta[b] * log2f((E + 1.f) / denom);
       }
+      pen[o_at] = lp;
     }
     // ---- tiles of this block ------------------------------------------------
     while (have && cu.j == j) {
@@ -212,10 +215,11 @@ __global__ void __launch_bounds__(NT, 1) k_tc_sweep(SweepArgs a, TcLayout L) {
       const int nvalid = (int)(cu.hi - cu.pos < 128 ? cu.hi - cu.pos : 128);
       const int cell = cid[buf * 128 + row];
       const int cat = ccat[buf * 128 + row];
-      const float* prow = pen + cat * K;
-      // pass 1: v = exp(-2/sigma (1-s)) * pen, row partial sums; v overwrites s in TMEM.
-      // Two 8-column loads are in flight per wait; exp runs on the SFU (ex2.approx).
-      float rs = 0.f, km = 0.f;
+      const float* prow = pen + cat * K;  // log2 of the penalty row
+      // pass 1: v = exp(-2/sigma (1-s)) * pen = exp2(c2 (1-s) + log2 pen) (one SFU op),
+      // row partial sums of v, v (1-s) (kmeans error) and v * exponent (entropy);
+      // v overwrites s in TMEM.  Two 8-column loads are in flight per wait.
+      float rs = 0.f, km = 0.f, vx = 0.f;
       for (int c = c_lo; c < c_hi; c += 16) {
         const bool two = c + 8 < c_hi;
         float v[8], w2[8];
@@ -230,9 +234,10 @@ __global__ void __launch_bounds__(NT, 1) k_tc_sweep(SweepArgs a, TcLayout L) {
           float val = 0.f;
           if (k < K) {
             const float om = 1.f - x;
-            val = tc::ex2_approx(c2 * om);
-            if (!a.init_mode) val *= prow[k];
+            const float ex = fmaf(c2, om, prow[k]);
+            val = tc::ex2_approx(ex);
             km = fmaf(val, om, km);
+            vx = fmaf(val, ex, vx);
           }
           rs += val;
           x = val;
@@ -261,8 +266,7 @@ __global__ void __launch_bounds__(NT, 1) k_tc_sweep(SweepArgs a, TcLayout L) {
       __syncthreads();
       const float rsum = NT == 256 ? rsp[row] + rsp[128 + row] : rs;
       const float inv = a.init_mode ? 1.f / fmaxf(rsum, 1e-12f) : 1.f / rsum;
-      // pass 2: normalise, round to 16 bits, stage the row, entropy term (lg2 on the SFU)
-      float ent = 0.f;
+      // pass 2: normalise, round to 16 bits, stage the row
       for (int c = c_lo; c < c_hi; c += 16) {
         const bool two = c + 8 < c_hi;
         float v[8], w2[8];
@@ -273,16 +277,20 @@ __global__ void __launch_bounds__(NT, 1) k_tc_sweep(SweepArgs a, TcLayout L) {
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
           if (i >= 8 && !two) break;
-          const float r = (i < 8 ? v[i] : w2[i - 8]) * inv;
-          hv[i] = from_f<H>(r);
-          if (c + i < K) ent = fmaf(r, tc::lg2_approx(r + 1e-12f), ent);
+          hv[i] = from_f<H>((i < 8 ? v[i] : w2[i - 8]) * inv);
         }
         *(uint4*)(Rst + row * L.ldst + c) = *(const uint4*)hv;
         if (two) *(uint4*)(Rst + row * L.ldst + c + 8) = *(const uint4*)(hv + 8);
       }
-      ent *= 0.6931471805599453f;  // lg2 -> natural log
       tc::fence_before_sync();
-      if (cell >= 0) obj_local += (double)(inv * km) + (double)(sig * ent);
+      // objective terms of the row (kernels_kmeans.cuh:30-96, kernels_clustering.cuh:8-62):
+      // kmeans error sum r (2 (1-s)); entropy sum r ln r = (ln 2 / rs) sum v x - ln rs
+      // (r = v / rs, ln v = x ln 2); each half adds its partial sums, half 0 the -ln rs.
+      if (cell >= 0) {
+        double e = (double)(inv * km) + (double)(sig * 0.6931471805599453f * inv * vx);
+        if (half == 0) e -= (double)sig * log((double)(a.init_mode ? fmaxf(rsum, 1e-12f) : rsum));
+        obj_local += e;
+      }
       __syncthreads();
       // observed-count delta: one thread per cluster column, summed per batch run
       for (int kc = tid; kc < K; kc += NT) {

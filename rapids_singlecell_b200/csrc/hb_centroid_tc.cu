@@ -66,7 +66,7 @@ __device__ __forceinline__ void cen_produce(const CenArgs& a, const CenLayout& L
     int k = -1;
     if (r < nr) {
       cell = __ldg(a.idx + pos + r);
-      k = (int)((pos + r) / a.bs) * (a.B + 1) + __ldg(a.cats + cell);
+      k = (int)((pos + r) / a.bs) * (a.B + 1) + __ldg(a.lcat + pos + r);
     }
     rows[i] = cell;
     key[r] = k;

@@ -101,6 +101,7 @@ struct Work {
   double* Omin;  // [nblk][B+1][K] old contribution of each block of the current iteration
   unsigned* barrier;  // grid-barrier counter of the persistent sweep
   int32_t* idx;
+  int32_t* lcat;
   int* err;
   AccumChunk* cen_chunks;
   AccumChunk* m_chunks;
@@ -130,6 +131,7 @@ void carve(const hb_plan& P, Carver& cv, Work& w) {
   w.Omin = cv.take<double>((size_t)P.ml.nblk * (B + 1) * K);
   w.barrier = cv.take<unsigned>(4);
   w.idx = cv.take<int32_t>((size_t)kMaxIterChunk * n);
+  w.lcat = cv.take<int32_t>((size_t)kMaxIterChunk * n);
   w.err = cv.take<int>(4);
   w.cen_chunks = cv.take<AccumChunk>(P.cen_chunks);
   w.m_chunks = cv.take<AccumChunk>(P.max_m_chunks);
@@ -338,28 +340,28 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
   double* obj_init = w.obj_out + std::max(p.max_iter_clustering, 1);
   constexpr bool tc_path = !std::is_same<S, float>::value && !std::is_same<S, double>::value;
   // one persistent sweep (16-bit path) over `nblk` blocks of `idx`, objective into obj_dst
-  auto sweep = [&](const int32_t* idx, int64_t bs, int nb, const double* Omin, int init,
+  auto sweep = [&](const int32_t* idx, const int32_t* lcat, int64_t bs, int nb, const double* Omin, int init,
                    double* obj_dst) -> int {
     if constexpr (tc_path) {
       SweepArgs sa{};
       sa.Zn = Zn; sa.ldz = P->ldz; sa.R = R; sa.ldr = P->ldr; sa.cats = cats; sa.Yn = Yn; sa.ldy = P->ldy;
-      sa.idx = idx; sa.n = n; sa.bs = bs; sa.nblk = nb;
+      sa.idx = idx; sa.lcat = lcat; sa.n = n; sa.bs = bs; sa.nblk = nb;
       sa.Obuf[0] = w.O[0]; sa.Obuf[1] = w.O[1]; sa.Obuf[2] = w.O[2]; sa.b0 = ring.cur;
       sa.Omin = Omin; sa.Pr = w.Pr; sa.theta = w.theta; sa.obj_acc = w.obj_acc; sa.obj_out = obj_dst;
       sa.sigma = p.sigma; sa.d = d; sa.K = K; sa.B = B; sa.stabilized = p.stabilized_penalty;
-      sa.init_mode = init; sa.barrier = w.barrier; sa.err = w.err;
+      sa.init_mode = init; sa.batch_sorted = P->ml.nsub > 1 || B <= 1; sa.barrier = w.barrier; sa.err = w.err;
       HB_CUDA(cudaMemsetAsync(w.barrier, 0, sizeof(unsigned), st));
       HB_TRY(launch_tc_sweep<S>(sa, st));
       ring.cur = (ring.cur + nb) % 3;
       return HB_OK;
     } else {
-      (void)idx; (void)bs; (void)nb; (void)Omin; (void)init; (void)obj_dst;
+      (void)idx; (void)lcat; (void)bs; (void)nb; (void)Omin; (void)init; (void)obj_dst;
       set_error("internal: sweep on the plain path");
       return HB_ERR_INTERNAL;
     }
   };
   if constexpr (tc_path) {
-    HB_TRY(sweep(nullptr, n, 1, nullptr, 1, obj_init));
+    HB_TRY(sweep(nullptr, cats, n, 1, nullptr, 1, obj_init));
   } else {
     BlockArgs a = base;
     a.idx_new = nullptr; a.new_start = 0; a.n_new = n; a.Om_cur = nullptr; a.Om_next = nullptr;
@@ -412,10 +414,11 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
     bool stop = false;
     for (int it0 = 0; it0 < p.max_iter_clustering && !stop; it0 += kMaxIterChunk) {
       const int C = std::min(kMaxIterChunk, p.max_iter_clustering - it0);
-      HB_TRY(membership_build_dev(ml, w.mb, nullptr, seed + (uint32_t)it0, C, cats, w.idx, st));
+      HB_TRY(membership_build_dev(ml, w.mb, nullptr, seed + (uint32_t)it0, C, cats, w.idx, st, w.lcat));
       for (int c = 0; c < C && !stop; ++c) {
         const int it = it0 + c;
         const int32_t* idx = w.idx + (size_t)c * n;
+        const int32_t* lcat = w.lcat + (size_t)c * n;
         // centroids Y = R^T Z_norm, L2-normalised (clustering.cu:272-281).  The pass walks
         // the block-ordered cell list, so it also sums every block's current rows per
         // batch: the "remove old contribution" terms of the sweep (clustering.cu:321-332).
@@ -423,7 +426,7 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
         HB_CUDA(cudaMemsetAsync(w.Omin, 0, sizeof(double) * nblk * omsz, st));
         int sp = span_begin(1, (double)n * (zb + rb + 8));
         if constexpr (tc_path) {
-          CenArgs ca{Zn, P->ldz, R, P->ldr, cats, idx, n, ml.bs, d, K, B, (float*)w.Ypart, w.Omin, w.err};
+          CenArgs ca{Zn, P->ldz, R, P->ldr, cats, idx, lcat, n, ml.bs, d, K, B, (float*)w.Ypart, w.Omin, w.err};
           HB_TRY(launch_tc_centroid<S>(ca, P->cen_chunks, st));
         } else {
           HB_TRY(launch_accum<S, S, TA>(R, P->ldr, Zn, P->ldz, idx, w.cen_chunks, P->cen_chunks, K, d,
@@ -434,7 +437,7 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
         // sweep the blocks (clustering.cu:308-372)
         if constexpr (tc_path) {
           sp = span_begin(0, (double)n * (zb + rb + 8));
-          HB_TRY(sweep(idx, ml.bs, nblk, w.Omin, 0, w.obj_out + it));
+          HB_TRY(sweep(idx, lcat, ml.bs, nblk, w.Omin, 0, w.obj_out + it));
           span_end(sp);
         } else {
         for (int j = 0; j < nblk; ++j) {

@@ -32,11 +32,13 @@ struct MembershipBufs {
 };
 MembershipLayout membership_layout(int64_t n, int64_t bs, int nsub);
 void membership_carve(Carver& cv, const MembershipLayout& L, MembershipBufs& B);
+// lcat (optional): lcat[c*n + p] = cats[idx[c*n + p]], the batch of each list position
 int membership_build(const MembershipLayout& L, const MembershipBufs& B, const uint32_t* h_seeds,
-                     int n_iters, const int32_t* cats, int32_t* idx, cudaStream_t st);
+                     int n_iters, const int32_t* cats, int32_t* idx, cudaStream_t st,
+                     int32_t* lcat = nullptr);
 int membership_build_dev(const MembershipLayout& L, const MembershipBufs& B, const uint32_t* seeds,
                          uint32_t seed0, int n_iters, const int32_t* cats, int32_t* idx,
-                         cudaStream_t st);
+                         cudaStream_t st, int32_t* lcat = nullptr);
 
 // ---- SIMT kernels of the plain (fp32 / fp64) path ----------------------------
 // Row L2 normalisation, inverse norm clamped to 1e12 (reference semantics).
@@ -123,6 +125,7 @@ struct SweepArgs {
   const void* Yn;
   int ldy;
   const int32_t* idx;      // block-ordered cell list (nullptr: identity, one block)
+  const int32_t* lcat;     // batch of each list position (cats itself for the identity list)
   int64_t n, bs;
   int nblk;
   double* Obuf[3];
@@ -136,6 +139,7 @@ struct SweepArgs {
   int d, K, B;
   int stabilized;
   int init_mode;
+  int batch_sorted;        // the list is ordered by batch within each block
   unsigned* barrier;       // zero on entry
   int* err;
 };
@@ -150,6 +154,7 @@ struct CenArgs {
   int ldr;
   const int32_t* cats;
   const int32_t* idx;   // block-ordered cell list
+  const int32_t* lcat;  // batch of each list position
   int64_t n, bs;
   int d, K, B;
   float* P;             // [G][K][d] partial sums

@@ -199,7 +199,7 @@ __global__ void k_part_count(int64_t n, int nblk, int nsub, const int32_t* __res
   for (int q = threadIdx.x; q < kPartTile; q += blockDim.x) {
     int64_t i = base + q;
     if (i < n) {
-      const int bucket = block_of(pcg_key((uint32_t)i, seed), sp, nb) * nsub + (cats ? cats[i] : 0);
+      const int bucket = block_of(pcg_key((uint32_t)i, seed), sp, nb) * nsub + (nsub > 1 ? cats[i] : 0);
       atomicAdd(&cnt[bucket], 1u);
     }
   }
@@ -259,7 +259,8 @@ __global__ void __launch_bounds__(256) k_part_scatter(int64_t n, int64_t bs, int
                                                       const uint32_t* __restrict__ split,
                                                       const uint32_t* __restrict__ offsets,
                                                       const uint32_t* __restrict__ totals,
-                                                      int ntiles, int32_t* __restrict__ idx) {
+                                                      int ntiles, int32_t* __restrict__ idx,
+                                                      int32_t* __restrict__ lcat) {
   extern __shared__ uint32_t dyn[];
   const int nbk = nblk * nsub;
   uint32_t* base = dyn;               // [nbk]
@@ -287,7 +288,7 @@ __global__ void __launch_bounds__(256) k_part_scatter(int64_t n, int64_t bs, int
   for (int r = 0; r < kPartTile / 256; ++r) {
     const int64_t i = tbase + r * 256 + t;
     const bool valid = i < n;
-    const int bk = valid ? block_of(pcg_key((uint32_t)i, seed), sp, nb) * nsub + (cats ? cats[i] : 0)
+    const int bk = valid ? block_of(pcg_key((uint32_t)i, seed), sp, nb) * nsub + (nsub > 1 ? cats[i] : 0)
                          : nbk;
     const unsigned peers = __match_any_sync(0xffffffffu, bk);
     const unsigned lrank = __popc(peers & lanemask_lt());
@@ -300,7 +301,11 @@ __global__ void __launch_bounds__(256) k_part_scatter(int64_t n, int64_t bs, int
       base[j] = run;
     }
     __syncthreads();
-    if (valid) out[wc[w * nbk + bk] + lrank] = (int32_t)i;
+    if (valid) {
+      const uint32_t at = wc[w * nbk + bk] + lrank;
+      out[at] = (int32_t)i;
+      if (lcat) lcat[(size_t)c * n + at] = cats ? cats[i] : 0;
+    }
     __syncthreads();
     for (int j = t; j < nbk; j += 256) {
 #pragma unroll
@@ -350,20 +355,20 @@ void membership_carve(Carver& cv, const MembershipLayout& L, MembershipBufs& B) 
 // Writes, for each of `n_iters` (<= kMaxIterChunk) seeds, the cell list of every
 // block: idx[c*n + j*bs + r] is the r-th cell (ascending) of block j.
 int membership_build(const MembershipLayout& L, const MembershipBufs& B, const uint32_t* h_seeds,
-                     int n_iters, const int32_t* cats, int32_t* idx, cudaStream_t st) {
+                     int n_iters, const int32_t* cats, int32_t* idx, cudaStream_t st, int32_t* lcat) {
   if (n_iters < 1 || n_iters > kMaxIterChunk) {
     set_error("membership_build: n_iters out of range");
     return HB_ERR_INVALID;
   }
   HB_CUDA(cudaMemcpyAsync(B.seeds, h_seeds, sizeof(uint32_t) * n_iters, cudaMemcpyHostToDevice, st));
-  return membership_build_dev(L, B, B.seeds, 0, n_iters, cats, idx, st);
+  return membership_build_dev(L, B, B.seeds, 0, n_iters, cats, idx, st, lcat);
 }
 
 // Block lists for the consecutive seeds seed0 .. seed0+n_iters-1 (no host copy),
 // or for the device list `seeds` when it is not null.
 int membership_build_dev(const MembershipLayout& L, const MembershipBufs& B, const uint32_t* seeds,
                          uint32_t seed0, int n_iters, const int32_t* cats, int32_t* idx,
-                         cudaStream_t st) {
+                         cudaStream_t st, int32_t* lcat) {
   const int nb = L.nblk - 1;
   const int sms = num_sms();
   const int nsub = cats ? L.nsub : 1;
@@ -400,7 +405,7 @@ int membership_build_dev(const MembershipLayout& L, const MembershipBufs& B, con
   if (ssm > 48 * 1024)
     HB_CUDA(cudaFuncSetAttribute(k_part_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm));
   k_part_scatter<<<dim3(L.ntiles, n_iters), 256, ssm, st>>>(L.n, L.bs, L.nblk, nsub, cats, seeds, seed0,
-                                                           B.split, B.offsets, B.totals, L.ntiles, idx);
+                                                           B.split, B.offsets, B.totals, L.ntiles, idx, lcat);
   HB_LAUNCH_CHECK();
   return HB_OK;
 }

@@ -155,9 +155,9 @@ __global__ void __launch_bounds__(NT, 1) k_tc_sweep(SweepArgs a, TcLayout L) {
     int64_t lo, hi;
     slice_of(a, j, blockIdx.x, gridDim.x, lo, hi);
     int cmin = 0, cmax = B - 1;
-    if (a.idx && lo < hi) {
-      cmin = __ldg(a.cats + __ldg(a.idx + lo));
-      cmax = __ldg(a.cats + __ldg(a.idx + hi - 1));
+    if (a.idx && a.batch_sorted && lo < hi) {
+      cmin = __ldg(a.lcat + lo);
+      cmax = __ldg(a.lcat + hi - 1);
     }
     crange[j] = make_int2(cmin, lo < hi ? cmax : cmin - 1);
   }

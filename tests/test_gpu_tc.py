@@ -72,3 +72,20 @@ def test_16bit_odd_shapes_fp16(n, d, K, B):
                     precision="fp16", **kw)
     ref = ho.harmonize(Z, cats, B, Y0, dtype=np.float64, **kw)
     assert rel_maxabs(out.cpu().numpy(), ref.Z_hat) < 2e-3
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp16"])
+def test_many_blocks_times_batches(prec):
+    """250 blocks x 48 batches exceeds the (block, batch) bucket limit of the
+    partition, so the lists are ordered by cell index only inside each block."""
+    n, d, K, B = 12000, 20, 30, 48
+    spec = MixtureSpec(n, d, 4, B, "dirichlet", (), 0.5, (0.8, 1.2))
+    Z, cats, _ = make_mixture(spec, 31)
+    Y0 = initial_centroids(Z, K, 32)
+    labels = pd.Categorical.from_codes(cats, categories=[f"b{i}" for i in range(B)])
+    kw = dict(n_clusters=K, max_iter_harmony=2, max_iter_clustering=3, tol_harmony=-np.inf,
+              tol_clustering=-np.inf, block_proportion=0.004)
+    out = harmonize(torch.as_tensor(Z, device="cuda"), labels, None, init_centroids=Y0,
+                    precision=prec, **kw)
+    ref = ho.harmonize(Z, cats, B, Y0, dtype=np.float64, **kw)
+    assert rel_maxabs(out.cpu().numpy(), ref.Z_hat) < (1e-4 if prec == "fp32" else 2e-3)

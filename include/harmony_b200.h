@@ -107,7 +107,8 @@ HB_API size_t hb_plan_workspace_bytes(const hb_plan* plan);
 /* Full Harmony integration of one problem.
  *   X             device [n_cells, n_pcs] row-major; float64 for HB_FP64, else float32
  *   cats          device int32 [n_cells] batch code per cell (0 .. n_batches-1)
- *   cell_index    device int32 [n_cells] cells sorted by batch (stable)
+ *   cell_index    device int32 [n_cells] cells sorted by batch (stable), or NULL: the
+ *                 engine then builds it in the workspace (needs n_batches <= 4096)
  *   batch_offsets host int64 [n_batches + 1] CSR offsets into cell_index
  *   theta         host float64 [n_batches] (tau discount already applied)
  *   Y0            device [n_clusters, n_pcs] initial centroids, same dtype as X

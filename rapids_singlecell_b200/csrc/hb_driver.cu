@@ -71,6 +71,7 @@ struct hb_plan {
   int asz;        // bytes of the split-n partial sums (4 or 8)
   int ldz, ldr, ldy;
   MembershipLayout ml;
+  MembershipLayout ml1;  // one block ordered by batch: the cell_index when the caller passes none
   int cen_chunks; // split-n chunks of the centroid sum
   int cen_tiles;  // output tiles per chunk
   int max_m_chunks, max_apply_tiles;
@@ -102,12 +103,14 @@ struct Work {
   unsigned* barrier;  // grid-barrier counter of the persistent sweep
   int32_t* idx;
   int32_t* lcat;
+  int32_t* cell_index;  // cells sorted by batch (stable), built when the caller passes none
   int* err;
   AccumChunk* cen_chunks;
   AccumChunk* m_chunks;
   int32_t* batch_chunk_off;
   ApplyTile* apply_tiles;
   MembershipBufs mb;
+  MembershipBufs mb1;
 };
 
 void carve(const hb_plan& P, Carver& cv, Work& w) {
@@ -138,6 +141,8 @@ void carve(const hb_plan& P, Carver& cv, Work& w) {
   w.batch_chunk_off = cv.take<int32_t>(B + 1);
   w.apply_tiles = cv.take<ApplyTile>(P.max_apply_tiles);
   membership_carve(cv, P.ml, w.mb);
+  w.cell_index = cv.take<int32_t>((size_t)n);
+  membership_carve(cv, P.ml1, w.mb1);
 }
 
 int validate(const hb_params& p) {
@@ -198,6 +203,7 @@ int hb_plan_create(const hb_params* params, hb_plan** plan) {
   P->ldr = (int)align_up(p.n_clusters, vec);
   P->ldy = P->ldz;
   P->ml = membership_layout(p.n_cells, p.block_size, p.n_batches);
+  P->ml1 = membership_layout(p.n_cells, p.n_cells, p.n_batches);
   const int sms = num_sms();
   P->cen_tiles = div_up(p.n_clusters, 128) * div_up(p.n_pcs, 64);
   const int64_t target = std::max(1, 2 * sms / P->cen_tiles);
@@ -291,6 +297,15 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
   if (batch_offsets[0] != 0 || batch_offsets[B] != n) {
     set_error("batch_offsets must start at 0 and end at n_cells");
     return HB_ERR_INVALID;
+  }
+  if (!cell_index) {
+    // counting sort of the cells by batch: the partition with a single block
+    if (B > 1 && P->ml1.nsub != B) {
+      set_error("cell_index must be given when n_batches > %d", kMaxBuckets);
+      return HB_ERR_INVALID;
+    }
+    HB_TRY(membership_build_dev(P->ml1, w.mb1, nullptr, 0, 1, cats, w.cell_index, st));
+    cell_index = w.cell_index;
   }
   std::vector<AccumChunk> cen(P->cen_chunks);
   {
@@ -533,7 +548,7 @@ extern "C" {
 int hb_harmonize(hb_plan* plan, const void* X, const int32_t* cats, const int32_t* cell_index,
                  const int64_t* batch_offsets, const double* theta, const void* Y0, void* workspace,
                  size_t workspace_bytes, void* Z_hat, hb_outputs* out, void* stream) {
-  if (!plan || !X || !cats || !cell_index || !batch_offsets || !theta || !Y0 || !Z_hat) {
+  if (!plan || !X || !cats || !batch_offsets || !theta || !Y0 || !Z_hat) {
     set_error("hb_harmonize: null argument");
     return HB_ERR_INVALID;
   }

@@ -57,8 +57,11 @@ class HarmonyProblem:
         self.n_batches = int(n_batches)
         N_b = np.bincount(cats, minlength=self.n_batches).astype(np.int64)
         self.cats = torch.as_tensor(cats, device=self.device)
-        self.cell_index = torch.as_tensor(np.argsort(cats, kind="stable").astype(np.int32),
-                                          device=self.device)
+        # the engine sorts the cells by batch itself up to 4096 batches
+        self.cell_index = None
+        if self.n_batches > 4096:
+            self.cell_index = torch.as_tensor(np.argsort(cats, kind="stable").astype(np.int32),
+                                              device=self.device)
         self.offsets = np.zeros(self.n_batches + 1, dtype=np.int64)
         self.offsets[1:] = np.cumsum(N_b)
         self.theta = np.asarray(theta, dtype=np.float64)
@@ -118,7 +121,8 @@ class HarmonyProblem:
                         ctypes.pointer(prof) if profile else None)
         st = self.stream if self.stream is not None else torch.cuda.current_stream(self.device)
         _lib.check(self.lib.hb_harmonize(
-            self.plan, self.X.data_ptr(), self.cats.data_ptr(), self.cell_index.data_ptr(),
+            self.plan, self.X.data_ptr(), self.cats.data_ptr(),
+            None if self.cell_index is None else self.cell_index.data_ptr(),
             self._off_c, self._th_c, self.Y0.data_ptr(), self.ws.data_ptr(), self.ws_bytes,
             self.Z_hat.data_ptr(), ctypes.byref(out), ctypes.c_void_p(st.cuda_stream)))
         n_outer = n_obj.value - 1
@@ -140,6 +144,21 @@ class HarmonyProblem:
             self.close()
         except Exception:  # noqa: BLE001
             pass
+
+
+def _integer_codes(labels):
+    """Categorical codes of plain non-negative integer labels without pandas:
+    the categories are the sorted distinct values, as ``astype("category")``
+    gives them.  Returns (None, 0) for anything else."""
+    if isinstance(labels, torch.Tensor):
+        labels = labels.detach().cpu().numpy()
+    if not isinstance(labels, np.ndarray) or labels.ndim != 1 or labels.dtype.kind not in "iu":
+        return None, 0
+    if labels.size == 0 or labels.min() < 0 or labels.max() > 16 * labels.size + (1 << 20):
+        return None, 0
+    present = np.bincount(labels) > 0
+    remap = np.cumsum(present, dtype=np.int64) - 1
+    return remap[labels].astype(np.int32), int(present.sum())
 
 
 def get_batch_codes(batch_mat, batch_key):
@@ -273,9 +292,11 @@ def harmonize(
     ``HarmonyInfo`` when ``return_info``).
     """
     n_cells, n_pcs = (int(v) for v in Z.shape)
-    codes = get_batch_codes(batch_mat, batch_key)
-    n_batches = int(codes.cat.categories.size)
-    cats_np = np.asarray(codes.cat.codes.values, dtype=np.int32)
+    cats_np, n_batches = _integer_codes(batch_mat) if batch_key is None else (None, 0)
+    if cats_np is None:
+        codes = get_batch_codes(batch_mat, batch_key)
+        n_batches = int(codes.cat.categories.size)
+        cats_np = np.asarray(codes.cat.codes.values, dtype=np.int32)
     if cats_np.shape[0] != n_cells:
         raise ValueError("batch labels must have one entry per cell")
     N_b = np.bincount(cats_np, minlength=n_batches).astype(np.int64)

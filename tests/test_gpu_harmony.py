@@ -113,3 +113,24 @@ def test_harmony_integrate_dropin_surface():
     c.obsm["X_pca"][0, 0] = np.nan
     with pytest.raises(RuntimeError, match="NaN"):
         harmony_integrate(c, "batch")
+
+
+def test_engine_cell_index_matches_caller_sorted():
+    """cell_index=NULL (the engine sorts by batch) gives the result of the
+    caller's stable argsort (up to the float64 atomic summation order of the
+    observed counts, which differs from run to run)."""
+    from rapids_singlecell_b200.harmony import HarmonyProblem
+
+    spec = MixtureSpec(7000, 20, 4, 5, "dirichlet", (), 0.5, (0.8, 1.2))
+    Z, cats, _ = make_mixture(spec, 41)
+    Y0 = torch.as_tensor(initial_centroids(Z, 25, 42), device="cuda")
+    X = torch.as_tensor(Z, device="cuda")
+    kw = dict(precision="fp32", n_clusters=25, max_iter_harmony=2, max_iter_clustering=3,
+              tol_harmony=-np.inf, tol_clustering=-np.inf)
+    a = HarmonyProblem(X, cats, 5, Y0, np.full(5, 2.0), **kw)
+    assert a.cell_index is None
+    za = a.run()[0].clone()
+    b = HarmonyProblem(X, cats, 5, Y0, np.full(5, 2.0), **kw)
+    b.cell_index = torch.as_tensor(np.argsort(cats, kind="stable").astype(np.int32), device="cuda")
+    zb = b.run()[0]
+    assert rel_maxabs(za.cpu().numpy(), zb.cpu().numpy()) < 1e-5

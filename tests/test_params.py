@@ -62,3 +62,23 @@ def test_flavor_validation():
         harmony_integrate(A(), "batch", flavor="harmony3")
     with pytest.raises(ValueError, match="is not available in adata.obsm"):
         harmony_integrate(A(), "batch", basis="nope")
+
+
+@pytest.mark.parametrize("labels", [np.array([5, 2, 2, 9, 5, 0], dtype=np.int64),
+                                    np.array([3, 3, 3], dtype=np.int32),
+                                    np.arange(1000, dtype=np.uint16)[::-1].copy()])
+def test_integer_codes_match_pandas(labels):
+    from rapids_singlecell_b200.harmony import _integer_codes, get_batch_codes
+
+    codes, nb = _integer_codes(labels)
+    ref = get_batch_codes(labels, None)
+    assert nb == ref.cat.categories.size
+    np.testing.assert_array_equal(codes, ref.cat.codes.values.astype(np.int32))
+
+
+@pytest.mark.parametrize("labels", [np.array([-1, 2]), np.array(["a", "b"]), np.zeros((2, 2), int),
+                                    np.array([1.0, 2.0])])
+def test_integer_codes_declines(labels):
+    from rapids_singlecell_b200.harmony import _integer_codes
+
+    assert _integer_codes(labels) == (None, 0)

@@ -47,8 +47,10 @@ def parse():
     ap.add_argument("--precision", default="bf16", choices=["bf16", "fp16", "fp32"])
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--profile-case", action="store_true",
-                    help="one short run for ncu: 200,000 cells of the same workload, 1 outer x 2 "
-                         "k-means iterations, then exit")
+                    help="one short run for ncu: the same workload for 1 outer x 2 k-means "
+                         "iterations, then exit")
+    ap.add_argument("--profile-cells", type=int, default=500_000,
+                    help="cells of the --profile-case run")
     return ap.parse_args()
 
 
@@ -58,7 +60,7 @@ def run_profile_case(args):
     from rapids_singlecell_b200.harmony import HarmonyProblem
     from rapids_singlecell_b200.synthetic import make_config
 
-    cfg = make_config(WORKLOAD, seed=0, n_cells=200_000)
+    cfg = make_config(WORKLOAD, seed=0, n_cells=args.profile_cells)
     X = torch.as_tensor(cfg["Z"], device="cuda")
     prob = HarmonyProblem(X, cfg["cats"], cfg["n_batches"], torch.as_tensor(cfg["Y0"], device="cuda"),
                           np.full(cfg["n_batches"], 2.0), precision=args.precision,

@@ -5,15 +5,20 @@
 // similarity matrix round-tripping through HBM (_cuda/harmony/clustering/
 // clustering.cu:308-372).  Here one cooperative launch walks all blocks of an
 // iteration.  For block j every CTA takes an even, contiguous slice of the
-// block's cell list (ordered by batch, then cell), and for each tile of <= 128
-// cells: gathers the 16-bit normalised embeddings into a swizzled shared tile,
-// runs S = Z_tile . Y_norm^T on the tensor core (fp32 in TMEM), and in the
-// epilogue forms R = normalise_L1(exp(-2/sigma (1-s)) * pen[batch]), writes it,
-// and adds it to a per-CTA observed-count delta.  The deltas are flushed with
+// block's cell list (ordered by batch, then cell) and splits it between its NG
+// thread groups of 256 threads; each group, for each tile of <= 128 cells:
+// gathers the 16-bit normalised embeddings into a swizzled shared tile, runs
+// S = Z_tile . Y_norm^T on the tensor core (fp32 in its own TMEM columns), and in
+// the epilogue forms R = normalise_L1(exp(-2/sigma (1-s)) * pen[batch]), writes
+// it, and adds it to its observed-count delta.  The deltas are flushed with
 // float64 atomics and a bounded grid barrier separates the blocks, because the
 // penalty of block j+1 depends on the counts after block j.  The "remove old
 // contribution" step of every block comes precomputed from the centroid pass
 // (Omin), so no R row is read in the sweep.
+//
+// Two groups per CTA instead of two CTAs per SM: the runtime admits one
+// TMEM-allocating CTA per SM into a cooperative launch, and the groups share
+// the penalty table and the centroid tile.
 //
 // O state: three rotating buffers of (B+1) x K float64 (row B holds the column
 // sums, i.e. E / Pr_b).  Block j reads buffer (b0+j)%3, accumulates into
@@ -28,27 +33,68 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
   return v;
 }
 
-// Grid-wide barrier for a cooperative launch.  Every wait is bounded: after
-// ~2^26 polls the CTA records error 3 and proceeds (the host reports a timeout).
-__device__ __forceinline__ void grid_barrier(unsigned* ctr, unsigned target, int* err) {
+// Grid-wide barrier of a cooperative launch, split in two: arrive once this
+// CTA's writes of the block are issued, wait before the next block's counts are
+// read; work that does not depend on the other CTAs goes in between.  The wait
+// is bounded: after ~2^26 polls the CTA records error 3 and proceeds (the host
+// reports a timeout).
+__device__ __forceinline__ void grid_arrive(unsigned* ctr) {
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
     atomicAdd(ctr, 1u);
+  }
+}
+__device__ __forceinline__ void grid_wait(unsigned* ctr, unsigned target, int* err) {
+  if (threadIdx.x == 0) {
     unsigned spins = 0;
     while (ld_acquire_u32(ctr) < target) {
       if (++spins > (1u << 26)) {
         atomicExch(err, 3);
         break;
       }
-      __nanosleep(64);
+      __nanosleep(32);
     }
     __threadfence();
   }
   __syncthreads();
 }
 
-// The slice of block j processed by CTA c of G: list positions [lo, hi).
+// barrier of the 256 threads of thread group g (named barrier 1 + g)
+__device__ __forceinline__ void group_sync(int g) {
+  asm volatile("bar.sync %0, 256;" ::"r"(1 + g) : "memory");
+}
+
+// Shared memory of the sweep: NG groups, each with two A tiles, a staging tile,
+// its delta table and row tables; one centroid tile and one penalty table.
+struct SweepLayout {
+  TcLayout t;        // tile geometry (dpad, npad, tcols per group, ldst)
+  int ng;
+  uint32_t atile;    // bytes of one A tile
+  uint32_t offA, offB, offRst, rstBytes, offPen, offOsm, osmBytes, offRows, offMisc, bytes;
+};
+
+inline SweepLayout sweep_layout(int d, int K, int B, int ldr, int ng) {
+  SweepLayout S{};
+  S.t = tc_layout(d, K, B, ldr, 4);
+  S.ng = ng;
+  auto al = [](uint32_t x, uint32_t a) { return (x + a - 1) / a * a; };
+  S.atile = (uint32_t)S.t.kblk * 16384u;
+  uint32_t o = 0;
+  S.offA = o; o += (uint32_t)ng * 2u * S.atile;
+  S.offB = o; o += (uint32_t)S.t.kblk * S.t.npad * 128u;
+  S.rstBytes = al(128u * S.t.ldst * 2u, 16);
+  S.offRst = al(o, 16); o = S.offRst + (uint32_t)ng * S.rstBytes;
+  S.offPen = al(o, 16); o = S.offPen + (uint32_t)B * K * 4u;
+  S.osmBytes = al((uint32_t)B * K * 4u, 16);
+  S.offOsm = al(o, 16); o = S.offOsm + (uint32_t)ng * S.osmBytes;
+  S.offRows = al(o, 16); o = S.offRows + (uint32_t)ng * 3u * 256u * 4u;  // cid, ccat, rsp: [2][128] each
+  S.offMisc = al(o, 16); o = S.offMisc + 64u + 32u * 8u;
+  S.bytes = o + 1024u;  // slack for 1024-byte alignment of the base
+  return S;
+}
+
+// The slice of block j processed by (virtual) worker c of G: list positions [lo, hi).
 __device__ __forceinline__ void slice_of(const SweepArgs& a, int j, int c, int G, int64_t& lo, int64_t& hi) {
   const int64_t s = (int64_t)j * a.bs;
   const int64_t nj = min(a.bs, a.n - s);
@@ -56,16 +102,16 @@ __device__ __forceinline__ void slice_of(const SweepArgs& a, int j, int c, int G
   hi = s + nj * (c + 1) / G;
 }
 
-// Work cursor over (block, tile start) for this CTA; tile = up to 128 positions.
+// Work cursor over (block, tile start) of one thread group; tile = up to 128 positions.
 struct Cursor {
   int j;
   int64_t pos, hi;
 };
 
-__device__ __forceinline__ bool cursor_first(const SweepArgs& a, int j, Cursor& cu) {
+__device__ __forceinline__ bool cursor_first(const SweepArgs& a, int j, int v, int nv, Cursor& cu) {
   for (; j < a.nblk; ++j) {
     int64_t lo, hi;
-    slice_of(a, j, blockIdx.x, gridDim.x, lo, hi);
+    slice_of(a, j, v, nv, lo, hi);
     if (lo < hi) {
       cu.j = j;
       cu.pos = lo;
@@ -76,81 +122,137 @@ __device__ __forceinline__ bool cursor_first(const SweepArgs& a, int j, Cursor& 
   return false;
 }
 
-__device__ __forceinline__ bool cursor_next(const SweepArgs& a, const Cursor& cu, Cursor& nx) {
+__device__ __forceinline__ bool cursor_next(const SweepArgs& a, const Cursor& cu, int v, int nv, Cursor& nx) {
   if (cu.pos + 128 < cu.hi) {
     nx = cu;
     nx.pos = cu.pos + 128;
     return true;
   }
-  return cursor_first(a, cu.j + 1, nx);
+  return cursor_first(a, cu.j + 1, v, nv, nx);
 }
 
+__device__ __forceinline__ int tile_rows(const Cursor& cu) {
+  return (int)(cu.hi - cu.pos < 128 ? cu.hi - cu.pos : 128);
+}
+
+// Cell id and batch of row r of the tile at list position pos.  Issued early;
+// the registers are consumed by stage_tile once the loads have landed.
+struct TileIds {
+  int cell, cat;
+};
+__device__ __forceinline__ TileIds load_tile_ids(const SweepArgs& a, int64_t pos, int nr, int r) {
+  TileIds t{-1, 0};
+  if (r < nr) {
+    t.cell = a.idx ? __ldg(a.idx + pos + r) : (int)(pos + r);
+    t.cat = __ldg(a.lcat + pos + r);
+  }
+  return t;
+}
+
+// Copies of the tile's normalised embedding rows into the 128B-swizzled K-major
+// A tile (zero fill past the PCs and for missing rows).  gt = thread index in the
+// group: it owns row gt % 128 and every other 16-byte chunk of it.
 template <typename H>
-__device__ __forceinline__ void gather_item(const SweepArgs& a, const Cursor& cu, uint32_t sA,
-                                            const TcLayout& L, int* cid, int* ccat) {
-  const int64_t nr = cu.hi - cu.pos < 128 ? cu.hi - cu.pos : 128;
-  gather_rows_swizzled((const H*)a.Zn, a.ldz, a.idx ? a.idx + cu.pos : nullptr, cu.pos, nr, 0, sA, L,
-                       cid, ccat, a.cats);
+__device__ __forceinline__ void stage_tile(const SweepArgs& a, TileIds t, int gt, uint32_t sA, int dpad,
+                                           int* cid, int* ccat) {
+  const int r = gt & 127, part = gt >> 7;
+  if (part == 0) {
+    cid[r] = t.cell;
+    ccat[r] = t.cat;
+  }
+  const H* Zn = (const H*)a.Zn;
+  const H* src = t.cell >= 0 ? Zn + (int64_t)t.cell * a.ldz : Zn;
+  const int nch = dpad / 8;
+  for (int ch = part; ch < nch; ch += 2) {
+    const bool ok = t.cell >= 0 && ch * 8 < a.ldz;
+    const uint32_t dst = sA + (uint32_t)(ch >> 3) * 16384u + tc::sw128_off(r, ch & 7);
+    tc::cp_async16(dst, ok ? (const void*)(src + ch * 8) : (const void*)Zn, ok ? 16u : 0u);
+  }
 }
 
-// NT = 256: warps 0-3 and 4-7 take the two column halves of the same 128 rows
-// (one CTA per SM).  NT = 128: each thread owns a full row; used when two CTAs
-// fit on an SM so that one CTA's latency chain overlaps the other's.
-template <typename H, int NT>
-__global__ void __launch_bounds__(NT, 1) k_tc_sweep(SweepArgs a, TcLayout L) {
+// Starts of the runs of equal batch in a tile (rows are ordered by batch inside
+// a block), ascending, terminated by nvalid.  Executed by one full warp.
+__device__ __forceinline__ void tile_runs(const int* cc, int nvalid, int* runs, int* nruns) {
+  const int lane = threadIdx.x & 31;
+  int cnt = 0;
+  for (int r0 = 0; r0 < nvalid; r0 += 32) {
+    const int r = r0 + lane;
+    const bool start = r < nvalid && (r == 0 || cc[r] != cc[r - 1]);
+    const unsigned m = __ballot_sync(0xffffffffu, start);
+    if (start) runs[cnt + __popc(m & lanemask_lt())] = r;
+    cnt += __popc(m);
+  }
+  if (lane == 0) {
+    runs[cnt] = nvalid;
+    *nruns = cnt;
+  }
+}
+
+template <typename H, int NG>
+__global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayout SL) {
+  constexpr int NT = 256 * NG;
   extern __shared__ __align__(1024) unsigned char smem_dyn[];
   unsigned char* sm = (unsigned char*)(((uintptr_t)smem_dyn + 1023) & ~(uintptr_t)1023);
+  const TcLayout& L = SL.t;
   const int K = a.K, B = a.B;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  float* pen = (float*)(sm + L.offPen);   // [B][K]
-  float* osm = (float*)(sm + L.offOsm);   // [B][K] observed-count delta of this CTA
-  H* Rst = (H*)(sm + L.offRst);
-  int* cid = (int*)(sm + L.offCid);       // [2][128]
-  int* ccat = (int*)(sm + L.offCat);      // [2][128]
-  float* rsp = (float*)(sm + L.offRs);    // [2][128]
-  uint64_t* mbar = (uint64_t*)(sm + L.offMisc);
-  uint32_t* tmem_slot = (uint32_t*)(sm + L.offMisc + 8);
-  double* red = (double*)(sm + L.offMisc + 16);
-  __shared__ float dsum[256];             // column sums of the delta (row B)
-  __shared__ double ocol[256];            // column sums of the state
-  __shared__ int2 crange[kMaxBlocks];    // batch range of this CTA's slice, per block
-  __shared__ int runs[130];               // tile run starts (batch changes), terminated by nrows
-  __shared__ int nruns;
+  const int g = tid >> 8, gt = tid & 255, gw = gt >> 5;   // thread group, index and warp in it
+  const int vid = blockIdx.x * NG + g, nvw = gridDim.x * NG;  // the group's worker index, workers
+  float* pen = (float*)(sm + SL.offPen);                     // [B][K] log2 of the penalty
+  float* osm = (float*)(sm + SL.offOsm + g * SL.osmBytes);   // [B][K] observed-count delta
+  H* Rst = (H*)(sm + SL.offRst + g * SL.rstBytes);           // [128][ldst] staged rows
+  int* cid = (int*)(sm + SL.offRows + g * 3072);             // [2][128] cell per row
+  int* ccat = cid + 256;                                     // [2][128] batch per row
+  float* rsp = (float*)(ccat + 256);                         // [2][128] row sums of the halves
+  uint64_t* mbar = (uint64_t*)(sm + SL.offMisc) + g;
+  uint32_t* tmem_slot = (uint32_t*)(sm + SL.offMisc + 32);
+  double* red = (double*)(sm + SL.offMisc + 64);
+  __shared__ float dsum_s[NG][256];        // column sums of the deltas (row B)
+  __shared__ double ocol[256];             // column sums of the state
+  __shared__ int2 crange[kMaxBlocks];      // batch range of this CTA's slice, per block
+  __shared__ int runs_s[NG][2][130];       // run starts of the two tile buffers
+  __shared__ int nruns_s[NG][2];
+  float* dsum = dsum_s[g];
+  int(*runs)[130] = runs_s[g];
+  int* nruns = nruns_s[g];
   H* R = (H*)a.R;
-  const uint32_t sA[2] = {tc::smem_u32(sm + L.offA0), tc::smem_u32(sm + L.offA1)};
-  const uint32_t sB = tc::smem_u32(sm + L.offB);
+  const uint32_t sA[2] = {tc::smem_u32(sm + SL.offA + (uint32_t)(2 * g) * SL.atile),
+                          tc::smem_u32(sm + SL.offA + (uint32_t)(2 * g + 1) * SL.atile)};
+  const uint32_t sB = tc::smem_u32(sm + SL.offB);
   const size_t ldo = (size_t)(B + 1) * K;
 
   if (warp == 0) {
-    tc::tmem_alloc(tmem_slot, (uint32_t)L.tcols);
+    tc::tmem_alloc(tmem_slot, (uint32_t)(NG * L.tcols));
     tc::tmem_relinquish();
     tc::fence_before_sync();
   }
-  if (tid == 0) {
+  if (gt == 0) {
     tc::mbar_init(mbar, 1);
     tc::fence_mbar_init();
   }
   load_centroids_swizzled((const H*)a.Yn, a.ldy, K, sB, L);
   Cursor cu;
-  bool have = cursor_first(a, 0, cu);
-  if (have) gather_item<H>(a, cu, sA[0], L, cid, ccat);
+  bool have = cursor_first(a, 0, vid, nvw, cu);
+  if (have) stage_tile<H>(a, load_tile_ids(a, cu.pos, tile_rows(cu), gt & 127), gt, sA[0], L.dpad, cid, ccat);
   __syncthreads();
+  if (have && gw == 0) tile_runs(ccat, tile_rows(cu), runs[0], &nruns[0]);
   tc::fence_after_sync();
-  const uint32_t tmem = *tmem_slot;
+  const uint32_t tmem = *tmem_slot + (uint32_t)(g * L.tcols);
 
   const uint32_t idesc = tc::idesc_f16(128, L.npad, is_bf16<H>::value, false, false);
   const float c2 = (float)(-2.0 / a.sigma * 1.4426950408889634);  // exp(x) = exp2(x log2 e)
   const float sig = (float)a.sigma;
-  const int half = NT == 256 ? warp >> 2 : 0;
-  const int row = (warp & 3) * 32 + lane;
+  const int half = gw >> 2;  // warps 0-3 / 4-7 of the group: the two column halves
+  const int row = (gw & 3) * 32 + lane;
   const uint32_t tl = tmem + ((uint32_t)((warp & 3) * 32) << 16);
-  const int nh = NT == 256 ? (L.npad / 2 + 7) / 8 * 8 : L.npad;
+  const int nh = (L.npad / 2 + 7) / 8 * 8;
   const int c_lo = half * nh, c_hi = min(L.npad, c_lo + nh);
   double obj_local = 0.0;
   uint32_t phase = 0;
   int buf = 0;
-  bool pre_issued = false;  // the MMA of the current tile was issued before the last barrier
-  // batch range of every block's slice (the list is ordered by batch within a block)
+  bool pre_issued = false;  // the MMA of the group's current tile was issued before the last barrier
+  // batch range of every block's CTA slice (the list is ordered by batch within a block);
+  // the CTA slice is the union of its groups' slices
   for (int j = tid; j < a.nblk; j += NT) {
     int64_t lo, hi;
     slice_of(a, j, blockIdx.x, gridDim.x, lo, hi);
@@ -168,14 +270,13 @@ __global__ void __launch_bounds__(NT, 1) k_tc_sweep(SweepArgs a, TcLayout L) {
     double* Ozero = a.Obuf[(a.b0 + j + 2) % 3];
     const double* Omc = (a.Omin && j == 0) ? a.Omin : nullptr;                       // this block
     const double* Omn = (a.Omin && j + 1 < a.nblk) ? a.Omin + (size_t)(j + 1) * ldo : nullptr;  // next
-    int64_t lo, hi;
-    slice_of(a, j, blockIdx.x, gridDim.x, lo, hi);
     for (size_t e = (size_t)blockIdx.x * NT + tid; e < ldo; e += (size_t)gridDim.x * NT) Ozero[e] = 0.0;
     for (int k = tid; k < K; k += NT) {
       double s = Oin[(size_t)B * K + k];
       if (Omc) s -= Omc[(size_t)B * K + k];
       ocol[k] = s;
-      dsum[k] = 0.f;
+#pragma unroll
+      for (int q = 0; q < NG; ++q) dsum_s[q][k] = 0.f;
     }
     __syncthreads();
     const int cmin = crange[j].x, cmax = crange[j].y;
@@ -184,7 +285,8 @@ __global__ void __launch_bounds__(NT, 1) k_tc_sweep(SweepArgs a, TcLayout L) {
     for (int e = tid; e < (cmax - cmin + 1) * K; e += NT) {
       const int b = cmin + e / K, k = e % K;
       const size_t o_at = (size_t)b * K + k;
-      osm[o_at] = 0.f;
+#pragma unroll
+      for (int q = 0; q < NG; ++q) ((float*)(sm + SL.offOsm + q * SL.osmBytes))[o_at] = 0.f;
       float lp = 0.f;
       if (!a.init_mode) {
         const float o = (float)(Oin[o_at] - (Omc ? Omc[o_at] : 0.0));
@@ -194,25 +296,25 @@ __global__ void __launch_bounds__(NT, 1) k_tc_sweep(SweepArgs a, TcLayout L) {
       }
       pen[o_at] = lp;
     }
-    // ---- tiles of this block ------------------------------------------------
+    __syncthreads();
+    // ---- this group's tiles of the block ------------------------------------------
     while (have && cu.j == j) {
       if (!pre_issued) {
         tc::cp_async_wait_all();
         tc::fence_proxy_async_smem();
         tc::fence_before_sync();
-        __syncthreads();
-        if (tid == 0) issue_similarity_mma(tmem, sA[buf], sB, L, idesc, mbar);
-      } else {
-        __syncthreads();  // penalty rows of this block are complete
+        group_sync(g);
+        if (gt == 0) issue_similarity_mma(tmem, sA[buf], sB, L, idesc, mbar);
       }
       pre_issued = false;
       Cursor nx;
-      const bool have_nx = cursor_next(a, cu, nx);
-      if (have_nx) gather_item<H>(a, nx, sA[buf ^ 1], L, cid + (buf ^ 1) * 128, ccat + (buf ^ 1) * 128);
+      const bool have_nx = cursor_next(a, cu, vid, nvw, nx);
+      TileIds tn{-1, 0};
+      if (have_nx) tn = load_tile_ids(a, nx.pos, tile_rows(nx), gt & 127);
       if (!tc::mbar_wait(mbar, phase, kMaxPolls)) atomicExch(a.err, 2);
       phase ^= 1u;
       tc::fence_after_sync();
-      const int nvalid = (int)(cu.hi - cu.pos < 128 ? cu.hi - cu.pos : 128);
+      const int nvalid = tile_rows(cu);
       const int cell = cid[buf * 128 + row];
       const int cat = ccat[buf * 128 + row];
       const float* prow = pen + cat * K;  // log2 of the penalty row
@@ -247,26 +349,13 @@ __global__ void __launch_bounds__(NT, 1) k_tc_sweep(SweepArgs a, TcLayout L) {
       }
       km *= 2.f;
       tc::tmem_st_wait();
-      if (NT == 256) rsp[half * 128 + row] = rs;
-      // run starts of equal batch inside the tile (rows are ordered by batch)
-      if (warp == 0) {
-        int cnt = 0;
-        for (int r0 = 0; r0 < nvalid; r0 += 32) {
-          const int r = r0 + lane;
-          const bool start = r < nvalid && (r == 0 || ccat[buf * 128 + r] != ccat[buf * 128 + r - 1]);
-          const unsigned m = __ballot_sync(0xffffffffu, start);
-          if (start) runs[cnt + __popc(m & lanemask_lt())] = r;
-          cnt += __popc(m);
-        }
-        if (lane == 0) {
-          runs[cnt] = nvalid;
-          nruns = cnt;
-        }
-      }
-      __syncthreads();
-      const float rsum = NT == 256 ? rsp[row] + rsp[128 + row] : rs;
-      const float inv = a.init_mode ? 1.f / fmaxf(rsum, 1e-12f) : 1.f / rsum;
-      // pass 2: normalise, round to 16 bits, stage the row
+      rsp[half * 128 + row] = rs;
+      group_sync(g);
+      const float rsum = rsp[row] + rsp[128 + row];
+      const float rsafe = a.init_mode ? fmaxf(rsum, 1e-12f) : rsum;
+      const float inv = 1.f / rsafe;
+      // pass 2: normalise, round to 16 bits; write the row to R and stage it for the counts
+      H* Rrow = R + (int64_t)(cell >= 0 ? cell : 0) * a.ldr;
       for (int c = c_lo; c < c_hi; c += 16) {
         const bool two = c + 8 < c_hi;
         float v[8], w2[8];
@@ -281,22 +370,32 @@ __global__ void __launch_bounds__(NT, 1) k_tc_sweep(SweepArgs a, TcLayout L) {
         }
         *(uint4*)(Rst + row * L.ldst + c) = *(const uint4*)hv;
         if (two) *(uint4*)(Rst + row * L.ldst + c + 8) = *(const uint4*)(hv + 8);
+        if (cell >= 0) {
+          if (c < a.ldr) *(uint4*)(Rrow + c) = *(const uint4*)hv;
+          if (two && c + 8 < a.ldr) *(uint4*)(Rrow + c + 8) = *(const uint4*)(hv + 8);
+        }
       }
       tc::fence_before_sync();
       // objective terms of the row (kernels_kmeans.cuh:30-96, kernels_clustering.cuh:8-62):
       // kmeans error sum r (2 (1-s)); entropy sum r ln r = (ln 2 / rs) sum v x - ln rs
       // (r = v / rs, ln v = x ln 2); each half adds its partial sums, half 0 the -ln rs.
       if (cell >= 0) {
-        double e = (double)(inv * km) + (double)(sig * 0.6931471805599453f * inv * vx);
-        if (half == 0) e -= (double)sig * log((double)(a.init_mode ? fmaxf(rsum, 1e-12f) : rsum));
-        obj_local += e;
+        constexpr float kLn2 = 0.6931471805599453f;
+        float e = inv * fmaf(sig * kLn2, vx, km);
+        if (half == 0) e -= sig * kLn2 * tc::lg2_approx(rsafe);
+        obj_local += (double)e;
       }
-      __syncthreads();
-      // observed-count delta: one thread per cluster column, summed per batch run
-      for (int kc = tid; kc < K; kc += NT) {
+      // copies of the next tile (its ids have landed by now)
+      if (have_nx) stage_tile<H>(a, tn, gt, sA[buf ^ 1], L.dpad, cid + (buf ^ 1) * 128, ccat + (buf ^ 1) * 128);
+      group_sync(g);
+      if (have_nx && gw == 0) tile_runs(ccat + (buf ^ 1) * 128, tile_rows(nx), runs[buf ^ 1], &nruns[buf ^ 1]);
+      // observed-count delta: one thread per cluster column (warp 0 last), summed per batch run
+      const int* rn = runs[buf];
+      const int nrn = nruns[buf];
+      for (int kc = (gt + 224) & 255; kc < K; kc += 256) {
         float tot = 0.f;
-        for (int q = 0; q < nruns; ++q) {
-          const int r0 = runs[q], r1 = runs[q + 1];
+        for (int q = 0; q < nrn; ++q) {
+          const int r0 = rn[q], r1 = rn[q + 1];
           float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
           int r = r0;
           for (; r + 4 <= r1; r += 4) {
@@ -312,25 +411,25 @@ __global__ void __launch_bounds__(NT, 1) k_tc_sweep(SweepArgs a, TcLayout L) {
         }
         dsum[kc] += tot;
       }
-      // write the new assignment rows
-      for (int e = tid; e < nvalid * L.ldr_chunks; e += NT) {
-        const int r = e / L.ldr_chunks, ch = e % L.ldr_chunks;
-        const int64_t cl = cid[buf * 128 + r];
-        *(uint4*)(R + cl * a.ldr + ch * 8) = *(const uint4*)(Rst + r * L.ldst + ch * 8);
-      }
       buf ^= 1;
       have = have_nx;
       cu = nx;
     }
-    // ---- flush this CTA's delta and carry the state (CTA 0) ----------------------
+    // ---- flush the CTA's deltas and carry the state ------------------------------
     __syncthreads();
     for (int e = tid; e < (cmax - cmin + 1) * K; e += NT) {
       const size_t o_at = (size_t)cmin * K + e;
-      const double v = (double)osm[o_at];
-      if (v != 0.0) atomicAdd(&Oout[o_at], v);
+      float v = 0.f;
+#pragma unroll
+      for (int q = 0; q < NG; ++q) v += ((const float*)(sm + SL.offOsm + q * SL.osmBytes))[o_at];
+      if (v != 0.f) atomicAdd(&Oout[o_at], (double)v);
     }
-    for (int k = tid; k < K; k += NT)
-      if (dsum[k] != 0.f) atomicAdd(&Oout[(size_t)B * K + k], (double)dsum[k]);
+    for (int k = tid; k < K; k += NT) {
+      float v = 0.f;
+#pragma unroll
+      for (int q = 0; q < NG; ++q) v += dsum_s[q][k];
+      if (v != 0.f) atomicAdd(&Oout[(size_t)B * K + k], (double)v);
+    }
     // carry the state forward (O_in - old(this block) - old(next block)), spread over the CTAs
     for (size_t e = ldo * blockIdx.x / gridDim.x + tid; e < ldo * (blockIdx.x + 1) / gridDim.x; e += NT) {
       double v = Oin[e];
@@ -338,21 +437,22 @@ __global__ void __launch_bounds__(NT, 1) k_tc_sweep(SweepArgs a, TcLayout L) {
       if (Omn) v -= Omn[e];
       if (v != 0.0) atomicAdd(&Oout[e], v);
     }
-    // the similarity of the next block's first tile does not depend on the counts:
-    // start it before the barrier
-    if (have && cu.j == j + 1) {
-      tc::cp_async_wait_all();
-      tc::fence_proxy_async_smem();
-      tc::fence_before_sync();
-      __syncthreads();
-      if (tid == 0) issue_similarity_mma(tmem, sA[buf], sB, L, idesc, mbar);
-      pre_issued = true;
-    }
     if (j == a.nblk - 1) {
       const double tot = block_sum(obj_local, red);
       if (tid == 0 && tot != 0.0) atomicAdd(a.obj_acc, tot);
     }
-    grid_barrier(a.barrier, (unsigned)(j + 1) * gridDim.x, a.err);
+    grid_arrive(a.barrier);
+    // the similarity of the group's next tile (next block) does not depend on the
+    // counts: start it while the other CTAs finish this block
+    if (have && cu.j == j + 1) {
+      tc::cp_async_wait_all();
+      tc::fence_proxy_async_smem();
+      tc::fence_before_sync();
+      group_sync(g);
+      if (gt == 0) issue_similarity_mma(tmem, sA[buf], sB, L, idesc, mbar);
+      pre_issued = true;
+    }
+    grid_wait(a.barrier, (unsigned)(j + 1) * gridDim.x, a.err);
   }
 
   // ---- objective: diversity term from the final state (kernels_clustering.cuh:68-103)
@@ -376,48 +476,42 @@ __global__ void __launch_bounds__(NT, 1) k_tc_sweep(SweepArgs a, TcLayout L) {
   __syncthreads();
   if (warp == 0) {
     tc::fence_after_sync();
-    tc::tmem_dealloc(tmem, (uint32_t)L.tcols);
+    tc::tmem_dealloc(*tmem_slot, (uint32_t)(NG * L.tcols));
   }
 }
 
-template <typename H, int NT>
-static int launch_sweep_nt(const SweepArgs& a, const TcLayout& L, int occ_target, cudaStream_t st) {
-  const void* fn = (const void*)k_tc_sweep<H, NT>;
-  cudaFuncAttributes fa;
-  HB_CUDA(cudaFuncGetAttributes(&fa, fn));
-  const size_t stat = fa.sharedSizeBytes;  // static shared memory of the kernel
-  size_t smem = L.bytes;
-  const size_t per_sm = 228u * 1024u;
-  // pad the request so that no more than occ_target CTAs share an SM (TMEM budget)
-  if (per_sm / (smem + stat + 1024) > (size_t)occ_target)
-    smem = std::min<size_t>(227u * 1024u - stat, per_sm / occ_target - stat - 2048);
-  if (smem < L.bytes) smem = L.bytes;
+template <typename H, int NG>
+static int launch_sweep_ng(const SweepArgs& a, const SweepLayout& SL, cudaStream_t st) {
+  const void* fn = (const void*)k_tc_sweep<H, NG>;
+  const size_t smem = SL.bytes;
   HB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int occ = 0;
-  HB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, NT, smem));
-  occ = std::min(occ, occ_target);
+  HB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 256 * NG, smem));
   if (occ < 1) {
     set_error("tensor-core sweep: kernel does not fit on an SM");
     return HB_ERR_UNSUPPORTED;
   }
+  // one CTA per SM: the TMEM of an SM is shared out between the CTA's groups
   const int64_t tiles = std::max<int64_t>(1, (std::min<int64_t>(a.bs, a.n) + 127) / 128);
-  const int grid = (int)std::min<int64_t>((int64_t)num_sms() * occ, tiles);
+  const int grid = (int)std::min<int64_t>((int64_t)num_sms(), tiles);
   SweepArgs args = a;
-  TcLayout lay = L;
+  SweepLayout lay = SL;
   void* kargs[] = {(void*)&args, (void*)&lay};
-  HB_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(NT), kargs, smem, st));
+  HB_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(256 * NG), kargs, smem, st));
   ++g_launches;
   return HB_OK;
 }
 
 template <typename H>
 int launch_tc_sweep(const SweepArgs& a, cudaStream_t st) {
-  const TcLayout L = tc_layout(a.d, a.K, a.B, a.ldr, 4);
-  if (L.bytes > 227u * 1024u) {
+  const SweepLayout S2 = sweep_layout(a.d, a.K, a.B, a.ldr, 2);
+  if (S2.bytes <= 227u * 1024u && 2 * S2.t.tcols <= 512) return launch_sweep_ng<H, 2>(a, S2, st);
+  const SweepLayout S1 = sweep_layout(a.d, a.K, a.B, a.ldr, 1);
+  if (S1.bytes > 227u * 1024u) {
     set_error("tensor-core sweep: shared-memory tables too large (B=%d K=%d d=%d)", a.B, a.K, a.d);
     return HB_ERR_UNSUPPORTED;
   }
-  return launch_sweep_nt<H, 256>(a, L, std::max(1, 512 / L.tcols), st);
+  return launch_sweep_ng<H, 1>(a, S1, st);
 }
 template int launch_tc_sweep<__half>(const SweepArgs&, cudaStream_t);
 template int launch_tc_sweep<__nv_bfloat16>(const SweepArgs&, cudaStream_t);

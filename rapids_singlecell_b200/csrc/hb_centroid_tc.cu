@@ -127,8 +127,7 @@ struct CenColumn {
   }
   __device__ __forceinline__ void flush(const CenArgs& a) {
     if (key < 0) return;
-    atomicAdd(&a.Omin[(size_t)key * a.K + kcol], tot);
-    atomicAdd(&a.Omin[(size_t)(key - key % (a.B + 1) + a.B) * a.K + kcol], tot);
+    atomicAdd(&a.Omin[(size_t)key * a.K + kcol], tot);  // the sweep keeps no column-sum row
   }
   template <typename H>
   __device__ __forceinline__ void tile(const CenArgs& a, const CenLayout& L, int s, const int* kr,

@@ -85,7 +85,7 @@ inline SweepLayout sweep_layout(int d, int K, int B, int ldr, int ng) {
   S.offB = o; o += (uint32_t)S.t.kblk * S.t.npad * 128u;
   S.rstBytes = al(128u * S.t.ldst * 2u, 16);
   S.offRst = al(o, 16); o = S.offRst + (uint32_t)ng * S.rstBytes;
-  S.offPen = al(o, 16); o = S.offPen + (uint32_t)B * K * 4u;
+  S.offPen = al(o, 16); o = S.offPen + (uint32_t)B * S.t.npad * 4u;  // rows padded to npad
   S.osmBytes = al((uint32_t)B * K * 4u, 16);
   S.offOsm = al(o, 16); o = S.offOsm + (uint32_t)ng * S.osmBytes;
   S.offRows = al(o, 16); o = S.offRows + (uint32_t)ng * 3u * 256u * 4u;  // cid, ccat, rsp: [2][128] each
@@ -170,6 +170,19 @@ __device__ __forceinline__ void stage_tile(const SweepArgs& a, TileIds t, int gt
   }
 }
 
+// ocol[k] += sum over batches b of (O[b][k] - Om[b][k]) (ocol zeroed by the caller):
+// the rows are split over the threads, np threads per column.
+__device__ __forceinline__ void column_sums(const double* O, const double* Om, int B, int K, float* ocol,
+                                            int nt) {
+  const int np = K < nt ? nt / K : 1;
+  for (int t = threadIdx.x; t < np * K; t += nt) {
+    const int k = t % K, p = t / K;
+    double s = 0.0;
+    for (int b = p; b < B; b += np) s += O[(size_t)b * K + k] - (Om ? Om[(size_t)b * K + k] : 0.0);
+    atomicAdd(&ocol[k], (float)s);
+  }
+}
+
 // Starts of the runs of equal batch in a tile (rows are ordered by batch inside
 // a block), ascending, terminated by nvalid.  Executed by one full warp.
 __device__ __forceinline__ void tile_runs(const int* cc, int nvalid, int* runs, int* nruns) {
@@ -198,7 +211,7 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int g = tid >> 8, gt = tid & 255, gw = gt >> 5;   // thread group, index and warp in it
   const int vid = blockIdx.x * NG + g, nvw = gridDim.x * NG;  // the group's worker index, workers
-  float* pen = (float*)(sm + SL.offPen);                     // [B][K] log2 of the penalty
+  float* pen = (float*)(sm + SL.offPen);                     // [B][npad] exponent offsets
   float* osm = (float*)(sm + SL.offOsm + g * SL.osmBytes);   // [B][K] observed-count delta
   H* Rst = (H*)(sm + SL.offRst + g * SL.rstBytes);           // [128][ldst] staged rows
   int* cid = (int*)(sm + SL.offRows + g * 3072);             // [2][128] cell per row
@@ -207,12 +220,10 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
   uint64_t* mbar = (uint64_t*)(sm + SL.offMisc) + g;
   uint32_t* tmem_slot = (uint32_t*)(sm + SL.offMisc + 32);
   double* red = (double*)(sm + SL.offMisc + 64);
-  __shared__ float dsum_s[NG][256];        // column sums of the deltas (row B)
-  __shared__ double ocol[256];             // column sums of the state
+  __shared__ float ocol_s[2][256];         // column sums of the state (E / Pr_b), by block parity
   __shared__ int2 crange[kMaxBlocks];      // batch range of this CTA's slice, per block
   __shared__ int runs_s[NG][2][130];       // run starts of the two tile buffers
   __shared__ int nruns_s[NG][2];
-  float* dsum = dsum_s[g];
   int(*runs)[130] = runs_s[g];
   int* nruns = nruns_s[g];
   H* R = (H*)a.R;
@@ -241,6 +252,7 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
 
   const uint32_t idesc = tc::idesc_f16(128, L.npad, is_bf16<H>::value, false, false);
   const float c2 = (float)(-2.0 / a.sigma * 1.4426950408889634);  // exp(x) = exp2(x log2 e)
+  const int ldp = L.npad;
   const float sig = (float)a.sigma;
   const int half = gw >> 2;  // warps 0-3 / 4-7 of the group: the two column halves
   const int row = (gw & 3) * 32 + lane;
@@ -264,6 +276,8 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
     crange[j] = make_int2(cmin, lo < hi ? cmax : cmin - 1);
   }
 
+  for (int k = tid; k < 256; k += NT) ocol_s[0][k] = 0.f;
+  __syncthreads();
   for (int j = 0; j < a.nblk; ++j) {
     const double* Oin = a.Obuf[(a.b0 + j) % 3];
     double* Oout = a.Obuf[(a.b0 + j + 1) % 3];
@@ -271,30 +285,49 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
     const double* Omc = (a.Omin && j == 0) ? a.Omin : nullptr;                       // this block
     const double* Omn = (a.Omin && j + 1 < a.nblk) ? a.Omin + (size_t)(j + 1) * ldo : nullptr;  // next
     for (size_t e = (size_t)blockIdx.x * NT + tid; e < ldo; e += (size_t)gridDim.x * NT) Ozero[e] = 0.0;
-    for (int k = tid; k < K; k += NT) {
-      double s = Oin[(size_t)B * K + k];
-      if (Omc) s -= Omc[(size_t)B * K + k];
-      ocol[k] = s;
-#pragma unroll
-      for (int q = 0; q < NG; ++q) dsum_s[q][k] = 0.f;
-    }
-    __syncthreads();
+    // one round of loads: the column sums (into ocol, zeroed in the previous block)
+    // and the state entries of the first penalty rows
+    float* ocol = ocol_s[j & 1];
     const int cmin = crange[j].x, cmax = crange[j].y;
-    // log2 of the penalty rows of the batches present (kernels_pen.cuh:8-21):
-    // log2 pen = theta_b * log2((E+1)/(O[+E]+1)); zero the delta rows
-    for (int e = tid; e < (cmax - cmin + 1) * K; e += NT) {
-      const int b = cmin + e / K, k = e % K;
-      const size_t o_at = (size_t)b * K + k;
+    const int npen = (cmax - cmin + 1) * ldp;
+    constexpr int kPre = 2;
+    float opre[kPre];
 #pragma unroll
-      for (int q = 0; q < NG; ++q) ((float*)(sm + SL.offOsm + q * SL.osmBytes))[o_at] = 0.f;
-      float lp = 0.f;
-      if (!a.init_mode) {
-        const float o = (float)(Oin[o_at] - (Omc ? Omc[o_at] : 0.0));
-        const float E = (float)(a.Pr[b] * ocol[k]);
-        const float denom = a.stabilized ? (o + E + 1.f) : (o + 1.f);
-        lp = (float)a.theta[b] * log2f((E + 1.f) / denom);
+    for (int q = 0; q < kPre; ++q) {
+      const int e = tid + q * NT, k = e % ldp;
+      opre[q] = 0.f;
+      if (!a.init_mode && e < npen && k < K) {
+        const size_t o_at = (size_t)(cmin + e / ldp) * K + k;
+        opre[q] = (float)(Oin[o_at] - (Omc ? Omc[o_at] : 0.0));
       }
-      pen[o_at] = lp;
+    }
+    if (!a.init_mode) column_sums(Oin, Omc, B, K, ocol, NT);
+    for (int k = tid; k < K; k += NT) ocol_s[(j + 1) & 1][k] = 0.f;
+    __syncthreads();
+    // exponent offsets of the batches present: v = exp2(c2 (1 - s) + log2 pen)
+    // = exp2(pc - c2 s) with pc = c2 + theta_b log2((E+1)/(O[+E]+1)) (kernels_pen.cuh:8-21);
+    // padding columns get a large negative offset (v = 0).  Zero the delta rows.
+    for (int e = tid, q = 0; e < npen; e += NT, ++q) {
+      const int b = cmin + e / ldp, k = e % ldp;
+      float pc = -1e30f;
+      if (k < K) {
+        const size_t o_at = (size_t)b * K + k;
+#pragma unroll
+        for (int gq = 0; gq < NG; ++gq) ((float*)(sm + SL.offOsm + gq * SL.osmBytes))[o_at] = 0.f;
+        float lp = 0.f;
+        if (!a.init_mode) {
+          float o = 0.f;
+#pragma unroll
+          for (int i = 0; i < kPre; ++i)
+            if (q == i) o = opre[i];
+          if (q >= kPre) o = (float)(Oin[o_at] - (Omc ? Omc[o_at] : 0.0));
+          const float E = (float)a.Pr[b] * ocol[k];
+          const float denom = a.stabilized ? (o + E + 1.f) : (o + 1.f);
+          lp = (float)a.theta[b] * log2f((E + 1.f) / denom);
+        }
+        pc = c2 + lp;
+      }
+      pen[(size_t)b * ldp + k] = pc;
     }
     __syncthreads();
     // ---- this group's tiles of the block ------------------------------------------
@@ -317,45 +350,45 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
       const int nvalid = tile_rows(cu);
       const int cell = cid[buf * 128 + row];
       const int cat = ccat[buf * 128 + row];
-      const float* prow = pen + cat * K;  // log2 of the penalty row
-      // pass 1: v = exp(-2/sigma (1-s)) * pen = exp2(c2 (1-s) + log2 pen) (one SFU op),
-      // row partial sums of v, v (1-s) (kmeans error) and v * exponent (entropy);
-      // v overwrites s in TMEM.  Two 8-column loads are in flight per wait.
-      float rs = 0.f, km = 0.f, vx = 0.f;
+      const float* prow = pen + cat * ldp;  // exponent offsets of the row's batch
+      // pass 1: v = exp(-2/sigma (1-s)) * pen = exp2(pc - c2 s) (one SFU op), row
+      // partial sums of v, v s (kmeans error) and v * exponent (entropy); v
+      // overwrites s in TMEM.  Two 8-column loads are in flight per wait.
+      float rs = 0.f, kx = 0.f, vx = 0.f;
       for (int c = c_lo; c < c_hi; c += 16) {
         const bool two = c + 8 < c_hi;
-        float v[8], w2[8];
+        float v[8], w2[8], pc[16];
         tc::tmem_ld8(tl + (uint32_t)c, v);
         if (two) tc::tmem_ld8(tl + (uint32_t)(c + 8), w2);
+        *(float4*)(pc + 0) = *(const float4*)(prow + c);
+        *(float4*)(pc + 4) = *(const float4*)(prow + c + 4);
+        if (two) {
+          *(float4*)(pc + 8) = *(const float4*)(prow + c + 8);
+          *(float4*)(pc + 12) = *(const float4*)(prow + c + 12);
+        }
         tc::tmem_ld_wait();
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
           if (i >= 8 && !two) break;
           float& x = i < 8 ? v[i] : w2[i - 8];
-          const int k = c + i;
-          float val = 0.f;
-          if (k < K) {
-            const float om = 1.f - x;
-            const float ex = fmaf(c2, om, prow[k]);
-            val = tc::ex2_approx(ex);
-            km = fmaf(val, om, km);
-            vx = fmaf(val, ex, vx);
-          }
+          const float ex = fmaf(-c2, x, pc[i]);
+          const float val = tc::ex2_approx(ex);
+          kx = fmaf(val, x, kx);
+          vx = fmaf(val, ex, vx);
           rs += val;
           x = val;
         }
         tc::tmem_st8(tl + (uint32_t)c, v);
         if (two) tc::tmem_st8(tl + (uint32_t)(c + 8), w2);
       }
-      km *= 2.f;
+      const float km = 2.f * (rs - kx);  // sum v (2 (1 - s))
       tc::tmem_st_wait();
       rsp[half * 128 + row] = rs;
       group_sync(g);
       const float rsum = rsp[row] + rsp[128 + row];
       const float rsafe = a.init_mode ? fmaxf(rsum, 1e-12f) : rsum;
       const float inv = 1.f / rsafe;
-      // pass 2: normalise, round to 16 bits; write the row to R and stage it for the counts
-      H* Rrow = R + (int64_t)(cell >= 0 ? cell : 0) * a.ldr;
+      // pass 2: normalise, round to 16 bits, stage the row (for the counts and the R store)
       for (int c = c_lo; c < c_hi; c += 16) {
         const bool two = c + 8 < c_hi;
         float v[8], w2[8];
@@ -370,11 +403,8 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
         }
         *(uint4*)(Rst + row * L.ldst + c) = *(const uint4*)hv;
         if (two) *(uint4*)(Rst + row * L.ldst + c + 8) = *(const uint4*)(hv + 8);
-        if (cell >= 0) {
-          if (c < a.ldr) *(uint4*)(Rrow + c) = *(const uint4*)hv;
-          if (two && c + 8 < a.ldr) *(uint4*)(Rrow + c + 8) = *(const uint4*)(hv + 8);
-        }
       }
+      tc::fence_proxy_async_smem();  // the staged rows are the source of bulk stores
       tc::fence_before_sync();
       // objective terms of the row (kernels_kmeans.cuh:30-96, kernels_clustering.cuh:8-62):
       // kmeans error sum r (2 (1-s)); entropy sum r ln r = (ln 2 / rs) sum v x - ln rs
@@ -388,12 +418,15 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
       // copies of the next tile (its ids have landed by now)
       if (have_nx) stage_tile<H>(a, tn, gt, sA[buf ^ 1], L.dpad, cid + (buf ^ 1) * 128, ccat + (buf ^ 1) * 128);
       group_sync(g);
+      // the new assignment rows: one bulk store per row (ldr 16-bit values)
+      if (gt < nvalid) tc::bulk_store(R + (int64_t)cid[buf * 128 + gt] * a.ldr, tc::smem_u32(Rst + gt * L.ldst),
+                                      (uint32_t)a.ldr * 2u);
+      tc::bulk_commit();
       if (have_nx && gw == 0) tile_runs(ccat + (buf ^ 1) * 128, tile_rows(nx), runs[buf ^ 1], &nruns[buf ^ 1]);
       // observed-count delta: one thread per cluster column (warp 0 last), summed per batch run
       const int* rn = runs[buf];
       const int nrn = nruns[buf];
       for (int kc = (gt + 224) & 255; kc < K; kc += 256) {
-        float tot = 0.f;
         for (int q = 0; q < nrn; ++q) {
           const int r0 = rn[q], r1 = rn[q + 1];
           float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
@@ -407,10 +440,9 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
           for (; r < r1; ++r) s0 += h2f(Rst[r * L.ldst + kc]);
           const float srun = (s0 + s1) + (s2 + s3);
           osm[ccat[buf * 128 + r0] * K + kc] += srun;
-          tot += srun;
         }
-        dsum[kc] += tot;
       }
+      tc::bulk_wait_read_all();  // Rst is rewritten by the next tile (after a barrier)
       buf ^= 1;
       have = have_nx;
       cu = nx;
@@ -424,14 +456,9 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
       for (int q = 0; q < NG; ++q) v += ((const float*)(sm + SL.offOsm + q * SL.osmBytes))[o_at];
       if (v != 0.f) atomicAdd(&Oout[o_at], (double)v);
     }
-    for (int k = tid; k < K; k += NT) {
-      float v = 0.f;
-#pragma unroll
-      for (int q = 0; q < NG; ++q) v += dsum_s[q][k];
-      if (v != 0.f) atomicAdd(&Oout[(size_t)B * K + k], (double)v);
-    }
     // carry the state forward (O_in - old(this block) - old(next block)), spread over the CTAs
-    for (size_t e = ldo * blockIdx.x / gridDim.x + tid; e < ldo * (blockIdx.x + 1) / gridDim.x; e += NT) {
+    const size_t lds = (size_t)B * K;  // the batch rows (the column-sum row is not kept)
+    for (size_t e = lds * blockIdx.x / gridDim.x + tid; e < lds * (blockIdx.x + 1) / gridDim.x; e += NT) {
       double v = Oin[e];
       if (Omc) v -= Omc[e];
       if (Omn) v -= Omn[e];
@@ -458,11 +485,16 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
   // ---- objective: diversity term from the final state (kernels_clustering.cuh:68-103)
   if (blockIdx.x == 0) {
     const double* Of = a.Obuf[(a.b0 + a.nblk) % 3];
+    float* ocol = ocol_s[0];
+    for (int k = tid; k < K; k += NT) ocol[k] = 0.f;
+    __syncthreads();
+    column_sums(Of, nullptr, B, K, ocol, NT);
+    __syncthreads();
     double acc = 0.0;
     for (int e = tid; e < B * K; e += NT) {
       const int b = e / K, k = e % K;
       const double o = Of[e];
-      const double E = a.Pr[b] * Of[(size_t)B * K + k];
+      const double E = a.Pr[b] * (double)ocol[k];
       const double num_ = a.stabilized ? (o + E + 1.0) : (o + 1.0);
       acc += a.theta[b] * o * log(num_ / (E + 1.0));
     }
@@ -472,6 +504,7 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
       *a.obj_acc = 0.0;
     }
   }
+  tc::bulk_wait_all();
   tc::fence_before_sync();
   __syncthreads();
   if (warp == 0) {

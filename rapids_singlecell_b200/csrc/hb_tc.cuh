@@ -85,6 +85,22 @@ __device__ __forceinline__ void tma_gather4(uint32_t dst, const CUtensorMap* tm,
       : "memory");
 }
 
+// ---- bulk (TMA) store of contiguous bytes, shared -> global, in bulk groups ------
+// src and dst 16-byte aligned, bytes a multiple of 16.  The shared-memory source
+// must be made visible to the async proxy first (fence_proxy_async_smem by the
+// writing threads, then a barrier).
+__device__ __forceinline__ void bulk_store(void* dst, uint32_t src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(src), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// wait until the sources of all committed bulk stores of this thread have been read
+__device__ __forceinline__ void bulk_wait_read_all() {
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+// wait until all committed bulk stores of this thread are complete
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
 // ---- MMA ---------------------------------------------------------------------
 // Instruction descriptor of tcgen05.mma.kind::f16 (dense):
 //   [4,6) D format (1 = f32), [7,10) A format, [10,13) B format (0 = f16, 1 = bf16),

@@ -134,6 +134,18 @@ HB_API int hb_block_lists(int64_t n, int64_t block_size, const uint32_t* seeds, 
                    const int32_t* cats, int32_t n_batches, int32_t* idx, void* workspace,
                    size_t workspace_bytes, void* stream);
 
+/* hb_block_lists without a workspace: the scratch is a fixed device array of the library,
+ * HB_BLOCK_LISTS_STATIC_MAX_BYTES per device, and the call allocates nothing.  No counterpart in
+ * the reference (its clustering loop allocates its workspace with CuPy).  For callers that cannot
+ * allocate device memory at the call: a serving loop that must not call cudaMalloc (it
+ * synchronises the device and can fail under memory pressure), or a C host with no allocator.
+ * Returns HB_ERR_WORKSPACE when hb_block_lists_workspace_bytes() exceeds the limit.  The first
+ * call on a device looks up the array (cudaGetSymbolAddress) and should come before any stream
+ * capture.  Calls that overlap in time race on the array; it keeps the last call's contents. */
+#define HB_BLOCK_LISTS_STATIC_MAX_BYTES ((size_t)16 << 20)
+HB_API int hb_block_lists_static(int64_t n, int64_t block_size, const uint32_t* seeds, int32_t n_iters,
+                                 const int32_t* cats, int32_t n_batches, int32_t* idx, void* stream);
+
 /* penalty[b,k] = ((E+1)/(O[+E]+1)) ** theta[b]; float64 arrays [B,K], theta [B] */
 HB_API int hb_penalty(const double* E, const double* O, const double* theta, double* penalty,
                int32_t n_batches, int32_t n_clusters, int32_t stabilized, void* stream);

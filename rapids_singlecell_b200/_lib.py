@@ -28,7 +28,8 @@ PRECISIONS = {"fp32": HB_FP32, "fp64": HB_FP64, "bf16": HB_BF16, "fp16": HB_FP16
 # every symbol include/harmony_b200.h declares
 EXPORTED = (
     "hb_plan_create", "hb_plan_destroy", "hb_plan_workspace_bytes", "hb_harmonize",
-    "hb_l2_normalize", "hb_block_lists_workspace_bytes", "hb_block_lists", "hb_penalty",
+    "hb_l2_normalize", "hb_block_lists_workspace_bytes", "hb_block_lists", "hb_block_lists_static",
+    "hb_penalty",
     "hb_lambda_kb", "hb_ridge_inverse", "hb_similarity", "hb_last_error", "hb_version",
 )
 
@@ -120,6 +121,9 @@ def load() -> ctypes.CDLL:
     lib.hb_block_lists.argtypes = [c_i64, c_i64, P(ctypes.c_uint32), c_i32, c_void_p, c_i32,
                                    c_void_p, c_void_p, c_size, c_void_p]
     lib.hb_block_lists.restype = c_int
+    lib.hb_block_lists_static.argtypes = [c_i64, c_i64, P(ctypes.c_uint32), c_i32, c_void_p, c_i32,
+                                          c_void_p, c_void_p]
+    lib.hb_block_lists_static.restype = c_int
     lib.hb_penalty.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_i32, c_i32, c_i32, c_void_p]
     lib.hb_penalty.restype = c_int
     lib.hb_lambda_kb.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_i32, c_i32,

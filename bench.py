@@ -181,9 +181,9 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """dram bytes per block-update launch from the committed ncu summary, if any."""
-    f = ROOT / "profiles" / "block_update_C2_bf16.md"
+def profiled_traffic(name):
+    """dram bytes per launch of a kernel from its committed ncu summary, if any."""
+    f = ROOT / "profiles" / name
     if not f.exists():
         return None
     for line in f.read_text().splitlines():
@@ -300,19 +300,29 @@ def run_ours(args):
             dist.destroy_process_group()
         return
 
-    # ---- roofline of the dominant kernel (fused block update) ------------------
+    # ---- roofline of the dominant kernel (the persistent sweep) ----------------
+    # algorithmic bytes per cell and launch: Z_norm row read + R row write (d and K
+    # 16-bit values) + cell id and batch (8 B); one launch = one k-means iteration.
     peak, peak_kind = measured_peaks()
     achieved = prof["block_bytes"] / (prof["block_ms"] / 1e3) / 1e9 if prof["block_ms"] > 0 else 0.0
     launches = prof["block_launches"]
-    traffic = profiled_traffic()
+    cen_launches = max(1, prof["centroid_launches"])
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                "kernel": "k_tc_block_update (fused similarity + exp/penalty + normalise + O delta)",
+                "frac": achieved / peak, "traffic": profiled_traffic("k_tc_sweep_C2_bf16.md"),
+                "peak_kind": peak_kind,
+                "kernel": "k_tc_sweep (all blocks of one k-means iteration: similarity MMA, "
+                          "exp/penalty, L1 normalise, R write, observed-count delta)",
                 "algorithmic_bytes_per_launch": prof["block_bytes"] / max(1, launches),
                 "avg_launch_us": prof["block_ms"] / max(1, launches) * 1e3,
-                "block_time_share": prof["block_ms"] / ms,
-                "centroid": {"achieved_gbs": prof["centroid_bytes"] / (prof["centroid_ms"] / 1e3) / 1e9
+                "time_share": prof["block_ms"] / ms,
+                "centroid": {"kernel": "k_tc_centroid + k_centroid_reduce (Y = R^T Z_norm and the "
+                                       "per-(block, batch) sums)",
+                             "achieved_gbs": prof["centroid_bytes"] / (prof["centroid_ms"] / 1e3) / 1e9
                              if prof["centroid_ms"] > 0 else 0.0,
+                             "frac": (prof["centroid_bytes"] / (prof["centroid_ms"] / 1e3) / 1e9 / peak)
+                             if prof["centroid_ms"] > 0 else 0.0,
+                             "avg_launch_us": prof["centroid_ms"] / cen_launches * 1e3,
+                             "traffic": profiled_traffic("k_tc_centroid_C2_bf16.md"),
                              "time_share": prof["centroid_ms"] / ms}}
 
     # ---- CPU baseline (bounded sample on the host cores) -----------------------

@@ -315,6 +315,8 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
       cen[c] = AccumChunk{s, (int32_t)std::max<int64_t>(0, e - s), 0};
     }
   }
+  constexpr bool tc_corr = !std::is_same<S, float>::value && !std::is_same<S, double>::value;
+  const int64_t apply_rows = tc_corr ? 128 : 32;  // cells per apply tile (tensor-core tiles are 128 rows)
   std::vector<AccumChunk> mch;
   std::vector<int32_t> bco(B + 1, 0);
   std::vector<ApplyTile> tiles;
@@ -322,8 +324,8 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
     bco[b] = (int32_t)mch.size();
     for (int64_t s = batch_offsets[b]; s < batch_offsets[b + 1]; s += P->m_chunk_len)
       mch.push_back(AccumChunk{s, (int32_t)std::min<int64_t>(P->m_chunk_len, batch_offsets[b + 1] - s), b});
-    for (int64_t s = batch_offsets[b]; s < batch_offsets[b + 1]; s += 32)
-      tiles.push_back(ApplyTile{s, (int32_t)std::min<int64_t>(32, batch_offsets[b + 1] - s), b});
+    for (int64_t s = batch_offsets[b]; s < batch_offsets[b + 1]; s += apply_rows)
+      tiles.push_back(ApplyTile{s, (int32_t)std::min<int64_t>(apply_rows, batch_offsets[b + 1] - s), b});
   }
   bco[B] = (int32_t)mch.size();
   HB_CUDA(cudaMemcpyAsync(w.Nb, Nb.data(), sizeof(double) * B, cudaMemcpyHostToDevice, st));
@@ -494,6 +496,7 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
       HB_CUDA(cudaMemcpyAsync(&err[1], w.err, sizeof(int), cudaMemcpyDeviceToHost, st));
       HB_CUDA(cudaStreamSynchronize(st));
       if (err[0]) { set_error("block splitter candidate buffer overflow"); return HB_ERR_INTERNAL; }
+      if (err[1] == 7) { set_error("fp16 correction: |X| or |W| reaches 65504, outside the fp16 range; use bf16"); return HB_ERR_UNSUPPORTED; }
       if (err[1]) { set_error("tensor-core wait timed out (code %d)", err[1]); return HB_ERR_TIMEOUT; }
     }
     if (out && out->kmeans_objectives) {
@@ -504,15 +507,25 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
     objs.push_back(kobj.empty() ? 0.0 : kobj.back());
 
     // ---- ridge correction (correction_batched.cu:17-130) -------------------
-    HB_TRY(launch_accum<S, T, TA>(R, P->ldr, X, d, cell_index, w.m_chunks, (int)mch.size(), K, d,
-                                  (TA*)w.Mpart, st));
+    if constexpr (tc_path) {
+      HB_TRY(launch_tc_moments<S>(R, P->ldr, X, d, cell_index, w.m_chunks, (int)mch.size(), K, d,
+                                  (float*)w.Mpart, w.err, st));
+    } else {
+      HB_TRY(launch_accum<S, T, TA>(R, P->ldr, X, d, cell_index, w.m_chunks, (int)mch.size(), K, d,
+                                    (TA*)w.Mpart, st));
+    }
     HB_TRY(launch_m_reduce<TA>((TA*)w.Mpart, mch.data(), (int)mch.size(), w.batch_chunk_off, K, B, d,
                                w.M, st));
     CorrArgs ca{w.M, ring.state(), w.Pr, w.Nb, p.alpha, p.ridge_lambda, p.batch_prune_threshold,
                 p.prune, p.dynamic_lambda, K, B, d};
     HB_TRY(launch_ridge_solve<T>(ca, (T*)w.W, st));
-    HB_TRY(launch_apply_t<T, S, S>(X, d, R, P->ldr, (T*)w.W, cell_index, w.apply_tiles,
-                                   (int)tiles.size(), K, d, Zhat, d, Zn, P->ldz, st));
+    if constexpr (tc_path) {
+      HB_TRY(launch_tc_apply<S>(X, d, R, P->ldr, (const float*)w.W, cell_index, w.apply_tiles, (int)tiles.size(),
+                                K, d, Zhat, d, Zn, P->ldz, w.err, st));
+    } else {
+      HB_TRY(launch_apply_t<T, S, S>(X, d, R, P->ldr, (T*)w.W, cell_index, w.apply_tiles,
+                                     (int)tiles.size(), K, d, Zhat, d, Zn, P->ldz, st));
+    }
     // outer convergence (_harmony/__init__.py:722-734)
     const size_t m = objs.size();
     if (m >= 2 && (objs[m - 2] - objs[m - 1]) < p.tol_harmony * std::fabs(objs[m - 2])) {
@@ -520,7 +533,14 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
       break;
     }
   }
-  HB_CUDA(cudaStreamSynchronize(st));
+  {
+    // errors of the last correction (the loop checks the flags before each correction)
+    int err = 0;
+    HB_CUDA(cudaMemcpyAsync(&err, w.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    HB_CUDA(cudaStreamSynchronize(st));
+    if (err == 7) { set_error("fp16 correction: |X| or |W| reaches 65504, outside the fp16 range; use bf16"); return HB_ERR_UNSUPPORTED; }
+    if (err) { set_error("tensor-core wait timed out (code %d)", err); return HB_ERR_TIMEOUT; }
+  }
   if (prof) {
     *prof = hb_profile{};
     for (const Span& sp : spans) {

@@ -192,4 +192,14 @@ int launch_apply_t(const T* X, int ldx, const TS* R, int ldr, const T* W, const 
                    const ApplyTile* tiles, int n_tiles, int K, int d, T* Zhat, int ldzh, TZ* Zn,
                    int ldz, cudaStream_t st);
 
+// tensor-core correction of the 16-bit path (X, W float32; R, Z_norm 16-bit)
+template <typename H>
+int launch_tc_moments(const H* R, int ldr, const float* X, int ldx, const int32_t* cell_index,
+                      const AccumChunk* chunks, int n_chunks, int K, int d, float* Mpart, int* err,
+                      cudaStream_t st);
+template <typename H>
+int launch_tc_apply(const float* X, int ldx, const H* R, int ldr, const float* W, const int32_t* cell_index,
+                    const ApplyTile* tiles, int n_tiles, int K, int d, float* Zhat, int ldzh, H* Zn, int ldz,
+                    int* err, cudaStream_t st);
+
 }  // namespace hb

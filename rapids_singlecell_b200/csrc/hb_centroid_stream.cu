@@ -1,0 +1,271 @@
+// Tensor-core centroid pass of the 16-bit path, streaming in cell order.
+//
+// The same sums as k_tc_centroid (hb_centroid_tc.cu): P[cluster][pc] = sum over
+// cells of R[cell][cluster] Z_norm[cell][pc] (the centroid GEMM of the reference,
+// _cuda/harmony/clustering/clustering.cu:272-276) and, per (block, batch) key of
+// the coming sweep, the sum of the cells' R rows (the "remove old contribution"
+// terms, clustering.cu:321-332).  Here the cells are read in storage order, so
+// each 128-cell tile of Z_norm and of R is one TMA tile load instead of a row
+// gather, and the per-key sums become a second MMA against a one-hot operand:
+//   D1[cluster][pc]  += R_tile^T Z_tile
+//   D2[cluster][key] += R_tile^T H_tile,  H[cell][key] = 1 for the cell's key
+// both accumulated in TMEM over the CTA's tiles (A = R_tile^T is shared).  The
+// one-hot tile stays resident: per tile only the previous tile's ones are
+// cleared and the new ones set.  D1 and D2 are written once per CTA and summed
+// over the CTAs by k_centroid_reduce and k_opart_reduce.
+//
+// Tensor maps: Z_norm and R viewed as 4-D {64 values, 8 rows, 64-value blocks,
+// 8-row groups}, box {64, 8, blocks, 16}, so one load lands a tile in the
+// MN-major layout [group][block][8 rows x 128 B] (128B swizzle).  The blocks of
+// a row reach past its stored columns into the next row; those values only feed
+// D rows / columns that are discarded.  The row count is padded to whole tiles
+// (+8 rows) and the padding rows are zero, so they add nothing.
+#include <cudaTypedefs.h>
+#include "hb_tc_tile.cuh"
+
+namespace hb {
+
+struct CsLayout {
+  int nbZ, nbB, nbK, nM2, ncolsZ, nkpad, tcols, stages;
+  uint32_t stZ, stB, offZ, offB, offOH, offBar, bytes;
+};
+
+inline CsLayout cs_layout(int d, int K, int nkeys, int ldz) {
+  CsLayout L{};
+  L.nbZ = (ldz + 63) / 64;
+  L.ncolsZ = 64 * L.nbZ;
+  L.nM2 = (K + 127) / 128;
+  L.nbB = 2 * L.nM2;            // 64-cluster blocks in pairs (M = 128 per MMA)
+  L.nkpad = (nkeys + 15) / 16 * 16;
+  L.nbK = (L.nkpad + 63) / 64;
+  int t = 32;
+  while (t < L.nM2 * (L.ncolsZ + L.nkpad)) t <<= 1;
+  L.tcols = t;
+  L.stZ = (uint32_t)L.nbZ * 16384u;
+  L.stB = (uint32_t)L.nbB * 16384u;
+  for (int st = 4; st >= 2; --st) {
+    uint32_t o = 0;
+    L.offZ = o; o += (uint32_t)st * L.stZ;
+    L.offB = o; o += (uint32_t)st * L.stB;
+    L.offOH = o; o += (uint32_t)L.nbK * 16384u;
+    L.offBar = o; o += 8u * 8u + 16u;
+    L.bytes = o + 1024u;
+    L.stages = st;
+    if (L.bytes <= 220u * 1024u) break;
+  }
+  (void)d;
+  return L;
+}
+
+// The streaming pass applies when its accumulators fit in TMEM and its tiles in shared memory.
+bool cs_supported(int d, int K, int nkeys, int ldz) {
+  const CsLayout L = cs_layout(d, K, nkeys, ldz);
+  return d <= 128 && K <= 256 && L.nkpad <= 256 && L.nM2 * (L.ncolsZ + L.nkpad) <= 512 &&
+         L.bytes <= 220u * 1024u;
+}
+
+template <typename H>
+__global__ void __launch_bounds__(256, 1) k_tc_centroid_stream(CenStreamArgs a, CsLayout L,
+                                                               const __grid_constant__ CUtensorMap tmZ,
+                                                               const __grid_constant__ CUtensorMap tmR) {
+  extern __shared__ __align__(1024) unsigned char smem_dyn[];
+  unsigned char* sm = (unsigned char*)(((uintptr_t)smem_dyn + 1023) & ~(uintptr_t)1023);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int K = a.K, S = L.stages;
+  uint64_t* full = (uint64_t*)(sm + L.offBar);  // [S] tile landed
+  uint64_t* mma_done = full + 4;                // MMAs of a tile completed (one phase per tile)
+  uint32_t* tmem_slot = (uint32_t*)(sm + L.offBar + 64);
+  const uint32_t sm32 = tc::smem_u32(sm);
+  const int t0 = (int)((int64_t)a.ntiles * blockIdx.x / gridDim.x);
+  const int nt = (int)((int64_t)a.ntiles * (blockIdx.x + 1) / gridDim.x) - t0;
+  const uint32_t tile_bytes = (uint32_t)(L.nbZ + L.nbB) * 16384u;
+
+  if (warp == 0) {
+    tc::tmem_alloc(tmem_slot, (uint32_t)L.tcols);
+    tc::tmem_relinquish();
+    tc::fence_before_sync();
+  }
+  if (tid == 0) {
+    for (int s = 0; s < S; ++s) tc::mbar_init(full + s, 1);
+    tc::mbar_init(mma_done, 1);
+    tc::fence_mbar_init();
+  }
+  for (uint32_t e = tid * 16u; e < (uint32_t)L.nbK * 16384u; e += 256u * 16u)
+    *(uint4*)(sm + L.offOH + e) = make_uint4(0u, 0u, 0u, 0u);
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *tmem_slot;
+  if (tid == 0) {
+    for (int j = 0; j < S && j < nt; ++j) {
+      tc::mbar_arrive_expect_tx(full + j, tile_bytes);
+      tc::tma_load4d(sm32 + L.offZ + j * L.stZ, &tmZ, 0, 0, 0, (t0 + j) * 16, full + j);
+      tc::tma_load4d(sm32 + L.offB + j * L.stB, &tmR, 0, 0, 0, (t0 + j) * 16, full + j);
+    }
+  }
+  auto key_of = [&](int i) -> int {  // key of row tid of the CTA's tile i (-1 past the cells)
+    const int64_t cell = (int64_t)(t0 + i) * 128 + tid;
+    return (i < nt && cell < a.n) ? __ldg(a.ckey + cell) : -1;
+  };
+  // one-hot element (row r, key k): MN-major [group][nbK][8 rows x 128 B]
+  auto oh_off = [&](int r, int k) -> uint32_t {
+    return (uint32_t)(r >> 3) * (uint32_t)L.nbK * 1024u + (uint32_t)(k >> 6) * 1024u + (uint32_t)(r & 7) * 128u +
+           ((((uint32_t)(k & 63) >> 3) ^ (uint32_t)(r & 7)) << 4) + (uint32_t)(k & 7) * 2u;
+  };
+  int key_cur = -1, key_next = -1, key_old = -1;
+  if (tid < 128) {
+    key_cur = key_of(0);
+    key_next = key_of(1);
+  }
+  const uint32_t idesc1 = tc::idesc_f16(128, L.ncolsZ, is_bf16<H>::value, true, true);
+  const uint32_t idesc2 = tc::idesc_f16(128, L.nkpad, is_bf16<H>::value, true, true);
+  const H one = from_f<H>(1.f), zero = from_f<H>(0.f);
+
+  for (int i = 0; i < nt; ++i) {
+    const int s = i % S;
+    if (tid < 128 && i >= 1) {  // the one-hot tile and stage of tile i-1 are free once its MMAs completed
+      if (!tc::mbar_wait(mma_done, (uint32_t)((i - 1) & 1), kMaxPolls)) atomicExch(a.err, 5);
+      tc::fence_after_sync();
+    }
+    if (tid == 0 && i >= 1 && i + S - 1 < nt) {
+      const int j = i + S - 1, sj = j % S;
+      tc::mbar_arrive_expect_tx(full + sj, tile_bytes);
+      tc::tma_load4d(sm32 + L.offZ + sj * L.stZ, &tmZ, 0, 0, 0, (t0 + j) * 16, full + sj);
+      tc::tma_load4d(sm32 + L.offB + sj * L.stB, &tmR, 0, 0, 0, (t0 + j) * 16, full + sj);
+    }
+    if (tid < 128) {
+      H* oh = (H*)(sm + L.offOH);
+      if (key_old >= 0) *(H*)((unsigned char*)oh + oh_off(tid, key_old)) = zero;
+      if (key_cur >= 0) *(H*)((unsigned char*)oh + oh_off(tid, key_cur)) = one;
+      key_old = key_cur;
+      key_cur = key_next;
+      key_next = key_of(i + 2);
+      tc::fence_proxy_async_smem();
+    }
+    if (tid == 0 && !tc::mbar_wait(full + s, (uint32_t)((i / S) & 1), kMaxPolls)) atomicExch(a.err, 6);
+    tc::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after_sync();
+      const uint32_t sZ = sm32 + L.offZ + s * L.stZ, sB = sm32 + L.offB + s * L.stB, sH = sm32 + L.offOH;
+      for (int m = 0; m < L.nM2; ++m) {
+        const uint32_t d1 = tmem + (uint32_t)(m * L.ncolsZ);
+        const uint32_t d2 = tmem + (uint32_t)(L.nM2 * L.ncolsZ + m * L.nkpad);
+        for (int k = 0; k < 8; ++k) {  // 8 steps of 16 cells
+          const uint64_t ad = tc::sdesc_sw128(sB + (uint32_t)(2 * m) * 1024u + (uint32_t)k * 2u * (uint32_t)L.nbB * 1024u,
+                                              1024, (uint32_t)L.nbB * 1024u);
+          const uint64_t bz = tc::sdesc_sw128(sZ + (uint32_t)k * 2u * (uint32_t)L.nbZ * 1024u, 1024,
+                                              (uint32_t)L.nbZ * 1024u);
+          const uint64_t bh = tc::sdesc_sw128(sH + (uint32_t)k * 2u * (uint32_t)L.nbK * 1024u, 1024,
+                                              (uint32_t)L.nbK * 1024u);
+          const uint32_t acc = (i > 0 || k > 0) ? 1u : 0u;
+          tc::mma_f16(d1, ad, bz, idesc1, acc);
+          tc::mma_f16(d2, ad, bh, idesc2, acc);
+        }
+      }
+      tc::mma_commit(mma_done);
+    }
+  }
+  if (nt > 0 && !tc::mbar_wait(mma_done, (uint32_t)((nt - 1) & 1), kMaxPolls)) atomicExch(a.err, 4);
+  tc::fence_after_sync();
+  // ---- epilogue: D1 -> P[cta][cluster][pc], D2 -> Opart[cta][key][cluster] -------------
+  {
+    const int half = warp >> 2, q = warp & 3;
+    for (int m = 0; m < L.nM2; ++m) {
+      const int k = m * 128 + q * 32 + lane;
+      const uint32_t tl = tmem + ((uint32_t)(q * 32) << 16);
+      float* outP = a.P + (size_t)blockIdx.x * K * a.d;
+      const int h1 = L.ncolsZ / 2;
+      for (int c0 = half * h1; c0 < (half + 1) * h1; c0 += 8) {
+        float v[8];
+        tc::tmem_ld8(tl + (uint32_t)(m * L.ncolsZ + c0), v);
+        tc::tmem_ld_wait();
+        if (k < K)
+#pragma unroll
+          for (int i = 0; i < 8; ++i)
+            if (c0 + i < a.d) outP[(size_t)k * a.d + c0 + i] = nt > 0 ? v[i] : 0.f;
+      }
+      float* outO = a.Opart + (size_t)blockIdx.x * a.nkeys * K;
+      const int h2 = (L.nkpad / 2 + 7) / 8 * 8;
+      for (int c0 = half * h2; c0 < min(L.nkpad, (half + 1) * h2); c0 += 8) {
+        float v[8];
+        tc::tmem_ld8(tl + (uint32_t)(L.nM2 * L.ncolsZ + m * L.nkpad + c0), v);
+        tc::tmem_ld_wait();
+        if (k < K)
+#pragma unroll
+          for (int i = 0; i < 8; ++i)
+            if (c0 + i < a.nkeys) outO[(size_t)(c0 + i) * K + k] = nt > 0 ? v[i] : 0.f;
+      }
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after_sync();
+    tc::tmem_dealloc(tmem, (uint32_t)L.tcols);
+  }
+}
+
+// Omin[key][k] = sum over the G CTAs of Opart[cta][key][k], in float64 (fixed order).
+__global__ void k_opart_reduce(const float* __restrict__ Opart, int G, int nkeys, int K, double* __restrict__ Omin) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (int64_t)nkeys * K) return;
+  double s = 0.0;
+  for (int g = 0; g < G; ++g) s += (double)Opart[(size_t)g * nkeys * K + e];
+  Omin[e] = s;
+}
+
+// 4-D view {64 values, 8 rows, blocks, 8-row groups} of a [rows][ld] 16-bit array, box {64, 8, blocks, 16}.
+int make_tile_map4(CUtensorMap* tm, const void* base, int64_t rows, int ld, int blocks, bool bf16) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", (void**)&encode, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !encode) {
+      encode = nullptr;
+      set_error("cuTensorMapEncodeTiled is not available from the driver");
+      return HB_ERR_CUDA;
+    }
+  }
+  if (((uintptr_t)base & 15) || (ld * 2) % 16 || rows % 8) {
+    set_error("tile map: base must be 16-byte aligned, rows a multiple of 16 bytes and of 8");
+    return HB_ERR_INVALID;
+  }
+  cuuint64_t gdim[4] = {64, 8, (cuuint64_t)blocks, (cuuint64_t)(rows / 8)};
+  cuuint64_t gstride[3] = {(cuuint64_t)ld * 2, 128, (cuuint64_t)ld * 16};
+  cuuint32_t box[4] = {64, 8, (cuuint32_t)blocks, 16};
+  cuuint32_t estr[4] = {1, 1, 1, 1};
+  const CUresult r = encode(tm, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 4,
+                            const_cast<void*>(base), gdim, gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                            CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled (4-D tile map) failed (%d) for rows=%lld ld=%d", (int)r, (long long)rows, ld);
+    return HB_ERR_CUDA;
+  }
+  return HB_OK;
+}
+
+template <typename H>
+int launch_tc_centroid_stream(const CenStreamArgs& a, const void* Zn, int ldz, const void* R, int ldr,
+                              int64_t rows_alloc, int grid, double* Omin, cudaStream_t st) {
+  const CsLayout L = cs_layout(a.d, a.K, a.nkeys, ldz);
+  CUtensorMap tmZ, tmR;
+  HB_TRY(make_tile_map4(&tmZ, Zn, rows_alloc, ldz, L.nbZ, is_bf16<H>::value));
+  HB_TRY(make_tile_map4(&tmR, R, rows_alloc, ldr, L.nbB, is_bf16<H>::value));
+  const void* fn = (const void*)k_tc_centroid_stream<H>;
+  // one CTA per SM: the request is padded so that a second CTA never fits (TMEM)
+  const size_t smem = std::max<size_t>(L.bytes, 116u * 1024u);
+  HB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_tc_centroid_stream<H><<<grid, 256, smem, st>>>(a, L, tmZ, tmR);
+  HB_LAUNCH_CHECK();
+  const int64_t ne = (int64_t)a.nkeys * a.K;
+  k_opart_reduce<<<(unsigned)((ne + 255) / 256), 256, 0, st>>>(a.Opart, grid, a.nkeys, a.K, Omin);
+  HB_LAUNCH_CHECK();
+  return HB_OK;
+}
+template int launch_tc_centroid_stream<__half>(const CenStreamArgs&, const void*, int, const void*, int, int64_t,
+                                               int, double*, cudaStream_t);
+template int launch_tc_centroid_stream<__nv_bfloat16>(const CenStreamArgs&, const void*, int, const void*, int,
+                                                      int64_t, int, double*, cudaStream_t);
+
+}  // namespace hb

@@ -76,6 +76,9 @@ struct hb_plan {
   int cen_tiles;  // output tiles per chunk
   int max_m_chunks, max_apply_tiles;
   int64_t m_chunk_len;
+  int64_t rows_alloc;  // rows of Z_norm and R: whole 128-cell tiles + 8, the padding rows zero
+  bool cen_stream;     // 16-bit path: centroid pass in cell order (hb_centroid_stream.cu)
+  int nkeys;           // (block, batch) keys: blocks * (batches + 1)
   size_t ws_bytes;
   std::vector<cudaEvent_t> events;  // profiling pool (created on first profiled run)
   ~hb_plan() {
@@ -103,6 +106,8 @@ struct Work {
   unsigned* barrier;  // grid-barrier counter of the persistent sweep
   int32_t* idx;
   int32_t* lcat;
+  int32_t* ckey;    // cell-order (block, batch) keys of the chunk's iterations (streaming centroid pass)
+  float* Opart;     // per-CTA per-key sums of the streaming centroid pass
   int32_t* cell_index;  // cells sorted by batch (stable), built when the caller passes none
   int* err;
   AccumChunk* cen_chunks;
@@ -117,8 +122,8 @@ void carve(const hb_plan& P, Carver& cv, Work& w) {
   const hb_params& p = P.p;
   const int64_t n = p.n_cells;
   const int K = p.n_clusters, B = p.n_batches, d = p.n_pcs;
-  w.Zn = cv.take<char>((size_t)n * P.ldz * P.ssz);
-  w.R = cv.take<char>((size_t)n * P.ldr * P.ssz);
+  w.Zn = cv.take<char>((size_t)P.rows_alloc * P.ldz * P.ssz);
+  w.R = cv.take<char>((size_t)P.rows_alloc * P.ldr * P.ssz);
   w.Yn = cv.take<char>((size_t)K * P.ldy * P.ssz);
   w.Ypart = cv.take<char>((size_t)P.cen_chunks * K * d * P.asz);
   w.Mpart = cv.take<char>((size_t)P.max_m_chunks * K * d * P.asz);
@@ -135,6 +140,8 @@ void carve(const hb_plan& P, Carver& cv, Work& w) {
   w.barrier = cv.take<unsigned>(4);
   w.idx = cv.take<int32_t>((size_t)kMaxIterChunk * n);
   w.lcat = cv.take<int32_t>((size_t)kMaxIterChunk * n);
+  w.ckey = P.cen_stream ? cv.take<int32_t>((size_t)kMaxIterChunk * n) : nullptr;
+  w.Opart = P.cen_stream ? cv.take<float>((size_t)P.cen_chunks * P.nkeys * K) : nullptr;
   w.err = cv.take<int>(4);
   w.cen_chunks = cv.take<AccumChunk>(P.cen_chunks);
   w.m_chunks = cv.take<AccumChunk>(P.max_m_chunks);
@@ -212,6 +219,18 @@ int hb_plan_create(const hb_params* params, hb_plan** plan) {
   P->m_chunk_len = std::max<int64_t>(256, (p.n_cells + target - 1) / target);
   P->max_m_chunks = (int)((p.n_cells + P->m_chunk_len - 1) / P->m_chunk_len) + p.n_batches;
   P->max_apply_tiles = (int)((p.n_cells + 31) / 32) + p.n_batches;
+  P->rows_alloc = (p.n_cells + 127) / 128 * 128 + 8;
+  P->nkeys = P->ml.nblk * (p.n_batches + 1);
+  P->cen_stream = false;
+  if (P->ssz == 2 && cs_supported((int)p.n_pcs, (int)p.n_clusters, P->nkeys, P->ldz)) {
+    // the 4-D tile maps must encode for these row strides (no memory is touched)
+    CUtensorMap probe;
+    const bool bf = p.precision == HB_BF16;
+    P->cen_stream = make_tile_map4(&probe, (const void*)(uintptr_t)4096, P->rows_alloc, P->ldz, (P->ldz + 63) / 64, bf) ==
+                        HB_OK &&
+                    make_tile_map4(&probe, (const void*)(uintptr_t)4096, P->rows_alloc, P->ldr,
+                                   2 * (((int)p.n_clusters + 127) / 128), bf) == HB_OK;
+  }
   Carver cv(nullptr, 0);
   Work w;
   carve(*P, cv, w);
@@ -352,6 +371,9 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
   base.sigma = p.sigma; base.d = d; base.K = K; base.B = B; base.stabilized = p.stabilized_penalty;
 
   // ---- initial state (_harmony/__init__.py:292-353) ------------------------
+  // padding rows of Z_norm and R (read by the tile loads of the streaming centroid pass) are zero
+  HB_CUDA(cudaMemsetAsync((char*)Zn + (size_t)n * P->ldz * P->ssz, 0, (size_t)(P->rows_alloc - n) * P->ldz * P->ssz, st));
+  HB_CUDA(cudaMemsetAsync((char*)R + (size_t)n * P->ldr * P->ssz, 0, (size_t)(P->rows_alloc - n) * P->ldr * P->ssz, st));
   HB_TRY(launch_l2_normalize<T, S>(X, n, d, d, Zn, P->ldz, st));
   HB_TRY(launch_l2_normalize<T, S>(Y0, K, d, d, Yn, P->ldy, st));
   double* obj_init = w.obj_out + std::max(p.max_iter_clustering, 1);
@@ -431,7 +453,8 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
     bool stop = false;
     for (int it0 = 0; it0 < p.max_iter_clustering && !stop; it0 += kMaxIterChunk) {
       const int C = std::min(kMaxIterChunk, p.max_iter_clustering - it0);
-      HB_TRY(membership_build_dev(ml, w.mb, nullptr, seed + (uint32_t)it0, C, cats, w.idx, st, w.lcat));
+      HB_TRY(membership_build_dev(ml, w.mb, nullptr, seed + (uint32_t)it0, C, cats, w.idx, st, w.lcat,
+                                  w.ckey, B));
       for (int c = 0; c < C && !stop; ++c) {
         const int it = it0 + c;
         const int32_t* idx = w.idx + (size_t)c * n;
@@ -443,8 +466,14 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
         HB_CUDA(cudaMemsetAsync(w.Omin, 0, sizeof(double) * nblk * omsz, st));
         int sp = span_begin(1, (double)n * (zb + rb + 8));
         if constexpr (tc_path) {
-          CenArgs ca{Zn, P->ldz, R, P->ldr, cats, idx, lcat, n, ml.bs, d, K, B, (float*)w.Ypart, w.Omin, w.err};
-          HB_TRY(launch_tc_centroid<S>(ca, P->cen_chunks, st));
+          if (P->cen_stream) {
+            CenStreamArgs ca{n, (int)((P->rows_alloc - 8) / 128), w.ckey + (size_t)c * n, d, K, P->nkeys,
+                             (float*)w.Ypart, w.Opart, w.err};
+            HB_TRY(launch_tc_centroid_stream<S>(ca, Zn, P->ldz, R, P->ldr, P->rows_alloc, P->cen_chunks, w.Omin, st));
+          } else {
+            CenArgs ca{Zn, P->ldz, R, P->ldr, cats, idx, lcat, n, ml.bs, d, K, B, (float*)w.Ypart, w.Omin, w.err};
+            HB_TRY(launch_tc_centroid<S>(ca, P->cen_chunks, st));
+          }
         } else {
           HB_TRY(launch_accum<S, S, TA>(R, P->ldr, Zn, P->ldz, idx, w.cen_chunks, P->cen_chunks, K, d,
                                         (TA*)w.Ypart, st, OminArgs{w.Omin, cats, ml.bs, B}));

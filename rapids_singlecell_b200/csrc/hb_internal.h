@@ -32,13 +32,16 @@ struct MembershipBufs {
 };
 MembershipLayout membership_layout(int64_t n, int64_t bs, int nsub);
 void membership_carve(Carver& cv, const MembershipLayout& L, MembershipBufs& B);
-// lcat (optional): lcat[c*n + p] = cats[idx[c*n + p]], the batch of each list position
+// lcat (optional): lcat[c*n + p] = cats[idx[c*n + p]], the batch of each list position;
+// ckey (optional): ckey[c*n + i] = block(i) * (n_batches + 1) + cats[i], the (block, batch)
+// key of each cell
 int membership_build(const MembershipLayout& L, const MembershipBufs& B, const uint32_t* h_seeds,
                      int n_iters, const int32_t* cats, int32_t* idx, cudaStream_t st,
-                     int32_t* lcat = nullptr);
+                     int32_t* lcat = nullptr, int32_t* ckey = nullptr, int n_batches = 0);
 int membership_build_dev(const MembershipLayout& L, const MembershipBufs& B, const uint32_t* seeds,
                          uint32_t seed0, int n_iters, const int32_t* cats, int32_t* idx,
-                         cudaStream_t st, int32_t* lcat = nullptr);
+                         cudaStream_t st, int32_t* lcat = nullptr, int32_t* ckey = nullptr,
+                         int n_batches = 0);
 
 // ---- SIMT kernels of the plain (fp32 / fp64) path ----------------------------
 // Row L2 normalisation, inverse norm clamped to 1e12 (reference semantics).
@@ -165,6 +168,22 @@ struct CenArgs {
 template <typename H>
 int launch_tc_centroid(const CenArgs& a, int grid, cudaStream_t st);
 int tc_centroid_grid(int K);
+
+// centroid pass in cell order (hb_centroid_stream.cu)
+struct CenStreamArgs {
+  int64_t n;
+  int ntiles;            // 128-cell tiles over the padded rows
+  const int32_t* ckey;   // [n] (block, batch) key of each cell for the coming sweep
+  int d, K, nkeys;
+  float* P;              // [G][K][d] partial sums
+  float* Opart;          // [G][nkeys][K] partial per-key sums
+  int* err;
+};
+bool cs_supported(int d, int K, int nkeys, int ldz);
+int make_tile_map4(CUtensorMap* tm, const void* base, int64_t rows, int ld, int blocks, bool bf16);
+template <typename H>
+int launch_tc_centroid_stream(const CenStreamArgs& a, const void* Zn, int ldz, const void* R, int ldr,
+                              int64_t rows_alloc, int grid, double* Omin, cudaStream_t st);
 
 struct CorrArgs {
   const double* M;      // [K][B+1][d]

@@ -260,7 +260,8 @@ __global__ void __launch_bounds__(256) k_part_scatter(int64_t n, int64_t bs, int
                                                       const uint32_t* __restrict__ offsets,
                                                       const uint32_t* __restrict__ totals,
                                                       int ntiles, int32_t* __restrict__ idx,
-                                                      int32_t* __restrict__ lcat) {
+                                                      int32_t* __restrict__ lcat, int32_t* __restrict__ ckey,
+                                                      int B) {
   extern __shared__ uint32_t dyn[];
   const int nbk = nblk * nsub;
   uint32_t* base = dyn;               // [nbk]
@@ -304,7 +305,9 @@ __global__ void __launch_bounds__(256) k_part_scatter(int64_t n, int64_t bs, int
     if (valid) {
       const uint32_t at = wc[w * nbk + bk] + lrank;
       out[at] = (int32_t)i;
-      if (lcat) lcat[(size_t)c * n + at] = cats ? cats[i] : 0;
+      const int cat = cats ? cats[i] : 0;
+      if (lcat) lcat[(size_t)c * n + at] = cat;
+      if (ckey) ckey[(size_t)c * n + i] = (int)((int64_t)at / bs) * (B + 1) + cat;
     }
     __syncthreads();
     for (int j = t; j < nbk; j += 256) {
@@ -355,20 +358,21 @@ void membership_carve(Carver& cv, const MembershipLayout& L, MembershipBufs& B) 
 // Writes, for each of `n_iters` (<= kMaxIterChunk) seeds, the cell list of every
 // block: idx[c*n + j*bs + r] is the r-th cell (ascending) of block j.
 int membership_build(const MembershipLayout& L, const MembershipBufs& B, const uint32_t* h_seeds,
-                     int n_iters, const int32_t* cats, int32_t* idx, cudaStream_t st, int32_t* lcat) {
+                     int n_iters, const int32_t* cats, int32_t* idx, cudaStream_t st, int32_t* lcat,
+                     int32_t* ckey, int n_batches) {
   if (n_iters < 1 || n_iters > kMaxIterChunk) {
     set_error("membership_build: n_iters out of range");
     return HB_ERR_INVALID;
   }
   HB_CUDA(cudaMemcpyAsync(B.seeds, h_seeds, sizeof(uint32_t) * n_iters, cudaMemcpyHostToDevice, st));
-  return membership_build_dev(L, B, B.seeds, 0, n_iters, cats, idx, st, lcat);
+  return membership_build_dev(L, B, B.seeds, 0, n_iters, cats, idx, st, lcat, ckey, n_batches);
 }
 
 // Block lists for the consecutive seeds seed0 .. seed0+n_iters-1 (no host copy),
 // or for the device list `seeds` when it is not null.
 int membership_build_dev(const MembershipLayout& L, const MembershipBufs& B, const uint32_t* seeds,
                          uint32_t seed0, int n_iters, const int32_t* cats, int32_t* idx,
-                         cudaStream_t st, int32_t* lcat) {
+                         cudaStream_t st, int32_t* lcat, int32_t* ckey, int n_batches) {
   const int nb = L.nblk - 1;
   const int sms = num_sms();
   const int nsub = cats ? L.nsub : 1;
@@ -405,7 +409,8 @@ int membership_build_dev(const MembershipLayout& L, const MembershipBufs& B, con
   if (ssm > 48 * 1024)
     HB_CUDA(cudaFuncSetAttribute(k_part_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm));
   k_part_scatter<<<dim3(L.ntiles, n_iters), 256, ssm, st>>>(L.n, L.bs, L.nblk, nsub, cats, seeds, seed0,
-                                                           B.split, B.offsets, B.totals, L.ntiles, idx, lcat);
+                                                           B.split, B.offsets, B.totals, L.ntiles, idx, lcat, ckey,
+                                                           n_batches);
   HB_LAUNCH_CHECK();
   return HB_OK;
 }

@@ -101,6 +101,16 @@ __device__ __forceinline__ void bulk_wait_read_all() {
 // wait until all committed bulk stores of this thread are complete
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
+// ---- TMA tile load (no multicast) of a 4-D tensor map box at {x0, x1, x2, x3} ------
+__device__ __forceinline__ void tma_load4d(uint32_t dst, const CUtensorMap* tm, int x0, int x1, int x2, int x3,
+                                           uint64_t* mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(dst),
+      "l"((uint64_t)tm), "r"(x0), "r"(x1), "r"(x2), "r"(x3), "r"(smem_u32(mbar))
+      : "memory");
+}
+
 // ---- MMA ---------------------------------------------------------------------
 // Instruction descriptor of tcgen05.mma.kind::f16 (dense):
 //   [4,6) D format (1 = f32), [7,10) A format, [10,13) B format (0 = f16, 1 = bf16),

@@ -48,7 +48,7 @@ inline CsLayout cs_layout(int d, int K, int nkeys, int ldz) {
     L.offZ = o; o += (uint32_t)st * L.stZ;
     L.offB = o; o += (uint32_t)st * L.stB;
     L.offOH = o; o += (uint32_t)L.nbK * 16384u;
-    L.offBar = o; o += 8u * 8u + 16u;
+    L.offBar = o; o += 16u * 8u + 16u;
     L.bytes = o + 1024u;
     L.stages = st;
     if (L.bytes <= 220u * 1024u) break;
@@ -64,6 +64,10 @@ bool cs_supported(int d, int K, int nkeys, int ldz) {
          L.bytes <= 220u * 1024u;
 }
 
+__device__ __forceinline__ void mbar_arrive_cta(uint64_t* m) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc::smem_u32(m)) : "memory");
+}
+
 template <typename H>
 __global__ void __launch_bounds__(256, 1) k_tc_centroid_stream(CenStreamArgs a, CsLayout L,
                                                                const __grid_constant__ CUtensorMap tmZ,
@@ -74,7 +78,9 @@ __global__ void __launch_bounds__(256, 1) k_tc_centroid_stream(CenStreamArgs a, 
   const int K = a.K, S = L.stages;
   uint64_t* full = (uint64_t*)(sm + L.offBar);  // [S] tile landed
   uint64_t* mma_done = full + 4;                // MMAs of a tile completed (one phase per tile)
-  uint32_t* tmem_slot = (uint32_t*)(sm + L.offBar + 64);
+  uint64_t* oh_ready = full + 5;                // one-hot of the next tile written (one phase per tile)
+  uint64_t* empty = full + 6;                   // [S] MMAs of the stage's last tile completed
+  uint32_t* tmem_slot = (uint32_t*)(sm + L.offBar + 128);
   const uint32_t sm32 = tc::smem_u32(sm);
   const int t0 = (int)((int64_t)a.ntiles * blockIdx.x / gridDim.x);
   const int nt = (int)((int64_t)a.ntiles * (blockIdx.x + 1) / gridDim.x) - t0;
@@ -88,6 +94,8 @@ __global__ void __launch_bounds__(256, 1) k_tc_centroid_stream(CenStreamArgs a, 
   if (tid == 0) {
     for (int s = 0; s < S; ++s) tc::mbar_init(full + s, 1);
     tc::mbar_init(mma_done, 1);
+    tc::mbar_init(oh_ready, 4);
+    for (int s = 0; s < S; ++s) tc::mbar_init(empty + s, 1);
     tc::fence_mbar_init();
   }
   for (uint32_t e = tid * 16u; e < (uint32_t)L.nbK * 16384u; e += 256u * 16u)
@@ -102,49 +110,20 @@ __global__ void __launch_bounds__(256, 1) k_tc_centroid_stream(CenStreamArgs a, 
       tc::tma_load4d(sm32 + L.offB + j * L.stB, &tmR, 0, 0, 0, (t0 + j) * 16, full + j);
     }
   }
-  auto key_of = [&](int i) -> int {  // key of row tid of the CTA's tile i (-1 past the cells)
-    const int64_t cell = (int64_t)(t0 + i) * 128 + tid;
-    return (i < nt && cell < a.n) ? __ldg(a.ckey + cell) : -1;
-  };
-  // one-hot element (row r, key k): MN-major [group][nbK][8 rows x 128 B]
-  auto oh_off = [&](int r, int k) -> uint32_t {
-    return (uint32_t)(r >> 3) * (uint32_t)L.nbK * 1024u + (uint32_t)(k >> 6) * 1024u + (uint32_t)(r & 7) * 128u +
-           ((((uint32_t)(k & 63) >> 3) ^ (uint32_t)(r & 7)) << 4) + (uint32_t)(k & 7) * 2u;
-  };
-  int key_cur = -1, key_next = -1, key_old = -1;
-  if (tid < 128) {
-    key_cur = key_of(0);
-    key_next = key_of(1);
-  }
   const uint32_t idesc1 = tc::idesc_f16(128, L.ncolsZ, is_bf16<H>::value, true, true);
   const uint32_t idesc2 = tc::idesc_f16(128, L.nkpad, is_bf16<H>::value, true, true);
-  const H one = from_f<H>(1.f), zero = from_f<H>(0.f);
-
-  for (int i = 0; i < nt; ++i) {
-    const int s = i % S;
-    if (tid < 128 && i >= 1) {  // the one-hot tile and stage of tile i-1 are free once its MMAs completed
-      if (!tc::mbar_wait(mma_done, (uint32_t)((i - 1) & 1), kMaxPolls)) atomicExch(a.err, 5);
-      tc::fence_after_sync();
-    }
-    if (tid == 0 && i >= 1 && i + S - 1 < nt) {
-      const int j = i + S - 1, sj = j % S;
-      tc::mbar_arrive_expect_tx(full + sj, tile_bytes);
-      tc::tma_load4d(sm32 + L.offZ + sj * L.stZ, &tmZ, 0, 0, 0, (t0 + j) * 16, full + sj);
-      tc::tma_load4d(sm32 + L.offB + sj * L.stB, &tmR, 0, 0, 0, (t0 + j) * 16, full + sj);
-    }
-    if (tid < 128) {
-      H* oh = (H*)(sm + L.offOH);
-      if (key_old >= 0) *(H*)((unsigned char*)oh + oh_off(tid, key_old)) = zero;
-      if (key_cur >= 0) *(H*)((unsigned char*)oh + oh_off(tid, key_cur)) = one;
-      key_old = key_cur;
-      key_cur = key_next;
-      key_next = key_of(i + 2);
-      tc::fence_proxy_async_smem();
-    }
-    if (tid == 0 && !tc::mbar_wait(full + s, (uint32_t)((i / S) & 1), kMaxPolls)) atomicExch(a.err, 6);
-    tc::fence_before_sync();
-    __syncthreads();
-    if (tid == 0) {
+  // Roles (no CTA-wide barrier inside the loop):
+  //   thread 0      MMA issuer: waits for the tile (full[s]) and its one-hot (oh_ready),
+  //                 commits to mma_done (one phase per tile);
+  //   thread 32     TMA producer: loads tile j into its stage once the MMAs of the
+  //                 stage's previous tile completed (empty[s]);
+  //   warps 4-7     one-hot writers (row = thread - 128): once tile i-1's MMAs
+  //                 completed, clear its ones and set tile i's; one arrival per warp.
+  if (tid == 0) {
+    for (int i = 0; i < nt; ++i) {
+      const int s = i % S;
+      if (!tc::mbar_wait(full + s, (uint32_t)((i / S) & 1), kMaxPolls)) atomicExch(a.err, 6);
+      if (!tc::mbar_wait(oh_ready, (uint32_t)(i & 1), kMaxPolls)) atomicExch(a.err, 6);
       tc::fence_after_sync();
       const uint32_t sZ = sm32 + L.offZ + s * L.stZ, sB = sm32 + L.offB + s * L.stB, sH = sm32 + L.offOH;
       for (int m = 0; m < L.nM2; ++m) {
@@ -162,7 +141,47 @@ __global__ void __launch_bounds__(256, 1) k_tc_centroid_stream(CenStreamArgs a, 
           tc::mma_f16(d2, ad, bh, idesc2, acc);
         }
       }
+      tc::mma_commit(empty + s);
       tc::mma_commit(mma_done);
+    }
+  } else if (tid == 32) {
+    for (int j = S; j < nt; ++j) {  // tile j reuses the stage of tile j - S
+      const int sj = j % S;
+      if (!tc::mbar_wait(empty + sj, (uint32_t)(((j / S) + 1) & 1), kMaxPolls)) atomicExch(a.err, 5);
+      tc::mbar_arrive_expect_tx(full + sj, tile_bytes);
+      tc::tma_load4d(sm32 + L.offZ + sj * L.stZ, &tmZ, 0, 0, 0, (t0 + j) * 16, full + sj);
+      tc::tma_load4d(sm32 + L.offB + sj * L.stB, &tmR, 0, 0, 0, (t0 + j) * 16, full + sj);
+    }
+  } else if (warp >= 4) {
+    const int row = tid - 128;
+    auto key_of = [&](int i) -> int {  // key of row `row` of the CTA's tile i (-1 past the cells)
+      const int64_t cell = (int64_t)(t0 + i) * 128 + row;
+      return (i < nt && cell < a.n) ? __ldg(a.ckey + cell) : -1;
+    };
+    // one-hot element (row r, key k): MN-major [group][nbK][8 rows x 128 B]
+    auto oh_off = [&](int r, int k) -> uint32_t {
+      return (uint32_t)(r >> 3) * (uint32_t)L.nbK * 1024u + (uint32_t)(k >> 6) * 1024u + (uint32_t)(r & 7) * 128u +
+             ((((uint32_t)(k & 63) >> 3) ^ (uint32_t)(r & 7)) << 4) + (uint32_t)(k & 7) * 2u;
+    };
+    const H one = from_f<H>(1.f), zero = from_f<H>(0.f);
+    unsigned char* oh = sm + L.offOH;
+    int kq[4];  // keys of tiles i .. i+3
+#pragma unroll
+    for (int q = 0; q < 4; ++q) kq[q] = key_of(q);
+    int key_old = -1;
+    for (int i = 0; i < nt; ++i) {
+      if (i >= 1 && !tc::mbar_wait(mma_done, (uint32_t)((i - 1) & 1), kMaxPolls)) atomicExch(a.err, 5);
+      const int key = kq[0];
+      if (key_old >= 0) *(H*)(oh + oh_off(row, key_old)) = zero;
+      if (key >= 0) *(H*)(oh + oh_off(row, key)) = one;
+      key_old = key;
+      kq[0] = kq[1];
+      kq[1] = kq[2];
+      kq[2] = kq[3];
+      kq[3] = key_of(i + 4);
+      tc::fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) mbar_arrive_cta(oh_ready);
     }
   }
   if (nt > 0 && !tc::mbar_wait(mma_done, (uint32_t)((nt - 1) & 1), kMaxPolls)) atomicExch(a.err, 4);

@@ -263,6 +263,7 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
   uint32_t phase = 0;
   int buf = 0;
   bool pre_issued = false;  // the MMA of the group's current tile was issued before the last barrier
+  int pend_rows = 0, pend_buf = 0;  // rows of the block's last tile whose R store is deferred
   // batch range of every block's CTA slice (the list is ordered by batch within a block);
   // the CTA slice is the union of its groups' slices
   for (int j = tid; j < a.nblk; j += NT) {
@@ -418,10 +419,18 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
       // copies of the next tile (its ids have landed by now)
       if (have_nx) stage_tile<H>(a, tn, gt, sA[buf ^ 1], L.dpad, cid + (buf ^ 1) * 128, ccat + (buf ^ 1) * 128);
       group_sync(g);
-      // the new assignment rows: one bulk store per row (ldr 16-bit values)
-      if (gt < nvalid) tc::bulk_store(R + (int64_t)cid[buf * 128 + gt] * a.ldr, tc::smem_u32(Rst + gt * L.ldst),
-                                      (uint32_t)a.ldr * 2u);
-      tc::bulk_commit();
+      // the new assignment rows: one bulk store per row (ldr 16-bit values).  The last
+      // tile of the block stores its rows after the grid arrival, while the other CTAs
+      // finish the block (nothing reads R during the sweep).
+      const bool last_of_block = !(have_nx && nx.j == j);
+      if (!last_of_block) {
+        if (gt < nvalid) tc::bulk_store(R + (int64_t)cid[buf * 128 + gt] * a.ldr, tc::smem_u32(Rst + gt * L.ldst),
+                                        (uint32_t)a.ldr * 2u);
+        tc::bulk_commit();
+      } else {
+        pend_rows = nvalid;
+        pend_buf = buf;
+      }
       if (have_nx && gw == 0) tile_runs(ccat + (buf ^ 1) * 128, tile_rows(nx), runs[buf ^ 1], &nruns[buf ^ 1]);
       // observed-count delta: one thread per cluster column (warp 0 last), summed per batch run
       const int* rn = runs[buf];
@@ -442,7 +451,7 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
           osm[ccat[buf * 128 + r0] * K + kc] += srun;
         }
       }
-      tc::bulk_wait_read_all();  // Rst is rewritten by the next tile (after a barrier)
+      if (!last_of_block) tc::bulk_wait_read_all();  // Rst is rewritten by the next tile (after a barrier)
       buf ^= 1;
       have = have_nx;
       cu = nx;
@@ -469,6 +478,14 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
       if (tid == 0 && tot != 0.0) atomicAdd(a.obj_acc, tot);
     }
     grid_arrive(a.barrier);
+    if (pend_rows > 0) {  // coalesced 16-byte stores: consecutive threads on consecutive chunks of a row
+      const int nch = a.ldr / 8;
+      for (int e = gt; e < pend_rows * nch; e += 256) {
+        const int r = e / nch, c = e - r * nch;
+        *(uint4*)(R + (int64_t)cid[pend_buf * 128 + r] * a.ldr + c * 8) = *(const uint4*)(Rst + r * L.ldst + c * 8);
+      }
+      pend_rows = 0;
+    }
     // the similarity of the group's next tile (next block) does not depend on the
     // counts: start it while the other CTAs finish this block
     if (have && cu.j == j + 1) {

@@ -224,13 +224,16 @@ __global__ void __launch_bounds__(256, 1) k_tc_centroid_stream(CenStreamArgs a, 
   }
 }
 
-// Omin[key][k] = sum over the G CTAs of Opart[cta][key][k], in float64 (fixed order).
+// Omin[key][k] += sum over the G CTAs of Opart[cta][key][k] (Omin zeroed by the caller).
+// blockIdx.y takes every gridDim.y-th CTA partial; its float64 sum is added atomically.
 __global__ void k_opart_reduce(const float* __restrict__ Opart, int G, int nkeys, int K, double* __restrict__ Omin) {
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= (int64_t)nkeys * K) return;
+  const int64_t ne = (int64_t)nkeys * K;
+  if (e >= ne) return;
   double s = 0.0;
-  for (int g = 0; g < G; ++g) s += (double)Opart[(size_t)g * nkeys * K + e];
-  Omin[e] = s;
+#pragma unroll 4
+  for (int g = blockIdx.y; g < G; g += gridDim.y) s += (double)__ldg(Opart + (size_t)g * ne + e);
+  if (s != 0.0) atomicAdd(Omin + e, s);
 }
 
 // 4-D view {64 values, 8 rows, blocks, 8-row groups} of a [rows][ld] 16-bit array, box {64, 8, blocks, 16}.
@@ -278,7 +281,7 @@ int launch_tc_centroid_stream(const CenStreamArgs& a, const void* Zn, int ldz, c
   k_tc_centroid_stream<H><<<grid, 256, smem, st>>>(a, L, tmZ, tmR);
   HB_LAUNCH_CHECK();
   const int64_t ne = (int64_t)a.nkeys * a.K;
-  k_opart_reduce<<<(unsigned)((ne + 255) / 256), 256, 0, st>>>(a.Opart, grid, a.nkeys, a.K, Omin);
+  k_opart_reduce<<<dim3((unsigned)((ne + 255) / 256), 8), 256, 0, st>>>(a.Opart, grid, a.nkeys, a.K, Omin);
   HB_LAUNCH_CHECK();
   return HB_OK;
 }

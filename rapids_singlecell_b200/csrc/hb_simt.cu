@@ -214,7 +214,8 @@ __device__ __forceinline__ void reduce_rows_into(const TA* __restrict__ P, int q
   // part: [RED_Y][d] scratch, out: [d]
   for (int c = threadIdx.x; c < d; c += 32) {
     double s = 0;
-    for (int q = q0 + (int)threadIdx.y; q < q1; q += RED_Y) s += (double)P[(size_t)q * stride + off + c];
+#pragma unroll 8
+    for (int q = q0 + (int)threadIdx.y; q < q1; q += RED_Y) s += (double)__ldg(P + (size_t)q * stride + off + c);
     part[threadIdx.y * d + c] = s;
   }
   __syncthreads();

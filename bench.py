@@ -315,14 +315,14 @@ def run_ours(args):
                 "algorithmic_bytes_per_launch": prof["block_bytes"] / max(1, launches),
                 "avg_launch_us": prof["block_ms"] / max(1, launches) * 1e3,
                 "time_share": prof["block_ms"] / ms,
-                "centroid": {"kernel": "k_tc_centroid + k_centroid_reduce (Y = R^T Z_norm and the "
-                                       "per-(block, batch) sums)",
+                "centroid": {"kernel": "k_tc_centroid_stream + reductions (Y = R^T Z_norm and the "
+                                       "per-(block, batch) sums, cell order)",
                              "achieved_gbs": prof["centroid_bytes"] / (prof["centroid_ms"] / 1e3) / 1e9
                              if prof["centroid_ms"] > 0 else 0.0,
                              "frac": (prof["centroid_bytes"] / (prof["centroid_ms"] / 1e3) / 1e9 / peak)
                              if prof["centroid_ms"] > 0 else 0.0,
                              "avg_launch_us": prof["centroid_ms"] / cen_launches * 1e3,
-                             "traffic": profiled_traffic("k_tc_centroid_C2_bf16.md"),
+                             "traffic": profiled_traffic("k_tc_centroid_stream_C2_bf16.md"),
                              "time_share": prof["centroid_ms"] / ms}}
 
     # ---- CPU baseline (bounded sample on the host cores) -----------------------

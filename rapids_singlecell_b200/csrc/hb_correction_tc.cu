@@ -197,8 +197,8 @@ template int launch_tc_moments<__nv_bfloat16>(const __nv_bfloat16*, int, const f
 // ---------------------------------------------------------------------------
 // Apply
 struct ApLayout {
-  int npad, kblk, nbX, ncols, tcols;
-  uint32_t offA, offWh, offWl, offId, offSs, offMisc, bytes;
+  int npad, kblk, nbX, ncols, tcols, ldxs;
+  uint32_t offA, offWh, offWl, offX, offId, offSs, offMisc, bytes;
 };
 
 inline ApLayout ap_layout(int K, int d) {
@@ -215,8 +215,10 @@ inline ApLayout ap_layout(int K, int d) {
   const uint32_t wt = (uint32_t)(L.npad / 8) * L.nbX * 1024u;  // npad rows of W_b, MN-major
   L.offWh = o; o += wt;
   L.offWl = o; o += wt;
+  L.ldxs = d + 1;  // odd row stride: a warp reading one column of 32 rows hits 32 banks
+  L.offX = o; o += 128u * (uint32_t)L.ldxs * 4u;
   L.offId = o; o += 128u * 4u;
-  L.offSs = o; o += 2u * 128u * 4u;
+  L.offSs = o; o += 3u * 128u * 4u;
   L.offMisc = o; o += 16u;
   L.bytes = o + 1024u;
   return L;
@@ -290,6 +292,19 @@ __global__ void __launch_bounds__(256) k_tc_apply(const float* __restrict__ X, i
       tc::cp_async16(sm32 + L.offA + (uint32_t)(c >> 3) * 16384u + tc::sw128_off((uint32_t)r, (uint32_t)(c & 7)),
                      ok ? (const void*)(R + (int64_t)cell * ldr + c * 8) : (const void*)R, ok ? 16u : 0u);
     }
+    // X rows of the tile (coalesced: consecutive threads on consecutive columns of a row)
+    {
+      float* sX = (float*)(sm + L.offX);
+      const int dr = 256 / d, dc = 256 % d;
+      int r = tid / d, c = tid % d;
+      for (; r < 128;) {
+        const int cell = ids[r];
+        sX[r * L.ldxs + c] = cell >= 0 ? __ldg(X + (int64_t)cell * ldx + c) : 0.f;
+        r += dr;
+        c += dc;
+        if (c >= d) { c -= d; ++r; }
+      }
+    }
     tc::cp_async_wait_all();
     tc::fence_proxy_async_smem();
     tc::fence_before_sync();
@@ -311,47 +326,62 @@ __global__ void __launch_bounds__(256) k_tc_apply(const float* __restrict__ X, i
     if (!tc::mbar_wait(mbar, phase, kMaxPolls)) atomicExch(err, 8);
     phase ^= 1u;
     tc::fence_after_sync();
-    // epilogue: z = X - D, Z_hat, then the row's L2 norm over both halves -> Z_norm
-    const int cell = ids[row];
-    float z[64];
-    float ss = 0.f;
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      if (q * 8 < hc) {
-        const int c0 = half * hc + q * 8;
-        float v[8];
-        tc::tmem_ld8(tl + (uint32_t)c0, v);
-        tc::tmem_ld_wait();
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          const int c = c0 + i;
-          float zz = 0.f;
-          if (cell >= 0 && c < d) {
-            zz = __ldg(X + (int64_t)cell * ldx + c) - v[i];
-            Zhat[(int64_t)cell * ldzh + c] = zz;
-          }
-          z[q * 8 + i] = zz;
-          ss = fmaf(zz, zz, ss);
-        }
-      }
-    }
-    ssp[half * 128 + row] = ss;
-    tc::fence_before_sync();
-    __syncthreads();
-    float inv = rsqrtf(ssp[row] + ssp[128 + row]);
-    if (inv > 1e12f) inv = 1e12f;
-    if (cell >= 0) {
+    // epilogue: z = X - D in shared memory, the row's L2 norm over both column halves, then
+    // Z_hat and Z_norm with coalesced stores (consecutive threads on consecutive columns)
+    float* sX = (float*)(sm + L.offX);
+    float* sinv = ssp + 256;
+    {
+      float ss = 0.f;
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
-        const int c0 = half * hc + q * 8;
-        if (q * 8 < hc && c0 < ldz) {
-          __align__(16) H h[8];
+        if (q * 8 < hc) {
+          const int c0 = half * hc + q * 8;
+          float v[8];
+          tc::tmem_ld8(tl + (uint32_t)c0, v);
+          tc::tmem_ld_wait();
 #pragma unroll
-          for (int i = 0; i < 8; ++i) h[i] = from_f<H>(z[q * 8 + i] * inv);
-          *(uint4*)(Zn + (int64_t)cell * ldz + c0) = *(const uint4*)h;
+          for (int i = 0; i < 8; ++i) {
+            const int c = c0 + i;
+            if (c < d) {
+              const float zz = sX[row * L.ldxs + c] - v[i];
+              sX[row * L.ldxs + c] = zz;
+              ss = fmaf(zz, zz, ss);
+            }
+          }
         }
       }
+      ssp[half * 128 + row] = ss;
     }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (tid < 128) {
+      float inv = rsqrtf(ssp[tid] + ssp[128 + tid]);
+      sinv[tid] = inv > 1e12f ? 1e12f : inv;
+    }
+    __syncthreads();
+    {
+      const int dr = 256 / d, dc = 256 % d;
+      int r = tid / d, c = tid % d;
+      for (; r < tile.len;) {
+        Zhat[(int64_t)ids[r] * ldzh + c] = sX[r * L.ldxs + c];
+        r += dr;
+        c += dc;
+        if (c >= d) { c -= d; ++r; }
+      }
+      const int nch = ldz / 8;
+      for (int e = tid; e < tile.len * nch; e += 256) {
+        const int rr = e / nch, ch = e - rr * nch;
+        const float inv = sinv[rr];
+        __align__(16) H h[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const int cc = ch * 8 + i;
+          h[i] = from_f<H>(cc < d ? sX[rr * L.ldxs + cc] * inv : 0.f);
+        }
+        *(uint4*)(Zn + (int64_t)ids[rr] * ldz + ch * 8) = *(const uint4*)h;
+      }
+    }
+    __syncthreads();  // ids, sX and the TMEM accumulator are reused by the next tile
   }
   if (bad) atomicExch(err, 7);
   tc::fence_before_sync();

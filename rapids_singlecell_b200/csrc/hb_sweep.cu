@@ -108,27 +108,27 @@ struct Cursor {
   int64_t pos, hi;
 };
 
-__device__ __forceinline__ bool cursor_first(const SweepArgs& a, int j, int v, int nv, Cursor& cu) {
+// sl[j] = the group's slice of block j (list positions [x, y)), precomputed per kernel
+__device__ __forceinline__ bool cursor_first(const SweepArgs& a, int j, const int2* sl, Cursor& cu) {
   for (; j < a.nblk; ++j) {
-    int64_t lo, hi;
-    slice_of(a, j, v, nv, lo, hi);
-    if (lo < hi) {
+    const int2 r = sl[j];
+    if (r.x < r.y) {
       cu.j = j;
-      cu.pos = lo;
-      cu.hi = hi;
+      cu.pos = r.x;
+      cu.hi = r.y;
       return true;
     }
   }
   return false;
 }
 
-__device__ __forceinline__ bool cursor_next(const SweepArgs& a, const Cursor& cu, int v, int nv, Cursor& nx) {
+__device__ __forceinline__ bool cursor_next(const SweepArgs& a, const Cursor& cu, const int2* sl, Cursor& nx) {
   if (cu.pos + 128 < cu.hi) {
     nx = cu;
     nx.pos = cu.pos + 128;
     return true;
   }
-  return cursor_first(a, cu.j + 1, v, nv, nx);
+  return cursor_first(a, cu.j + 1, sl, nx);
 }
 
 __device__ __forceinline__ int tile_rows(const Cursor& cu) {
@@ -210,7 +210,7 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
   const int K = a.K, B = a.B;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int g = tid >> 8, gt = tid & 255, gw = gt >> 5;   // thread group, index and warp in it
-  const int vid = blockIdx.x * NG + g, nvw = gridDim.x * NG;  // the group's worker index, workers
+  const int nvw = gridDim.x * NG;  // workers (thread groups) of the launch
   float* pen = (float*)(sm + SL.offPen);                     // [B][npad] exponent offsets
   float* osm = (float*)(sm + SL.offOsm + g * SL.osmBytes);   // [B][K] observed-count delta
   H* Rst = (H*)(sm + SL.offRst + g * SL.rstBytes);           // [128][ldst] staged rows
@@ -222,6 +222,7 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
   double* red = (double*)(sm + SL.offMisc + 64);
   __shared__ float ocol_s[2][256];         // column sums of the state (E / Pr_b), by block parity
   __shared__ int2 crange[kMaxBlocks];      // batch range of this CTA's slice, per block
+  __shared__ int2 gslice[NG][kMaxBlocks];  // each group's slice of every block (list positions)
   __shared__ int runs_s[NG][2][130];       // run starts of the two tile buffers
   __shared__ int nruns_s[NG][2];
   int(*runs)[130] = runs_s[g];
@@ -231,6 +232,9 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
                           tc::smem_u32(sm + SL.offA + (uint32_t)(2 * g + 1) * SL.atile)};
   const uint32_t sB = tc::smem_u32(sm + SL.offB);
   const size_t ldo = (size_t)(B + 1) * K;
+  // this CTA's share of the state carry (the batch rows; the column-sum row is not kept)
+  const int carry0 = (int)((int64_t)B * K * blockIdx.x / gridDim.x);
+  const int carry1 = (int)((int64_t)B * K * (blockIdx.x + 1) / gridDim.x);
 
   if (warp == 0) {
     tc::tmem_alloc(tmem_slot, (uint32_t)(NG * L.tcols));
@@ -242,8 +246,16 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
     tc::fence_mbar_init();
   }
   load_centroids_swizzled((const H*)a.Yn, a.ldy, K, sB, L);
+  for (int e = tid; e < NG * a.nblk; e += NT) {
+    const int gg = e / a.nblk, jj = e % a.nblk;
+    int64_t lo, hi;
+    slice_of(a, jj, blockIdx.x * NG + gg, nvw, lo, hi);
+    gslice[gg][jj] = make_int2((int)lo, (int)hi);
+  }
+  __syncthreads();
+  const int2* gsl = gslice[g];
   Cursor cu;
-  bool have = cursor_first(a, 0, vid, nvw, cu);
+  bool have = cursor_first(a, 0, gsl, cu);
   if (have) stage_tile<H>(a, load_tile_ids(a, cu.pos, tile_rows(cu), gt & 127), gt, sA[0], L.dpad, cid, ccat);
   __syncthreads();
   if (have && gw == 0) tile_runs(ccat, tile_rows(cu), runs[0], &nruns[0]);
@@ -342,7 +354,7 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
       }
       pre_issued = false;
       Cursor nx;
-      const bool have_nx = cursor_next(a, cu, vid, nvw, nx);
+      const bool have_nx = cursor_next(a, cu, gsl, nx);
       TileIds tn{-1, 0};
       if (have_nx) tn = load_tile_ids(a, nx.pos, tile_rows(nx), gt & 127);
       if (!tc::mbar_wait(mbar, phase, kMaxPolls)) atomicExch(a.err, 2);
@@ -466,8 +478,7 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
       if (v != 0.f) atomicAdd(&Oout[o_at], (double)v);
     }
     // carry the state forward (O_in - old(this block) - old(next block)), spread over the CTAs
-    const size_t lds = (size_t)B * K;  // the batch rows (the column-sum row is not kept)
-    for (size_t e = lds * blockIdx.x / gridDim.x + tid; e < lds * (blockIdx.x + 1) / gridDim.x; e += NT) {
+    for (int e = carry0 + tid; e < carry1; e += NT) {
       double v = Oin[e];
       if (Omc) v -= Omc[e];
       if (Omn) v -= Omn[e];

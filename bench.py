@@ -51,6 +51,8 @@ def parse():
                          "iterations, then exit")
     ap.add_argument("--profile-cells", type=int, default=500_000,
                     help="cells of the --profile-case run")
+    ap.add_argument("--profile-inner", type=int, default=2,
+                    help="k-means iterations of the --profile-case run")
     return ap.parse_args()
 
 
@@ -64,7 +66,8 @@ def run_profile_case(args):
     X = torch.as_tensor(cfg["Z"], device="cuda")
     prob = HarmonyProblem(X, cfg["cats"], cfg["n_batches"], torch.as_tensor(cfg["Y0"], device="cuda"),
                           np.full(cfg["n_batches"], 2.0), precision=args.precision,
-                          n_clusters=cfg["n_clusters"], max_iter_harmony=1, max_iter_clustering=2,
+                          n_clusters=cfg["n_clusters"], max_iter_harmony=1,
+                          max_iter_clustering=args.profile_inner,
                           tol_harmony=-np.inf, tol_clustering=-np.inf)
     _, info = prob.run(profile=True)
     torch.cuda.synchronize()

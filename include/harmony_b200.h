@@ -73,7 +73,10 @@ typedef struct hb_params {
   int32_t prune;                /* batch_prune_threshold is not None */
   int32_t stabilized_penalty;   /* harmony2 penalty */
   int32_t dynamic_lambda;       /* harmony2 lambda = alpha * E */
-  int32_t reserved;
+  int32_t max_sweep_ctas;       /* 0: the persistent sweep may use every SM; otherwise at most this
+                                   many CTAs (SMs).  Problems that run at the same time on one GPU
+                                   must together stay within the SM count, or their grid barriers
+                                   can wait on each other */
   uint64_t random_state;
 } hb_params;
 

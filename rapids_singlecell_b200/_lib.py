@@ -53,7 +53,7 @@ class HbParams(ctypes.Structure):
         ("prune", ctypes.c_int32),
         ("stabilized_penalty", ctypes.c_int32),
         ("dynamic_lambda", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("max_sweep_ctas", ctypes.c_int32),
         ("random_state", ctypes.c_uint64),
     ]
 

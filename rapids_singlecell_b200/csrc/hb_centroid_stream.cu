@@ -80,6 +80,7 @@ __global__ void __launch_bounds__(256, 1) k_tc_centroid_stream(CenStreamArgs a, 
   uint64_t* mma_done = full + 4;                // MMAs of a tile completed (one phase per tile)
   uint64_t* oh_ready = full + 5;                // one-hot of the next tile written (one phase per tile)
   uint64_t* empty = full + 6;                   // [S] MMAs of the stage's last tile completed
+  uint64_t* acc_bar = full + 10;                // all MMAs of the CTA completed (one phase)
   uint32_t* tmem_slot = (uint32_t*)(sm + L.offBar + 128);
   const uint32_t sm32 = tc::smem_u32(sm);
   const int t0 = (int)((int64_t)a.ntiles * blockIdx.x / gridDim.x);
@@ -96,6 +97,7 @@ __global__ void __launch_bounds__(256, 1) k_tc_centroid_stream(CenStreamArgs a, 
     tc::mbar_init(mma_done, 1);
     tc::mbar_init(oh_ready, 4);
     for (int s = 0; s < S; ++s) tc::mbar_init(empty + s, 1);
+    tc::mbar_init(acc_bar, 1);
     tc::fence_mbar_init();
   }
   for (uint32_t e = tid * 16u; e < (uint32_t)L.nbK * 16384u; e += 256u * 16u)
@@ -144,6 +146,7 @@ __global__ void __launch_bounds__(256, 1) k_tc_centroid_stream(CenStreamArgs a, 
       tc::mma_commit(empty + s);
       tc::mma_commit(mma_done);
     }
+    if (nt > 0) tc::mma_commit(acc_bar);
   } else if (tid == 32) {
     for (int j = S; j < nt; ++j) {  // tile j reuses the stage of tile j - S
       const int sj = j % S;
@@ -184,7 +187,9 @@ __global__ void __launch_bounds__(256, 1) k_tc_centroid_stream(CenStreamArgs a, 
       if (lane == 0) mbar_arrive_cta(oh_ready);
     }
   }
-  if (nt > 0 && !tc::mbar_wait(mma_done, (uint32_t)((nt - 1) & 1), kMaxPolls)) atomicExch(a.err, 4);
+  // the warps without a role in the loop never tracked mma_done's phases: wait on the
+  // single-phase acc_bar instead
+  if (nt > 0 && !tc::mbar_wait(acc_bar, 0, kMaxPolls)) atomicExch(a.err, 4);
   tc::fence_after_sync();
   // ---- epilogue: D1 -> P[cta][cluster][pc], D2 -> Opart[cta][key][cluster] -------------
   {
@@ -277,7 +282,7 @@ int launch_tc_centroid_stream(const CenStreamArgs& a, const void* Zn, int ldz, c
   const void* fn = (const void*)k_tc_centroid_stream<H>;
   // one CTA per SM: the request is padded so that a second CTA never fits (TMEM)
   const size_t smem = std::max<size_t>(L.bytes, 116u * 1024u);
-  HB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  HB_TRY(allow_max_dyn_smem(fn));
   k_tc_centroid_stream<H><<<grid, 256, smem, st>>>(a, L, tmZ, tmR);
   HB_LAUNCH_CHECK();
   const int64_t ne = (int64_t)a.nkeys * a.K;

@@ -372,7 +372,7 @@ int launch_tc_centroid(const CenArgs& a, int grid, cudaStream_t st) {
   const void* fn = (const void*)k_tc_centroid<H>;
   // one CTA per SM: the request is padded so that a second CTA never fits (TMEM)
   const size_t smem = std::max<size_t>(L.bytes, 116u * 1024u);
-  HB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  HB_TRY(allow_max_dyn_smem(fn));
   k_tc_centroid<H><<<grid, 256, smem, st>>>(a, L);
   HB_LAUNCH_CHECK();
   return HB_OK;

@@ -144,5 +144,10 @@ extern thread_local int64_t g_launches;  // kernels launched by this thread (pro
   } while (0)
 
 int num_sms();
+// Raises fn's dynamic shared-memory limit to the largest the device allows, once per
+// (function, device).  The limit is one per-function setting shared by every thread of the
+// process: plans of different shapes running at the same time must never lower it under
+// each other's launches, so it is only ever set to this one value.
+int allow_max_dyn_smem(const void* fn);
 
 }  // namespace hb

@@ -184,7 +184,7 @@ int launch_tc_moments(const H* R, int ldr, const float* X, int ldx, const int32_
   }
   const MomLayout L = mom_layout(K, d);
   const void* fn = (const void*)k_tc_moments<H>;
-  HB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.bytes));
+  HB_TRY(allow_max_dyn_smem(fn));
   k_tc_moments<H><<<n_chunks, 256, L.bytes, st>>>(R, ldr, X, ldx, cell_index, chunks, K, d, Mpart, L, err);
   HB_LAUNCH_CHECK();
   return HB_OK;
@@ -403,7 +403,7 @@ int launch_tc_apply(const float* X, int ldx, const H* R, int ldr, const float* W
   }
   const ApLayout L = ap_layout(K, d);
   const void* fn = (const void*)k_tc_apply<H>;
-  HB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.bytes));
+  HB_TRY(allow_max_dyn_smem(fn));
   // CTAs per SM by shared memory (the occupancy query counts one per SM for a TMEM-allocating
   // kernel); at most 512 / tcols so that the TMEM allocations always fit
   const int per_sm = std::max(1, std::min<int>(512 / L.tcols, (int)(233472u / (L.bytes + 2048u))));

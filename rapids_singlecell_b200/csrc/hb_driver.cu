@@ -7,6 +7,8 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
+#include <set>
 #include <vector>
 #include <cudaTypedefs.h>
 #include "hb_internal.h"
@@ -50,6 +52,22 @@ int make_row_gather_map(CUtensorMap* tm, const void* base, int64_t rows, int ld,
     set_error("cuTensorMapEncodeTiled failed (%d) for rows=%lld ld=%d", (int)r, (long long)rows, ld);
     return HB_ERR_CUDA;
   }
+  return HB_OK;
+}
+
+int allow_max_dyn_smem(const void* fn) {
+  static std::mutex mu;
+  static std::set<std::pair<const void*, int>> done;
+  int dev = 0;
+  HB_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.count({fn, dev})) return HB_OK;
+  cudaFuncAttributes fa;
+  HB_CUDA(cudaFuncGetAttributes(&fa, fn));
+  int optin = 0;
+  HB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  HB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes));
+  done.insert({fn, dev});
   return HB_OK;
 }
 
@@ -215,7 +233,11 @@ int hb_plan_create(const hb_params* params, hb_plan** plan) {
   P->cen_tiles = div_up(p.n_clusters, 128) * div_up(p.n_pcs, 64);
   const int64_t target = std::max(1, 2 * sms / P->cen_tiles);
   P->cen_chunks = (int)std::max<int64_t>(1, std::min<int64_t>(target, (p.n_cells + 255) / 256));
-  if (P->ssz == 2) P->cen_chunks = tc_centroid_grid(p.n_clusters);  // one partial per resident CTA
+  // 16-bit path: one partial per CTA, at most one CTA per SM and per 128-cell tile (four
+  // tiles per CTA at least, so that small problems leave SMs to concurrent ones)
+  if (P->ssz == 2)
+    P->cen_chunks = (int)std::max<int64_t>(1, std::min<int64_t>(tc_centroid_grid(p.n_clusters),
+                                                                (p.n_cells + 511) / 512));
   P->m_chunk_len = std::max<int64_t>(256, (p.n_cells + target - 1) / target);
   P->max_m_chunks = (int)((p.n_cells + P->m_chunk_len - 1) / P->m_chunk_len) + p.n_batches;
   P->max_apply_tiles = (int)((p.n_cells + 31) / 32) + p.n_batches;
@@ -388,7 +410,8 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
       sa.Obuf[0] = w.O[0]; sa.Obuf[1] = w.O[1]; sa.Obuf[2] = w.O[2]; sa.b0 = ring.cur;
       sa.Omin = Omin; sa.Pr = w.Pr; sa.theta = w.theta; sa.obj_acc = w.obj_acc; sa.obj_out = obj_dst;
       sa.sigma = p.sigma; sa.d = d; sa.K = K; sa.B = B; sa.stabilized = p.stabilized_penalty;
-      sa.init_mode = init; sa.batch_sorted = P->ml.nsub > 1 || B <= 1; sa.barrier = w.barrier; sa.err = w.err;
+      sa.init_mode = init; sa.batch_sorted = P->ml.nsub > 1 || B <= 1;
+      sa.max_ctas = p.max_sweep_ctas; sa.barrier = w.barrier; sa.err = w.err;
       HB_CUDA(cudaMemsetAsync(w.barrier, 0, sizeof(unsigned), st));
       HB_TRY(launch_tc_sweep<S>(sa, st));
       ring.cur = (ring.cur + nb) % 3;

@@ -271,7 +271,7 @@ static int prepare(const void* fn, const TcLayout& L, int* occ_out) {
     set_error("tensor-core block update: shared-memory tables too large");
     return HB_ERR_UNSUPPORTED;
   }
-  HB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.bytes));
+  HB_TRY(allow_max_dyn_smem(fn));
   int occ = 1;
   HB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 256, L.bytes));
   // at most 512 TMEM columns per SM are shared by the resident CTAs
@@ -293,8 +293,7 @@ int launch_tc_block_update(const BlockArgs& a, const double* O_in, double* O_out
   const size_t per_sm = 228u * 1024u;
   if (per_sm / (smem + 1024) > (size_t)occ) smem = std::min<size_t>(227u * 1024u, per_sm / occ - 2048);
   if (smem != L.bytes)
-    HB_CUDA(cudaFuncSetAttribute((const void*)k_tc_block_update<H>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem));
+    HB_TRY(allow_max_dyn_smem((const void*)k_tc_block_update<H>));
   k_tc_block_update<H><<<grid, 256, smem, st>>>(TcArgs{a, O_in, O_out, O_zero, err}, L);
   HB_LAUNCH_CHECK();
   return HB_OK;
@@ -316,8 +315,7 @@ int launch_tc_similarity(const H* Zn, int ldz, const H* Yn, int ldy, const int32
   const size_t per_sm = 228u * 1024u;
   if (per_sm / (smem + 1024) > (size_t)occ) smem = std::min<size_t>(227u * 1024u, per_sm / occ - 2048);
   if (smem != L.bytes)
-    HB_CUDA(cudaFuncSetAttribute((const void*)k_tc_similarity<H>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem));
+    HB_TRY(allow_max_dyn_smem((const void*)k_tc_similarity<H>));
   k_tc_similarity<H><<<grid, 256, smem, st>>>(Zn, ldz, Yn, ldy, idx, cats, n, K, S, L, err);
   HB_LAUNCH_CHECK();
   return HB_OK;

@@ -143,6 +143,7 @@ struct SweepArgs {
   int stabilized;
   int init_mode;
   int batch_sorted;        // the list is ordered by batch within each block
+  int max_ctas;            // 0: one CTA per SM; otherwise at most this many CTAs
   unsigned* barrier;       // zero on entry
   int* err;
 };

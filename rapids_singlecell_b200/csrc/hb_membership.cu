@@ -392,14 +392,13 @@ int membership_build_dev(const MembershipLayout& L, const MembershipBufs& B, con
   HB_LAUNCH_CHECK();
   const size_t smem = sizeof(uint32_t) * (size_t)L.cap;
   if (smem > 48 * 1024)
-    HB_CUDA(cudaFuncSetAttribute(k_select_splitters, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    HB_TRY(allow_max_dyn_smem((const void*)k_select_splitters));
   k_select_splitters<<<dim3(L.max_slots, n_iters), 512, smem, st>>>(
       nb, L.cap, B.nslots, B.cand_cnt, B.cand, B.bnd_slot, B.bnd_q, B.split, L.max_slots, L.cap);
   HB_LAUNCH_CHECK();
   }
   if (sizeof(uint32_t) * nbk > 48 * 1024)
-    HB_CUDA(cudaFuncSetAttribute(k_part_count, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(sizeof(uint32_t) * nbk)));
+    HB_TRY(allow_max_dyn_smem((const void*)k_part_count));
   k_part_count<<<dim3(L.ntiles, n_iters), 256, sizeof(uint32_t) * nbk, st>>>(
       L.n, L.nblk, nsub, cats, seeds, seed0, B.split, B.counts, L.ntiles);
   HB_LAUNCH_CHECK();
@@ -407,7 +406,7 @@ int membership_build_dev(const MembershipLayout& L, const MembershipBufs& B, con
   HB_LAUNCH_CHECK();
   const size_t ssm = sizeof(uint32_t) * 9 * (size_t)nbk;
   if (ssm > 48 * 1024)
-    HB_CUDA(cudaFuncSetAttribute(k_part_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm));
+    HB_TRY(allow_max_dyn_smem((const void*)k_part_scatter));
   k_part_scatter<<<dim3(L.ntiles, n_iters), 256, ssm, st>>>(L.n, L.bs, L.nblk, nsub, cats, seeds, seed0,
                                                            B.split, B.offsets, B.totals, L.ntiles, idx, lcat, ckey,
                                                            n_batches);

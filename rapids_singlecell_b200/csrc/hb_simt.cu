@@ -489,8 +489,7 @@ static int launch_block_kpt(const BlockArgsDev& p, cudaStream_t st) {
     set_error("block update: B*K too large for shared memory (B=%d K=%d)", a.B, a.K);
     return HB_ERR_UNSUPPORTED;
   }
-  HB_CUDA(cudaFuncSetAttribute(k_block_update<T, KPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem));
+  HB_TRY(allow_max_dyn_smem((const void*)k_block_update<T, KPT>));
   int occ = 1;
   HB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_block_update<T, KPT>, BU_THREADS, smem));
   if (occ < 1) occ = 1;

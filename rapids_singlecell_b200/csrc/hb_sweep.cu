@@ -36,8 +36,8 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
 // Grid-wide barrier of a cooperative launch, split in two: arrive once this
 // CTA's writes of the block are issued, wait before the next block's counts are
 // read; work that does not depend on the other CTAs goes in between.  The wait
-// is bounded: after ~2^26 polls the CTA records error 3 and proceeds (the host
-// reports a timeout).
+// is bounded: after 2 s (or once any CTA has given up) the CTA records error 3
+// and proceeds (the host reports a timeout).
 __device__ __forceinline__ void grid_arrive(unsigned* ctr) {
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -45,11 +45,19 @@ __device__ __forceinline__ void grid_arrive(unsigned* ctr) {
     atomicAdd(ctr, 1u);
   }
 }
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 __device__ __forceinline__ void grid_wait(unsigned* ctr, unsigned target, int* err) {
   if (threadIdx.x == 0) {
+    const uint64_t t0 = globaltimer_ns();
     unsigned spins = 0;
     while (ld_acquire_u32(ctr) < target) {
-      if (++spins > (1u << 26)) {
+      // give up after 2 s, or at once when another CTA has already given up
+      if ((++spins & 255u) == 0 &&
+          (globaltimer_ns() - t0 > 2000000000ull || *(volatile int*)err != 0)) {
         atomicExch(err, 3);
         break;
       }
@@ -545,7 +553,7 @@ template <typename H, int NG>
 static int launch_sweep_ng(const SweepArgs& a, const SweepLayout& SL, cudaStream_t st) {
   const void* fn = (const void*)k_tc_sweep<H, NG>;
   const size_t smem = SL.bytes;
-  HB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  HB_TRY(allow_max_dyn_smem(fn));
   int occ = 0;
   HB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 256 * NG, smem));
   if (occ < 1) {
@@ -554,7 +562,9 @@ static int launch_sweep_ng(const SweepArgs& a, const SweepLayout& SL, cudaStream
   }
   // one CTA per SM: the TMEM of an SM is shared out between the CTA's groups
   const int64_t tiles = std::max<int64_t>(1, (std::min<int64_t>(a.bs, a.n) + 127) / 128);
-  const int grid = (int)std::min<int64_t>((int64_t)num_sms(), tiles);
+  int64_t cap = num_sms();
+  if (a.max_ctas > 0) cap = std::min<int64_t>(cap, a.max_ctas);
+  const int grid = (int)std::min<int64_t>(cap, tiles);
   SweepArgs args = a;
   SweepLayout lay = SL;
   void* kargs[] = {(void*)&args, (void*)&lay};

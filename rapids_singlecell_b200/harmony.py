@@ -33,6 +33,34 @@ class HarmonyInfo:
     profile: dict | None = None
 
 
+def make_params(n_cells, n_pcs, n_clusters, n_batches, *, precision="fp32", max_iter_harmony=10,
+                max_iter_clustering=200, tol_harmony=1e-4, tol_clustering=1e-5, ridge_lambda=1.0,
+                sigma=0.1, block_proportion=0.05, random_state=0, stabilized_penalty=True,
+                dynamic_lambda=True, alpha=0.2, batch_prune_threshold=1e-5, max_sweep_ctas=0) -> HbParams:
+    """The engine's plan parameters (``hb_params``) for one problem."""
+    p = HbParams()
+    p.n_cells = int(n_cells)
+    p.n_pcs = int(n_pcs)
+    p.n_clusters = int(n_clusters)
+    p.n_batches = int(n_batches)
+    p.precision = PRECISIONS[precision]
+    p.block_size = int(n_cells * block_proportion)
+    p.max_iter_harmony = int(max_iter_harmony)
+    p.max_iter_clustering = int(max_iter_clustering)
+    p.tol_harmony = tol_harmony
+    p.tol_clustering = tol_clustering
+    p.sigma = sigma
+    p.ridge_lambda = ridge_lambda
+    p.alpha = alpha
+    p.batch_prune_threshold = 0.0 if batch_prune_threshold is None else batch_prune_threshold
+    p.prune = 0 if batch_prune_threshold is None else 1
+    p.stabilized_penalty = int(bool(stabilized_penalty))
+    p.dynamic_lambda = int(bool(dynamic_lambda))
+    p.random_state = int(random_state) & 0xFFFFFFFFFFFFFFFF
+    p.max_sweep_ctas = int(max_sweep_ctas)
+    return p
+
+
 class HarmonyProblem:
     """One Harmony problem resident on the GPU: the engine plan, its workspace and
     the device inputs.  ``run()`` integrates it (and can be called again, e.g. to
@@ -48,7 +76,7 @@ class HarmonyProblem:
                  max_iter_harmony=10, max_iter_clustering=200, tol_harmony=1e-4,
                  tol_clustering=1e-5, ridge_lambda=1.0, sigma=0.1, block_proportion=0.05,
                  random_state=0, stabilized_penalty=True, dynamic_lambda=True, alpha=0.2,
-                 batch_prune_threshold=1e-5, stream=None):
+                 batch_prune_threshold=1e-5, stream=None, max_sweep_ctas=0):
         self.lib = _lib.load()
         self.device = X.device
         self.X = X.contiguous()
@@ -70,25 +98,12 @@ class HarmonyProblem:
         self.max_iter_clustering = max_iter_clustering
         self.n_clusters = n_clusters
         self.precision = precision
-        p = HbParams()
-        p.n_cells = n_cells
-        p.n_pcs = n_pcs
-        p.n_clusters = n_clusters
-        p.n_batches = self.n_batches
-        p.precision = PRECISIONS[precision]
-        p.block_size = int(n_cells * block_proportion)
-        p.max_iter_harmony = max_iter_harmony
-        p.max_iter_clustering = max_iter_clustering
-        p.tol_harmony = tol_harmony
-        p.tol_clustering = tol_clustering
-        p.sigma = sigma
-        p.ridge_lambda = ridge_lambda
-        p.alpha = alpha
-        p.batch_prune_threshold = 0.0 if batch_prune_threshold is None else batch_prune_threshold
-        p.prune = 0 if batch_prune_threshold is None else 1
-        p.stabilized_penalty = int(bool(stabilized_penalty))
-        p.dynamic_lambda = int(bool(dynamic_lambda))
-        p.random_state = int(random_state) & 0xFFFFFFFFFFFFFFFF
+        p = make_params(n_cells, n_pcs, n_clusters, self.n_batches, precision=precision,
+                        max_iter_harmony=max_iter_harmony, max_iter_clustering=max_iter_clustering,
+                        tol_harmony=tol_harmony, tol_clustering=tol_clustering, ridge_lambda=ridge_lambda,
+                        sigma=sigma, block_proportion=block_proportion, random_state=random_state,
+                        stabilized_penalty=stabilized_penalty, dynamic_lambda=dynamic_lambda, alpha=alpha,
+                        batch_prune_threshold=batch_prune_threshold, max_sweep_ctas=max_sweep_ctas)
         self.params = p
         self.plan = ctypes.c_void_p()
         _lib.check(self.lib.hb_plan_create(ctypes.byref(p), ctypes.byref(self.plan)))

@@ -89,3 +89,21 @@ def test_many_blocks_times_batches(prec):
                     precision=prec, **kw)
     ref = ho.harmonize(Z, cats, B, Y0, dtype=np.float64, **kw)
     assert rel_maxabs(out.cpu().numpy(), ref.Z_hat) < (1e-4 if prec == "fp32" else 2e-3)
+
+
+@pytest.mark.parametrize("prec", ["bf16", "fp16"])
+def test_16bit_many_tiles_per_cta_vs_plain_fp32(prec):
+    """150,000 cells: every CTA of the centroid pass and every thread group of the
+    sweep handles several 128-cell tiles; checked against the plain fp32 path."""
+    cfg = make_config("C2", seed=3, n_cells=150_000)
+    kw = dict(n_clusters=100, max_iter_harmony=2, max_iter_clustering=4, tol_harmony=-np.inf,
+              tol_clustering=-np.inf)
+    labels = pd.Categorical.from_codes(cfg["cats"], categories=[f"b{i}" for i in range(cfg["n_batches"])])
+    Z = torch.as_tensor(cfg["Z"], device="cuda")
+    ref, ref_info = harmonize(Z, labels, None, init_centroids=cfg["Y0"], precision="fp32", return_info=True, **kw)
+    out, info = harmonize(Z, labels, None, init_centroids=cfg["Y0"], precision=prec, return_info=True, **kw)
+    err = rel_maxabs(out.cpu().numpy(), ref.cpu().numpy())
+    print(f"{prec} vs plain fp32: rel max-abs {err:.3e}; objectives {info.objectives_harmony} vs "
+          f"{ref_info.objectives_harmony}")
+    np.testing.assert_allclose(info.objectives_harmony, ref_info.objectives_harmony, rtol=5e-3)
+    assert err < 5e-3

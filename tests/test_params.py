@@ -82,3 +82,15 @@ def test_integer_codes_declines(labels):
     from rapids_singlecell_b200.harmony import _integer_codes
 
     assert _integer_codes(labels) == (None, 0)
+
+
+def test_request_bytes_counts_workspace_and_tensors():
+    from rapids_singlecell_b200.batched import HarmonyRequest, request_bytes
+    from rapids_singlecell_b200.harmony import HarmonyProblem, make_params
+
+    params = dict(n_clusters=30, max_iter_harmony=2, max_iter_clustering=5)
+    r = HarmonyRequest(np.zeros((1000, 50), np.float32), np.zeros(1000, np.int32), 3,
+                       np.zeros((30, 50), np.float32), np.ones(3), params)
+    ws = HarmonyProblem.workspace_bytes(make_params(1000, 50, 30, 3, precision="bf16",
+                                                    max_iter_harmony=2, max_iter_clustering=5))
+    assert request_bytes(r) == ws + 2 * 1000 * 50 * 4 + 30 * 50 * 4 + 1000 * 4

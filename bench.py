@@ -294,8 +294,15 @@ def run_ours(args):
         prob32 = HarmonyProblem(X, cats, B, torch.as_tensor(cfg["Y0"], device=dev), theta,
                                 precision="fp32", **common)
         ms32, per32 = timed(lambda: prob32.run(), max(1, min(args.steps, 3)), 1)
+        # error of the 16-bit result against the plain fp32 result of the same inputs (the
+        # float64 oracle is too slow for this size on the host)
+        z32 = prob32.Z_hat.double()
+        z16 = last["e2e"].to(dev).double()
+        diff = (z16 - z32).abs().max().item()
         plain = {"value": cell_iters * world / (ms32 / 1e3), "ms_per_step": ms32,
-                 "p50_ms": float(np.percentile(per32, 50)), "p99_ms": float(np.percentile(per32, 99))}
+                 "p50_ms": float(np.percentile(per32, 50)), "p99_ms": float(np.percentile(per32, 99)),
+                 "max_abs_diff_16bit_vs_fp32": diff,
+                 "rel_max_abs_diff_16bit_vs_fp32": diff / max(z32.abs().max().item(), 1e-300)}
         prob32.close()
 
     if rank != 0:

@@ -187,8 +187,10 @@ __global__ void __launch_bounds__(256, 1) k_tc_centroid_stream(CenStreamArgs a, 
       if (lane == 0) mbar_arrive_cta(oh_ready);
     }
   }
-  // the warps without a role in the loop never tracked mma_done's phases: wait on the
-  // single-phase acc_bar instead
+  // Threads without a role wait here in the hardware barrier: spinning on an mbarrier in the
+  // warps of the issuer and the producer would take their issue slots for the whole loop.
+  // Then the single-phase acc_bar (the warps without a role never tracked mma_done's phases).
+  __syncthreads();
   if (nt > 0 && !tc::mbar_wait(acc_bar, 0, kMaxPolls)) atomicExch(a.err, 4);
   tc::fence_after_sync();
   // ---- epilogue: D1 -> P[cta][cluster][pc], D2 -> Opart[cta][key][cluster] -------------

@@ -46,6 +46,10 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="bf16", choices=["bf16", "fp16", "fp32"])
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--sections", default="wide,batched,serving",
+                    help="extra measurements on rank 0 beside the headline line: wide (the "
+                         "2M-cell x 100-PC workload), batched (256 independent problems), "
+                         "serving (Poisson request stream); empty for none")
     ap.add_argument("--profile-case", action="store_true",
                     help="one short run for ncu: the same workload for 1 outer x 2 k-means "
                          "iterations, then exit")
@@ -196,6 +200,193 @@ def profiled_traffic(name):
             except ValueError:
                 return None
     return None
+
+
+# ---------------------------------------------------------------------------
+# Extra measurements beside the headline line (rank 0, one GPU each).
+
+def _rel(a, b):
+    return float((a.double() - b.double()).abs().max().item() / max(b.double().abs().max().item(), 1e-300))
+
+
+def _gpu_time(fn, reps):
+    """Device time of fn() per call (CUDA events on the current stream), after one warm-up call."""
+    import torch
+
+    fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def wide_section(dev):
+    """The 2,000,000-cell x 100-PC workload (50 types, 32 Zipf(1.2)-sized batches,
+    shift N(0, 0.7^2), K = 200, 10 outer x 20 k-means iterations fixed), device
+    resident: the bf16 path against the plain fp32 path, and the error of both
+    against the engine's float64 path on the same inputs."""
+    import torch
+
+    from rapids_singlecell_b200.harmony import HarmonyProblem
+    from rapids_singlecell_b200.synthetic import make_config
+
+    cfg = make_config("C3", seed=0)
+    n, d = cfg["Z"].shape
+    B, K = cfg["n_batches"], cfg["n_clusters"]
+    kw = dict(n_clusters=K, max_iter_harmony=OUTER, max_iter_clustering=INNER, tol_harmony=-np.inf,
+              tol_clustering=-np.inf)
+    theta = np.full(B, 2.0)
+    X = torch.as_tensor(cfg["Z"], device=dev)
+    Y0 = torch.as_tensor(cfg["Y0"], device=dev)
+    out = {"workload": f"C3: {n} cells x {d} PCs, {B} batches, K={K}, {OUTER} outer x {INNER} "
+                       "k-means iterations fixed, device resident"}
+    res = {}
+    for prec, reps in (("bf16", 2), ("fp32", 1)):
+        prob = HarmonyProblem(X, cfg["cats"], B, Y0, theta, precision=prec, **kw)
+        ms = _gpu_time(prob.run, reps)
+        res[prec] = prob.Z_hat.clone()
+        out[prec] = {"value": n * OUTER * INNER / (ms / 1e3), "unit": "cell-iters/s", "ms_per_run": ms}
+        prob.close()
+    out["speedup_bf16_vs_fp32"] = out["bf16"]["value"] / out["fp32"]["value"]
+    prob = HarmonyProblem(X.double(), cfg["cats"], B, Y0.double(), theta, precision="fp64", **kw)
+    prob.run()
+    z64 = prob.Z_hat.clone()
+    prob.close()
+    out["rel_max_abs_err_vs_fp64"] = {p: _rel(res[p], z64) for p in res}
+    out["max_abs_err_vs_fp64"] = {p: float((res[p].double() - z64).abs().max().item()) for p in res}
+    return out
+
+
+def batched_section(dev, n_problems=256, streams=8):
+    """Independent problems of uneven sizes on one GPU: cells log-uniform in
+    [2k, 200k], d in {30, 50}, B uniform in [2, 12], K = min(100, n / 30), each
+    from the mixture generator with its own seed (10 types, Dirichlet(1)
+    batches); 10 outer x 20 k-means iterations fixed; inputs resident on the
+    device.  All problems go through one HarmonyServer (8 streams); bf16 and
+    plain fp32 runs of the same set, and the per-problem bf16 vs fp32 error."""
+    import torch
+
+    from rapids_singlecell_b200.batched import HarmonyRequest, latency_summary, run_batched
+    from rapids_singlecell_b200.synthetic import MixtureSpec, initial_centroids, make_mixture
+
+    rng = np.random.default_rng(7)
+    specs = []
+    for i in range(n_problems):
+        n = int(np.exp(rng.uniform(np.log(2_000), np.log(200_000))))
+        specs.append((n, int(rng.choice([30, 50])), int(rng.integers(2, 13))))
+    data = []
+    for i, (n, d, B) in enumerate(specs):
+        Z, cats, _ = make_mixture(MixtureSpec(n, d, 10, B, "dirichlet", (), 0.5, (0.8, 1.2)), 1000 + i)
+        K = min(100, n // 30)
+        data.append((torch.as_tensor(Z, device=dev), cats, B, initial_centroids(Z, K, 5000 + i), K))
+    cell_iters = sum(s[0] for s in specs) * OUTER * INNER
+
+    def reqs(prec, sub=None):
+        sel = data if sub is None else data[:sub]
+        return [HarmonyRequest(Z, cats, B, Y0, np.full(B, 2.0),
+                               dict(n_clusters=K, max_iter_harmony=OUTER, max_iter_clustering=INNER,
+                                    tol_harmony=-np.inf, tol_clustering=-np.inf), precision=prec)
+                for Z, cats, B, Y0, K in sel]
+
+    out = {"workload": f"{n_problems} problems, cells log-uniform in [2k, 200k] (total "
+                       f"{sum(s[0] for s in specs)}), d in {{30, 50}}, B in [2, 12], K = min(100, n/30), "
+                       f"{OUTER} outer x {INNER} k-means iterations fixed, {streams} streams"}
+    results = {}
+    for prec in ("bf16", "fp32"):
+        run_batched(reqs(prec, 8), streams=streams, device=dev)  # warm-up: library, plans, threads
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = run_batched(reqs(prec), streams=streams, device=dev)
+        torch.cuda.synchronize()
+        t = time.perf_counter() - t0
+        results[prec] = r
+        out[prec] = {"value": cell_iters / t, "unit": "cell-iters/s", "wall_s": t,
+                     **{k: v for k, v in latency_summary(r).items()}}
+    out["speedup_bf16_vs_fp32"] = out["bf16"]["value"] / out["fp32"]["value"]
+    errs = [_rel(a.Z_hat, b.Z_hat) for a, b in zip(results["bf16"], results["fp32"])]
+    out["rel_max_abs_diff_bf16_vs_fp32"] = {"max": float(np.max(errs)), "median": float(np.median(errs))}
+    return out
+
+
+def serving_section(dev, n_requests=64, rates=(10.0, 100.0), fp32_rate=10.0, streams=8):
+    """A Poisson stream of integration requests through HarmonyServer (HBM budget
+    160 GB, 8 streams): cells log-uniform in [5k, 1M], d in {30, 50, 100}, B in
+    [2, 32], K = min(200, n / 30), 10 outer x 20 k-means iterations fixed.  Each
+    request is the first n cells of a seeded 1M-cell mixture of its d (50 types,
+    32 Zipf(1.2)-sized batches, shift N(0, 0.7^2)), its batches folded to B
+    (code mod B, renumbered); host input, host result (both copies inside the
+    latency).  Latency is from arrival to result."""
+    import torch
+
+    from rapids_singlecell_b200.batched import HarmonyRequest, HarmonyServer, latency_summary
+    from rapids_singlecell_b200.synthetic import MixtureSpec, initial_centroids, make_mixture
+
+    base = {d: make_mixture(MixtureSpec(1_000_000, d, 50, 32, "zipf", (), 0.7, None, zipf_s=1.2,
+                                        min_batch=500), 3000 + d)[:2] for d in (30, 50, 100)}
+    rng = np.random.default_rng(11)
+    reqs = []
+    for i in range(n_requests):
+        n = int(np.exp(rng.uniform(np.log(5_000), np.log(1_000_000))))
+        d = int(rng.choice([30, 50, 100]))
+        B = int(rng.integers(2, 33))
+        Z = base[d][0][:n]
+        _, cats = np.unique(base[d][1][:n] % B, return_inverse=True)
+        B = int(cats.max()) + 1
+        K = min(200, n // 30)
+        reqs.append((Z, cats.astype(np.int32), B, initial_centroids(Z, K, 7000 + i), K))
+    total_cells = sum(r[0].shape[0] for r in reqs)
+
+    def stream_run(prec, rate):
+        gaps = rng.exponential(1.0 / rate, len(reqs))
+        with HarmonyServer(streams=streams, hbm_budget_bytes=160 << 30, device=dev) as srv:
+            for Z, cats, B, Y0, K in reqs[:4]:  # warm-up
+                srv.submit(HarmonyRequest(Z, cats, B, Y0, np.full(B, 2.0),
+                                          dict(n_clusters=K, max_iter_harmony=1, max_iter_clustering=2),
+                                          precision=prec, to_host=True)).result()
+            t0 = time.perf_counter()
+            futs = []
+            for gap, (Z, cats, B, Y0, K) in zip(gaps, reqs):
+                time.sleep(gap)
+                futs.append(srv.submit(HarmonyRequest(
+                    Z, cats, B, Y0, np.full(B, 2.0),
+                    dict(n_clusters=K, max_iter_harmony=OUTER, max_iter_clustering=INNER,
+                         tol_harmony=-np.inf, tol_clustering=-np.inf), precision=prec, to_host=True)))
+            res, errors = [], 0
+            for f in futs:
+                try:
+                    res.append(f.result())
+                except Exception:  # noqa: BLE001 - counted and reported
+                    errors += 1
+            t = time.perf_counter() - t0
+        done = sum(r.Z_hat.shape[0] for r in res)
+        return {"rate_req_s": rate, "requests": len(reqs), "errors": errors, "makespan_s": t,
+                "cells_per_s": done / t, "cell_iters_per_s": done * OUTER * INNER / t,
+                **latency_summary(res)}
+
+    out = {"workload": f"{n_requests} Poisson arrivals, cells log-uniform in [5k, 1M] (total {total_cells}), "
+                       "d in {30, 50, 100}, B in [2, 32], K = min(200, n/30), "
+                       f"{OUTER} outer x {INNER} k-means iterations fixed, HBM budget 160 GB, {streams} streams",
+           "bf16": [stream_run("bf16", r) for r in rates],
+           "fp32": [stream_run("fp32", fp32_rate)]}
+    torch.cuda.synchronize()
+    return out
+
+
+def run_sections(args, dev):
+    out = {}
+    for name in [s for s in args.sections.split(",") if s]:
+        fn = {"wide": wide_section, "batched": batched_section, "serving": serving_section}[name]
+        t0 = time.perf_counter()
+        try:
+            out[name] = fn(dev)
+        except Exception as e:  # noqa: BLE001 - reported in the line; the headline stands
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+        out[name]["section_wall_s"] = time.perf_counter() - t0
+    return out
 
 
 def run_ours(args):
@@ -360,6 +551,7 @@ def run_ours(args):
         "clocks": clk,
         "gpu_launches": int(prof["kernel_launches"]) * args.steps,
     }
+    res.update(run_sections(args, dev))
     print(json.dumps(res))
     if dist is not None:
         dist.destroy_process_group()

@@ -13,9 +13,12 @@ Admission is by an HBM budget: a problem starts only when its workspace, inputs
 and output fit into what the running problems leave of the budget.
 
 The persistent sweep of each problem is a cooperative launch whose CTAs wait
-for each other at a grid barrier.  Two such grids that are both only partly
-resident could each wait for SMs the other holds, so every problem here caps its
-sweep at SMs / streams CTAs: all sweeps running at once fit on the GPU together.
+for each other at a grid barrier (one CTA per SM).  Two such grids that are both
+only partly resident could each wait for SMs the other holds, so SMs are a second
+admitted resource: a problem asks for min(SMs, 128-cell tiles of a block) sweep
+CTAs and is granted what the running problems leave, but never less than its fair
+share min(asked, SMs / streams); the grants of the running problems never sum
+above the SM count, so all their sweeps fit on the GPU together.
 """
 
 from __future__ import annotations
@@ -57,6 +60,14 @@ class HarmonyResult:
     run_s: float       # run only
 
 
+def sweep_ctas_wanted(req: HarmonyRequest, sms: int) -> int:
+    """CTAs the persistent sweep of a request uses when it has the GPU alone: one
+    per 128-cell tile of a block, at most one per SM."""
+    n = int(req.Z.shape[0])
+    bs = max(1, int(n * float(req.params.get("block_proportion", 0.05))))
+    return max(1, min(sms, -(-min(bs, n) // 128)))
+
+
 def request_bytes(req: HarmonyRequest) -> int:
     """Device bytes a request holds while it runs: the engine workspace, Z
     (float32) and Z_hat, the centroids and the batch codes."""
@@ -70,7 +81,8 @@ def request_bytes(req: HarmonyRequest) -> int:
 class HarmonyServer:
     """A request loop: ``submit`` returns a Future of ``HarmonyResult``.  A
     request runs once its device bytes fit into ``hbm_budget_bytes`` next to the
-    running ones; ``streams`` worker threads each own a CUDA stream."""
+    running ones and its sweep CTAs fit into the SMs they leave; ``streams``
+    worker threads each own a CUDA stream."""
 
     def __init__(self, *, streams: int = 8, hbm_budget_bytes: int = 160 << 30, device=None):
         dev = torch.device(device) if device is not None else torch.device("cuda")
@@ -79,11 +91,12 @@ class HarmonyServer:
         self.device = dev
         self.budget = int(hbm_budget_bytes)
         self.in_use = 0
+        self.sms_in_use = 0
         self._cv = threading.Condition()
         self._q: queue.Queue = queue.Queue()
         self._closed = False
-        sms = torch.cuda.get_device_properties(self.device).multi_processor_count
-        self.sweep_ctas = max(1, sms // max(1, streams))
+        self.sms = torch.cuda.get_device_properties(self.device).multi_processor_count
+        self.fair_ctas = max(1, self.sms // max(1, streams))
         self._workers = [threading.Thread(target=self._work, daemon=True) for _ in range(streams)]
         for t in self._workers:
             t.start()
@@ -97,15 +110,22 @@ class HarmonyServer:
         self._q.put((req, need, fut, time.perf_counter()))
         return fut
 
-    def _admit(self, need: int) -> None:
+    def _admit(self, need: int, want: int) -> int:
+        """Wait until the bytes fit and at least min(want, fair share) SMs are free;
+        returns the sweep CTAs granted."""
+        floor = min(want, self.fair_ctas)
         with self._cv:
-            while self.in_use + need > self.budget:
+            while self.in_use + need > self.budget or self.sms - self.sms_in_use < floor:
                 self._cv.wait()
+            grant = min(want, self.sms - self.sms_in_use)
             self.in_use += need
+            self.sms_in_use += grant
+            return grant
 
-    def _release(self, need: int) -> None:
+    def _release(self, need: int, grant: int) -> None:
         with self._cv:
             self.in_use -= need
+            self.sms_in_use -= grant
             self._cv.notify_all()
 
     def _work(self) -> None:
@@ -123,14 +143,14 @@ class HarmonyServer:
             if setup_error is not None:
                 fut.set_exception(setup_error)
                 continue
-            self._admit(need)
+            grant = self._admit(need, sweep_ctas_wanted(req, self.sms))
             try:
                 t0 = time.perf_counter()
                 with torch.cuda.stream(stream):
                     X = torch.as_tensor(req.Z).to(self.device, torch.float32)
                     Y0 = torch.as_tensor(req.Y0).to(self.device, torch.float32)
                     params = dict(req.params)
-                    params.setdefault("max_sweep_ctas", self.sweep_ctas)
+                    params["max_sweep_ctas"] = min(grant, int(params.get("max_sweep_ctas") or grant))
                     prob = HarmonyProblem(X, req.cats, req.n_batches, Y0, req.theta,
                                           precision=req.precision, stream=stream, **params)
                     Z_hat, info = prob.run()
@@ -142,7 +162,7 @@ class HarmonyServer:
             except Exception as e:  # noqa: BLE001 - delivered to the caller through the future
                 fut.set_exception(e)
             finally:
-                self._release(need)
+                self._release(need, grant)
 
     def close(self) -> None:
         if self._closed:

@@ -73,23 +73,28 @@ __device__ __forceinline__ void group_sync(int g) {
   asm volatile("bar.sync %0, 256;" ::"r"(1 + g) : "memory");
 }
 
-// Shared memory of the sweep: NG groups, each with two A tiles, a staging tile,
-// its delta table and row tables; one centroid tile and one penalty table.
+// Shared memory of the sweep: NG groups, each with one or two A tiles, a staging
+// tile, its delta table and row tables; one centroid tile and one penalty table.
+// With one A tile the next tile's rows are gathered into it once the current
+// tile's MMA has completed (which is where they are gathered with two as well);
+// two let the gather of a block's first tile overlap the previous block's end.
 struct SweepLayout {
   TcLayout t;        // tile geometry (dpad, npad, tcols per group, ldst)
   int ng;
+  int nbuf;          // A tiles per group (2, or 1 when two do not fit)
   uint32_t atile;    // bytes of one A tile
   uint32_t offA, offB, offRst, rstBytes, offPen, offOsm, osmBytes, offRows, offMisc, bytes;
 };
 
-inline SweepLayout sweep_layout(int d, int K, int B, int ldr, int ng) {
+inline SweepLayout sweep_layout(int d, int K, int B, int ldr, int ng, int nbuf) {
   SweepLayout S{};
   S.t = tc_layout(d, K, B, ldr, 4);
   S.ng = ng;
+  S.nbuf = nbuf;
   auto al = [](uint32_t x, uint32_t a) { return (x + a - 1) / a * a; };
   S.atile = (uint32_t)S.t.kblk * 16384u;
   uint32_t o = 0;
-  S.offA = o; o += (uint32_t)ng * 2u * S.atile;
+  S.offA = o; o += (uint32_t)(ng * nbuf) * S.atile;
   S.offB = o; o += (uint32_t)S.t.kblk * S.t.npad * 128u;
   S.rstBytes = al(128u * S.t.ldst * 2u, 16);
   S.offRst = al(o, 16); o = S.offRst + (uint32_t)ng * S.rstBytes;
@@ -236,8 +241,8 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
   int(*runs)[130] = runs_s[g];
   int* nruns = nruns_s[g];
   H* R = (H*)a.R;
-  const uint32_t sA[2] = {tc::smem_u32(sm + SL.offA + (uint32_t)(2 * g) * SL.atile),
-                          tc::smem_u32(sm + SL.offA + (uint32_t)(2 * g + 1) * SL.atile)};
+  const uint32_t sA[2] = {tc::smem_u32(sm + SL.offA + (uint32_t)(SL.nbuf * g) * SL.atile),
+                          tc::smem_u32(sm + SL.offA + (uint32_t)(SL.nbuf * g + SL.nbuf - 1) * SL.atile)};
   const uint32_t sB = tc::smem_u32(sm + SL.offB);
   const size_t ldo = (size_t)(B + 1) * K;
   // this CTA's share of the state carry (the batch rows; the column-sum row is not kept)
@@ -573,16 +578,34 @@ static int launch_sweep_ng(const SweepArgs& a, const SweepLayout& SL, cudaStream
   return HB_OK;
 }
 
+// Dynamic plus static shared memory of k_tc_sweep<H, NG> fits in one CTA.
+template <typename H, int NG>
+static int sweep_fits(const SweepLayout& SL, bool& fits) {
+  cudaFuncAttributes fa;
+  HB_CUDA(cudaFuncGetAttributes(&fa, (const void*)k_tc_sweep<H, NG>));
+  int dev = 0, optin = 0;
+  HB_CUDA(cudaGetDevice(&dev));
+  HB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  fits = (size_t)SL.bytes + fa.sharedSizeBytes <= (size_t)optin && NG * SL.t.tcols <= 512;
+  return HB_OK;
+}
+
+// Layout preference: two thread groups before one, two A tiles per group before one.
 template <typename H>
 int launch_tc_sweep(const SweepArgs& a, cudaStream_t st) {
-  const SweepLayout S2 = sweep_layout(a.d, a.K, a.B, a.ldr, 2);
-  if (S2.bytes <= 227u * 1024u && 2 * S2.t.tcols <= 512) return launch_sweep_ng<H, 2>(a, S2, st);
-  const SweepLayout S1 = sweep_layout(a.d, a.K, a.B, a.ldr, 1);
-  if (S1.bytes > 227u * 1024u) {
-    set_error("tensor-core sweep: shared-memory tables too large (B=%d K=%d d=%d)", a.B, a.K, a.d);
-    return HB_ERR_UNSUPPORTED;
+  bool fits = false;
+  for (int nbuf = 2; nbuf >= 1; --nbuf) {
+    const SweepLayout S2 = sweep_layout(a.d, a.K, a.B, a.ldr, 2, nbuf);
+    HB_TRY(sweep_fits<H, 2>(S2, fits));
+    if (fits) return launch_sweep_ng<H, 2>(a, S2, st);
   }
-  return launch_sweep_ng<H, 1>(a, S1, st);
+  for (int nbuf = 2; nbuf >= 1; --nbuf) {
+    const SweepLayout S1 = sweep_layout(a.d, a.K, a.B, a.ldr, 1, nbuf);
+    HB_TRY(sweep_fits<H, 1>(S1, fits));
+    if (fits) return launch_sweep_ng<H, 1>(a, S1, st);
+  }
+  set_error("tensor-core sweep: shared-memory tables too large (B=%d K=%d d=%d)", a.B, a.K, a.d);
+  return HB_ERR_UNSUPPORTED;
 }
 template int launch_tc_sweep<__half>(const SweepArgs&, cudaStream_t);
 template int launch_tc_sweep<__nv_bfloat16>(const SweepArgs&, cudaStream_t);

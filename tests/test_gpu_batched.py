@@ -43,7 +43,7 @@ def test_server_admits_by_budget():
     need = max(request_bytes(r) for r in reqs)
     with HarmonyServer(streams=4, hbm_budget_bytes=need) as srv:  # one request at a time fits
         res = [f.result() for f in [srv.submit(r) for r in reqs]]
-        assert srv.in_use == 0
+        assert srv.in_use == 0 and srv.sms_in_use == 0
     assert all(np.isfinite(r.Z_hat.numpy()).all() for r in res)
     s = latency_summary(res)
     assert s["p99_ms"] >= s["p50_ms"] > 0

@@ -107,3 +107,22 @@ def test_16bit_many_tiles_per_cta_vs_plain_fp32(prec):
           f"{ref_info.objectives_harmony}")
     np.testing.assert_allclose(info.objectives_harmony, ref_info.objectives_harmony, rtol=5e-3)
     assert err < 5e-3
+
+
+def test_bf16_wide_shapes_vs_plain_fp32():
+    """The 2M-cell workload's shapes (100 PCs, K = 200, 32 Zipf-sized batches) on
+    120,000 cells: the sweep runs one thread group per CTA with one A tile (two do
+    not fit in shared memory next to the 32 x 200 tables) and the centroid pass
+    runs in list order (660 (block, batch) keys); checked against plain fp32."""
+    cfg = make_config("C3", seed=5, n_cells=120_000)
+    kw = dict(n_clusters=200, max_iter_harmony=2, max_iter_clustering=4, tol_harmony=-np.inf,
+              tol_clustering=-np.inf)
+    labels = pd.Categorical.from_codes(cfg["cats"], categories=[f"b{i}" for i in range(cfg["n_batches"])])
+    Z = torch.as_tensor(cfg["Z"], device="cuda")
+    ref, ref_info = harmonize(Z, labels, None, init_centroids=cfg["Y0"], precision="fp32", return_info=True, **kw)
+    out, info = harmonize(Z, labels, None, init_centroids=cfg["Y0"], precision="bf16", return_info=True, **kw)
+    err = rel_maxabs(out.cpu().numpy(), ref.cpu().numpy())
+    print(f"bf16 vs plain fp32 (C3 shapes): rel max-abs {err:.3e}; objectives "
+          f"{info.objectives_harmony} vs {ref_info.objectives_harmony}")
+    np.testing.assert_allclose(info.objectives_harmony, ref_info.objectives_harmony, rtol=5e-3)
+    assert err < 5e-3

@@ -380,8 +380,10 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
       // pass 1: v = exp(-2/sigma (1-s)) * pen = exp2(pc - c2 s) (one SFU op), row
       // partial sums of v, v s (kmeans error) and v * exponent (entropy); v
       // overwrites s in TMEM.  Two 8-column loads are in flight per wait.
+      // warps whose 32 rows all lie past the tile's cells skip both passes (warp-uniform)
+      const bool rows_live = (gw & 3) * 32 < nvalid;
       float rs = 0.f, kx = 0.f, vx = 0.f;
-      for (int c = c_lo; c < c_hi; c += 16) {
+      if (rows_live) for (int c = c_lo; c < c_hi; c += 16) {
         const bool two = c + 8 < c_hi;
         float v[8], w2[8], pc[16];
         tc::tmem_ld8(tl + (uint32_t)c, v);
@@ -415,7 +417,7 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
       const float rsafe = a.init_mode ? fmaxf(rsum, 1e-12f) : rsum;
       const float inv = 1.f / rsafe;
       // pass 2: normalise, round to 16 bits, stage the row (for the counts and the R store)
-      for (int c = c_lo; c < c_hi; c += 16) {
+      if (rows_live) for (int c = c_lo; c < c_hi; c += 16) {
         const bool two = c + 8 < c_hi;
         float v[8], w2[8];
         tc::tmem_ld8(tl + (uint32_t)c, v);

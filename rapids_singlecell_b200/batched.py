@@ -155,7 +155,10 @@ class HarmonyServer:
                                           precision=req.precision, stream=stream, **params)
                     Z_hat, info = prob.run()
                     prob.close()
-                    out = Z_hat.to("cpu") if req.to_host else Z_hat
+                    out = Z_hat
+                    if req.to_host:  # pinned (torch's caching host allocator): no staged copy
+                        out = torch.empty(Z_hat.shape, dtype=Z_hat.dtype, pin_memory=True)
+                        out.copy_(Z_hat, non_blocking=True)
                 stream.synchronize()
                 t1 = time.perf_counter()
                 fut.set_result(HarmonyResult(out, info, t1 - t_submit, t1 - t0))

@@ -106,6 +106,48 @@ struct hb_plan {
 
 namespace {
 
+// Pinned host buffers for read-backs, reused across runs and never freed.  Copies into
+// pageable memory are staged by the driver and serialised plans running at the same time
+// on other streams; cudaFreeHost would synchronise the device.
+class PinnedLease {
+ public:
+  explicit PinnedLease(size_t bytes) {
+    std::lock_guard<std::mutex> lock(mu());
+    auto& pool = free_list();
+    for (size_t i = 0; i < pool.size(); ++i)
+      if (pool[i].second >= bytes) {
+        ptr = pool[i].first;
+        size = pool[i].second;
+        pool.erase(pool.begin() + (long)i);
+        return;
+      }
+    size = std::max<size_t>(bytes, 4096);
+    if (cudaMallocHost(&ptr, size) != cudaSuccess) {
+      cudaGetLastError();
+      ptr = nullptr;
+    }
+  }
+  ~PinnedLease() {
+    if (!ptr) return;
+    std::lock_guard<std::mutex> lock(mu());
+    free_list().emplace_back(ptr, size);
+  }
+  PinnedLease(const PinnedLease&) = delete;
+  PinnedLease& operator=(const PinnedLease&) = delete;
+  void* ptr = nullptr;
+  size_t size = 0;
+
+ private:
+  static std::mutex& mu() {
+    static std::mutex m;
+    return m;
+  }
+  static std::vector<std::pair<void*, size_t>>& free_list() {
+    static std::vector<std::pair<void*, size_t>> v;
+    return v;
+  }
+};
+
 struct Work {
   void* Zn;
   void* R;
@@ -432,9 +474,18 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
     HB_TRY(launch_objective_finalize(ring.state(), w.Pr, w.theta, p.sigma, B, K, p.stabilized_penalty,
                                      w.obj_acc, obj_init, st));
   }
-  double h_obj = 0;
-  HB_CUDA(cudaMemcpyAsync(&h_obj, obj_init, sizeof(double), cudaMemcpyDeviceToHost, st));
+  // pinned read-back slots: [0] one objective, [1 ..] the k-means objectives of an outer
+  // iteration, then the error flags
+  PinnedLease host(sizeof(double) * ((size_t)p.max_iter_clustering + 2) + 4 * sizeof(int));
+  if (!host.ptr) {
+    set_error("pinned host buffer for the read-backs: cudaMallocHost failed");
+    return HB_ERR_CUDA;
+  }
+  double* h_dbl = (double*)host.ptr;
+  int* h_err = (int*)(h_dbl + p.max_iter_clustering + 2);
+  HB_CUDA(cudaMemcpyAsync(h_dbl, obj_init, sizeof(double), cudaMemcpyDeviceToHost, st));
   HB_CUDA(cudaStreamSynchronize(st));
+  double h_obj = h_dbl[0];
   std::vector<double> objs{h_obj};
   int converged = 0;
   const MembershipLayout& ml = P->ml;
@@ -524,8 +575,9 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
                                          p.stabilized_penalty, w.obj_acc, w.obj_out + it, st));
         }
         if (early_stop) {
-          HB_CUDA(cudaMemcpyAsync(&h_obj, w.obj_out + it, sizeof(double), cudaMemcpyDeviceToHost, st));
+          HB_CUDA(cudaMemcpyAsync(h_dbl, w.obj_out + it, sizeof(double), cudaMemcpyDeviceToHost, st));
           HB_CUDA(cudaStreamSynchronize(st));
+          h_obj = h_dbl[0];
           kobj.push_back(h_obj);
           // window-3 convergence (clustering.cu:380-387)
           const size_t m = kobj.size();
@@ -537,16 +589,16 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
         }
       }
     }
-    if (!early_stop && p.max_iter_clustering > 0) {
-      kobj.resize(p.max_iter_clustering);
-      HB_CUDA(cudaMemcpyAsync(kobj.data(), w.obj_out, sizeof(double) * p.max_iter_clustering,
+    const bool read_kobj = !early_stop && p.max_iter_clustering > 0;
+    if (read_kobj)
+      HB_CUDA(cudaMemcpyAsync(h_dbl + 1, w.obj_out, sizeof(double) * p.max_iter_clustering,
                               cudaMemcpyDeviceToHost, st));
-    }
     {
-      int err[2] = {0, 0};
+      int* err = h_err;
       HB_CUDA(cudaMemcpyAsync(&err[0], w.mb.err, sizeof(int), cudaMemcpyDeviceToHost, st));
       HB_CUDA(cudaMemcpyAsync(&err[1], w.err, sizeof(int), cudaMemcpyDeviceToHost, st));
       HB_CUDA(cudaStreamSynchronize(st));
+      if (read_kobj) kobj.assign(h_dbl + 1, h_dbl + 1 + p.max_iter_clustering);
       if (err[0]) { set_error("block splitter candidate buffer overflow"); return HB_ERR_INTERNAL; }
       if (err[1] == 7) { set_error("fp16 correction: |X| or |W| reaches 65504, outside the fp16 range; use bf16"); return HB_ERR_UNSUPPORTED; }
       if (err[1]) { set_error("tensor-core wait timed out (code %d)", err[1]); return HB_ERR_TIMEOUT; }
@@ -587,9 +639,9 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
   }
   {
     // errors of the last correction (the loop checks the flags before each correction)
-    int err = 0;
-    HB_CUDA(cudaMemcpyAsync(&err, w.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    HB_CUDA(cudaMemcpyAsync(h_err + 2, w.err, sizeof(int), cudaMemcpyDeviceToHost, st));
     HB_CUDA(cudaStreamSynchronize(st));
+    const int err = h_err[2];
     if (err == 7) { set_error("fp16 correction: |X| or |W| reaches 65504, outside the fp16 range; use bf16"); return HB_ERR_UNSUPPORTED; }
     if (err) { set_error("tensor-core wait timed out (code %d)", err); return HB_ERR_TIMEOUT; }
   }

@@ -12,7 +12,7 @@
 // both accumulated in TMEM over the CTA's tiles (A = R_tile^T is shared).  The
 // one-hot tile stays resident: per tile only the previous tile's ones are
 // cleared and the new ones set.  D1 and D2 are written once per CTA and summed
-// over the CTAs by k_centroid_reduce and k_opart_reduce.
+// over the CTAs by k_cs_reduce (one launch for both).
 //
 // Tensor maps: Z_norm and R viewed as 4-D {64 values, 8 rows, 64-value blocks,
 // 8-row groups}, box {64, 8, blocks, 16}, so one load lands a tile in the
@@ -27,7 +27,8 @@ namespace hb {
 
 struct CsLayout {
   int nbZ, nbB, nbK, nM2, ncolsZ, nkpad, tcols, stages;
-  uint32_t stZ, stB, offZ, offB, offOH, offBar, bytes;
+  int noh;  // one-hot operands (2: the one-hot of tile i+1 is written while tile i's MMAs run)
+  uint32_t stZ, stB, offZ, offB, offOH, ohBytes, offBar, bytes;
 };
 
 inline CsLayout cs_layout(int d, int K, int nkeys, int ldz) {
@@ -43,15 +44,24 @@ inline CsLayout cs_layout(int d, int K, int nkeys, int ldz) {
   L.tcols = t;
   L.stZ = (uint32_t)L.nbZ * 16384u;
   L.stB = (uint32_t)L.nbB * 16384u;
-  for (int st = 4; st >= 2; --st) {
-    uint32_t o = 0;
-    L.offZ = o; o += (uint32_t)st * L.stZ;
-    L.offB = o; o += (uint32_t)st * L.stB;
-    L.offOH = o; o += (uint32_t)L.nbK * 16384u;
-    L.offBar = o; o += 16u * 8u + 16u;
-    L.bytes = o + 1024u;
-    L.stages = st;
-    if (L.bytes <= 220u * 1024u) break;
+  L.ohBytes = (uint32_t)L.nbK * 16384u;
+  // two one-hot operands when they fit beside three tile stages (without the second one the
+  // per-tile period is MMA -> one-hot rewrite -> MMA in series; with two stages the loads
+  // fall behind, which costs more: 500k cells, 180 keys measured 73 vs 68 us per pass)
+  for (int noh = 2; noh >= 1; --noh) {
+    bool fits = false;
+    for (int st = 4; st >= (noh == 2 ? 3 : 2) && !fits; --st) {
+      uint32_t o = 0;
+      L.offZ = o; o += (uint32_t)st * L.stZ;
+      L.offB = o; o += (uint32_t)st * L.stB;
+      L.offOH = o; o += (uint32_t)noh * L.ohBytes;
+      L.offBar = o; o += 16u * 8u + 16u;
+      L.bytes = o + 1024u;
+      L.stages = st;
+      L.noh = noh;
+      fits = L.bytes <= 220u * 1024u;
+    }
+    if (fits) break;
   }
   (void)d;
   return L;
@@ -76,11 +86,12 @@ __global__ void __launch_bounds__(256, 1) k_tc_centroid_stream(CenStreamArgs a, 
   unsigned char* sm = (unsigned char*)(((uintptr_t)smem_dyn + 1023) & ~(uintptr_t)1023);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int K = a.K, S = L.stages;
+  const int NOH = L.noh;
   uint64_t* full = (uint64_t*)(sm + L.offBar);  // [S] tile landed
-  uint64_t* mma_done = full + 4;                // MMAs of a tile completed (one phase per tile)
-  uint64_t* oh_ready = full + 5;                // one-hot of the next tile written (one phase per tile)
-  uint64_t* empty = full + 6;                   // [S] MMAs of the stage's last tile completed
-  uint64_t* acc_bar = full + 10;                // all MMAs of the CTA completed (one phase)
+  uint64_t* mma_done = full + 4;                // [NOH] MMAs of a tile on one-hot b completed (phase per such tile)
+  uint64_t* oh_ready = full + 6;                // [NOH] one-hot b holds its next tile (phase per such tile)
+  uint64_t* empty = full + 8;                   // [S] MMAs of the stage's last tile completed
+  uint64_t* acc_bar = full + 12;                // all MMAs of the CTA completed (one phase)
   uint32_t* tmem_slot = (uint32_t*)(sm + L.offBar + 128);
   const uint32_t sm32 = tc::smem_u32(sm);
   const int t0 = (int)((int64_t)a.ntiles * blockIdx.x / gridDim.x);
@@ -94,13 +105,15 @@ __global__ void __launch_bounds__(256, 1) k_tc_centroid_stream(CenStreamArgs a, 
   }
   if (tid == 0) {
     for (int s = 0; s < S; ++s) tc::mbar_init(full + s, 1);
-    tc::mbar_init(mma_done, 1);
-    tc::mbar_init(oh_ready, 4);
+    for (int b = 0; b < NOH; ++b) {
+      tc::mbar_init(mma_done + b, 1);
+      tc::mbar_init(oh_ready + b, 4);
+    }
     for (int s = 0; s < S; ++s) tc::mbar_init(empty + s, 1);
     tc::mbar_init(acc_bar, 1);
     tc::fence_mbar_init();
   }
-  for (uint32_t e = tid * 16u; e < (uint32_t)L.nbK * 16384u; e += 256u * 16u)
+  for (uint32_t e = tid * 16u; e < (uint32_t)NOH * L.ohBytes; e += 256u * 16u)
     *(uint4*)(sm + L.offOH + e) = make_uint4(0u, 0u, 0u, 0u);
   __syncthreads();
   tc::fence_after_sync();
@@ -115,19 +128,23 @@ __global__ void __launch_bounds__(256, 1) k_tc_centroid_stream(CenStreamArgs a, 
   const uint32_t idesc1 = tc::idesc_f16(128, L.ncolsZ, is_bf16<H>::value, true, true);
   const uint32_t idesc2 = tc::idesc_f16(128, L.nkpad, is_bf16<H>::value, true, true);
   // Roles (no CTA-wide barrier inside the loop):
-  //   thread 0      MMA issuer: waits for the tile (full[s]) and its one-hot (oh_ready),
-  //                 commits to mma_done (one phase per tile);
+  //   thread 0      MMA issuer: waits for the tile (full[s]) and its one-hot (oh_ready[b],
+  //                 b = i % NOH), commits to mma_done[b];
   //   thread 32     TMA producer: loads tile j into its stage once the MMAs of the
   //                 stage's previous tile completed (empty[s]);
-  //   warps 4-7     one-hot writers (row = thread - 128): once tile i-1's MMAs
-  //                 completed, clear its ones and set tile i's; one arrival per warp.
+  //   warps 4-7     one-hot writers (row = thread - 128): once the MMAs of tile i - NOH
+  //                 (the last user of one-hot b) completed, clear its ones and set tile
+  //                 i's; one arrival per warp on oh_ready[b].
+  // One barrier pair per one-hot operand: a waiter of either never falls two phases behind.
   if (tid == 0) {
     for (int i = 0; i < nt; ++i) {
       const int s = i % S;
       if (!tc::mbar_wait(full + s, (uint32_t)((i / S) & 1), kMaxPolls)) atomicExch(a.err, 6);
-      if (!tc::mbar_wait(oh_ready, (uint32_t)(i & 1), kMaxPolls)) atomicExch(a.err, 6);
+      const int b = i % NOH;
+      if (!tc::mbar_wait(oh_ready + b, (uint32_t)((i / NOH) & 1), kMaxPolls)) atomicExch(a.err, 6);
       tc::fence_after_sync();
-      const uint32_t sZ = sm32 + L.offZ + s * L.stZ, sB = sm32 + L.offB + s * L.stB, sH = sm32 + L.offOH;
+      const uint32_t sZ = sm32 + L.offZ + s * L.stZ, sB = sm32 + L.offB + s * L.stB;
+      const uint32_t sH = sm32 + L.offOH + (uint32_t)b * L.ohBytes;
       for (int m = 0; m < L.nM2; ++m) {
         const uint32_t d1 = tmem + (uint32_t)(m * L.ncolsZ);
         const uint32_t d2 = tmem + (uint32_t)(L.nM2 * L.ncolsZ + m * L.nkpad);
@@ -144,7 +161,7 @@ __global__ void __launch_bounds__(256, 1) k_tc_centroid_stream(CenStreamArgs a, 
         }
       }
       tc::mma_commit(empty + s);
-      tc::mma_commit(mma_done);
+      tc::mma_commit(mma_done + b);
     }
     if (nt > 0) tc::mma_commit(acc_bar);
   } else if (tid == 32) {
@@ -167,24 +184,26 @@ __global__ void __launch_bounds__(256, 1) k_tc_centroid_stream(CenStreamArgs a, 
              ((((uint32_t)(k & 63) >> 3) ^ (uint32_t)(r & 7)) << 4) + (uint32_t)(k & 7) * 2u;
     };
     const H one = from_f<H>(1.f), zero = from_f<H>(0.f);
-    unsigned char* oh = sm + L.offOH;
     int kq[4];  // keys of tiles i .. i+3
 #pragma unroll
     for (int q = 0; q < 4; ++q) kq[q] = key_of(q);
-    int key_old = -1;
+    int key_old[2] = {-1, -1};  // the key set in each one-hot operand
     for (int i = 0; i < nt; ++i) {
-      if (i >= 1 && !tc::mbar_wait(mma_done, (uint32_t)((i - 1) & 1), kMaxPolls)) atomicExch(a.err, 5);
+      const int b = i % NOH;
+      if (i >= NOH && !tc::mbar_wait(mma_done + b, (uint32_t)(((i - NOH) / NOH) & 1), kMaxPolls))
+        atomicExch(a.err, 5);
+      unsigned char* oh = sm + L.offOH + (uint32_t)b * L.ohBytes;
       const int key = kq[0];
-      if (key_old >= 0) *(H*)(oh + oh_off(row, key_old)) = zero;
+      if (key_old[b] >= 0) *(H*)(oh + oh_off(row, key_old[b])) = zero;
       if (key >= 0) *(H*)(oh + oh_off(row, key)) = one;
-      key_old = key;
+      key_old[b] = key;
       kq[0] = kq[1];
       kq[1] = kq[2];
       kq[2] = kq[3];
       kq[3] = key_of(i + 4);
       tc::fence_proxy_async_smem();
       __syncwarp();
-      if (lane == 0) mbar_arrive_cta(oh_ready);
+      if (lane == 0) mbar_arrive_cta(oh_ready + b);
     }
   }
   // Threads without a role wait here in the hardware barrier: spinning on an mbarrier in the
@@ -231,16 +250,57 @@ __global__ void __launch_bounds__(256, 1) k_tc_centroid_stream(CenStreamArgs a, 
   }
 }
 
-// Omin[key][k] += sum over the G CTAs of Opart[cta][key][k] (Omin zeroed by the caller).
-// blockIdx.y takes every gridDim.y-th CTA partial; its float64 sum is added atomically.
-__global__ void k_opart_reduce(const float* __restrict__ Opart, int G, int nkeys, int K, double* __restrict__ Omin) {
-  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+// Both reductions of the per-CTA partials in one launch (one wave), 32 x 8 threads per CTA;
+// threadIdx.y takes every 8th CTA partial and the eight float64 sums are combined in shared
+// memory:
+//   CTAs 0 .. K-1: centroid row k = blockIdx.x, Y[k] = sum_g P[g][k][:], written L2-normalised
+//                  as 16-bit Y_norm (inverse norm capped at 1e12, kernels_normalize.cuh:7-54);
+//   the others:    32 consecutive (key, cluster) entries e, Omin[e] = sum_g Opart[g][e].
+template <typename H>
+__global__ void __launch_bounds__(256) k_cs_reduce(const float* __restrict__ P, const float* __restrict__ Opart, int G,
+                                                   int K, int d, int nkeys, H* __restrict__ Yn, int ldy,
+                                                   double* __restrict__ Omin) {
+  __shared__ double part[8][128];
+  __shared__ double red[32];
+  const int lane = threadIdx.x, y = threadIdx.y, t = y * 32 + lane;
+  if ((int)blockIdx.x < K) {
+    const int k = blockIdx.x;
+    for (int c0 = 0; c0 < d; c0 += 128) {  // d <= 128 on this path: one round
+      for (int c = c0 + lane; c < min(d, c0 + 128); c += 32) {
+        double s = 0.0;
+#pragma unroll 8
+        for (int g = y; g < G; g += 8) s += (double)__ldg(P + ((size_t)g * K + k) * d + c);
+        part[y][c - c0] = s;
+      }
+    }
+    __syncthreads();
+    double v = 0.0, ss = 0.0;
+    if (t < d) {
+#pragma unroll
+      for (int q = 0; q < 8; ++q) v += part[q][t];
+      ss = v * v;
+    }
+    ss = block_sum(ss, red);
+    double inv = rsqrt(ss);
+    if (inv > 1e12) inv = 1e12;
+    for (int c = t; c < ldy; c += 256) Yn[(size_t)k * ldy + c] = from_f<H>(c < d ? (float)(v * inv) : 0.f);
+    return;
+  }
   const int64_t ne = (int64_t)nkeys * K;
-  if (e >= ne) return;
+  const int64_t e = (int64_t)(blockIdx.x - K) * 32 + lane;
   double s = 0.0;
-#pragma unroll 4
-  for (int g = blockIdx.y; g < G; g += gridDim.y) s += (double)__ldg(Opart + (size_t)g * ne + e);
-  if (s != 0.0) atomicAdd(Omin + e, s);
+  if (e < ne) {
+#pragma unroll 8
+    for (int g = y; g < G; g += 8) s += (double)__ldg(Opart + (size_t)g * ne + e);
+  }
+  part[y][lane] = s;
+  __syncthreads();
+  if (y == 0 && e < ne) {
+    double tot = 0.0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) tot += part[q][lane];
+    Omin[e] = tot;
+  }
 }
 
 // 4-D view {64 values, 8 rows, blocks, 8-row groups} of a [rows][ld] 16-bit array, box {64, 8, blocks, 16}.
@@ -288,7 +348,8 @@ int launch_tc_centroid_stream(const CenStreamArgs& a, const void* Zn, int ldz, c
   k_tc_centroid_stream<H><<<grid, 256, smem, st>>>(a, L, tmZ, tmR);
   HB_LAUNCH_CHECK();
   const int64_t ne = (int64_t)a.nkeys * a.K;
-  k_opart_reduce<<<dim3((unsigned)((ne + 255) / 256), 8), 256, 0, st>>>(a.Opart, grid, a.nkeys, a.K, Omin);
+  k_cs_reduce<H><<<(unsigned)(a.K + (ne + 31) / 32), dim3(32, 8), 0, st>>>(a.P, a.Opart, grid, a.K, a.d, a.nkeys,
+                                                                        (H*)a.Yn, a.ldy, Omin);
   HB_LAUNCH_CHECK();
   return HB_OK;
 }

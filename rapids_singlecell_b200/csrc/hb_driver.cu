@@ -537,12 +537,15 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
         // the block-ordered cell list, so it also sums every block's current rows per
         // batch: the "remove old contribution" terms of the sweep (clustering.cu:321-332).
         const size_t omsz = (size_t)(B + 1) * K;
-        HB_CUDA(cudaMemsetAsync(w.Omin, 0, sizeof(double) * nblk * omsz, st));
+        // the other passes add into Omin; the cell-order pass writes every entry
+        bool writes_omin = false;
+        if constexpr (tc_path) writes_omin = P->cen_stream;
+        if (!writes_omin) HB_CUDA(cudaMemsetAsync(w.Omin, 0, sizeof(double) * nblk * omsz, st));
         int sp = span_begin(1, (double)n * (zb + rb + 8));
         if constexpr (tc_path) {
           if (P->cen_stream) {
             CenStreamArgs ca{n, (int)((P->rows_alloc - 8) / 128), w.ckey + (size_t)c * n, d, K, P->nkeys,
-                             (float*)w.Ypart, w.Opart, w.err};
+                             (float*)w.Ypart, w.Opart, w.err, Yn, P->ldy};
             HB_TRY(launch_tc_centroid_stream<S>(ca, Zn, P->ldz, R, P->ldr, P->rows_alloc, P->cen_chunks, w.Omin, st));
           } else {
             CenArgs ca{Zn, P->ldz, R, P->ldr, cats, idx, lcat, n, ml.bs, d, K, B, (float*)w.Ypart, w.Omin, w.err};
@@ -552,7 +555,9 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
           HB_TRY(launch_accum<S, S, TA>(R, P->ldr, Zn, P->ldz, idx, w.cen_chunks, P->cen_chunks, K, d,
                                         (TA*)w.Ypart, st, OminArgs{w.Omin, cats, ml.bs, B}));
         }
-        HB_TRY(launch_centroid_reduce<TA, S>((TA*)w.Ypart, P->cen_chunks, K, d, Yn, P->ldy, st));
+        bool reduced = false;  // the cell-order pass reduces its partials itself
+        if constexpr (tc_path) reduced = P->cen_stream;
+        if (!reduced) HB_TRY(launch_centroid_reduce<TA, S>((TA*)w.Ypart, P->cen_chunks, K, d, Yn, P->ldy, st));
         span_end(sp);
         // sweep the blocks (clustering.cu:308-372)
         if constexpr (tc_path) {

@@ -179,6 +179,8 @@ struct CenStreamArgs {
   float* P;              // [G][K][d] partial sums
   float* Opart;          // [G][nkeys][K] partial per-key sums
   int* err;
+  void* Yn;              // [K][ldy] 16-bit normalised centroids (written by the reduction)
+  int ldy;
 };
 bool cs_supported(int d, int K, int nkeys, int ldz);
 int make_tile_map4(CUtensorMap* tm, const void* base, int64_t rows, int ld, int blocks, bool bf16);

@@ -238,6 +238,7 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
   __shared__ int2 gslice[NG][kMaxBlocks];  // each group's slice of every block (list positions)
   __shared__ int runs_s[NG][2][130];       // run starts of the two tile buffers
   __shared__ int nruns_s[NG][2];
+  __shared__ double carry_s[NT];           // the thread's first state-carry entry of the block
   int(*runs)[130] = runs_s[g];
   int* nruns = nruns_s[g];
   H* R = (H*)a.R;
@@ -311,8 +312,17 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
     const double* Omc = (a.Omin && j == 0) ? a.Omin : nullptr;                       // this block
     const double* Omn = (a.Omin && j + 1 < a.nblk) ? a.Omin + (size_t)(j + 1) * ldo : nullptr;  // next
     for (size_t e = (size_t)blockIdx.x * NT + tid; e < ldo; e += (size_t)gridDim.x * NT) Ozero[e] = 0.0;
-    // one round of loads: the column sums (into ocol, zeroed in the previous block)
-    // and the state entries of the first penalty rows
+    // one round of loads: this CTA's share of the state carry (O_in - old(this block) -
+    // old(next block); the first NT entries, parked in shared memory below so that the flush
+    // before the grid arrival does not wait for L2), the column sums (into ocol, zeroed in the
+    // previous block) and the state entries of the first penalty rows
+    const bool carry_mine = carry0 + tid < carry1;
+    double c_in = 0.0, c_mc = 0.0, c_mn = 0.0;
+    if (carry_mine) {
+      c_in = Oin[carry0 + tid];
+      if (Omc) c_mc = Omc[carry0 + tid];
+      if (Omn) c_mn = Omn[carry0 + tid];
+    }
     float* ocol = ocol_s[j & 1];
     const int cmin = crange[j].x, cmax = crange[j].y;
     const int npen = (cmax - cmin + 1) * ldp;
@@ -328,6 +338,7 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
       }
     }
     if (!a.init_mode) column_sums(Oin, Omc, B, K, ocol, NT);
+    if (carry_mine) carry_s[tid] = c_in - c_mc - c_mn;  // read back by this thread at the flush
     for (int k = tid; k < K; k += NT) ocol_s[(j + 1) & 1][k] = 0.f;
     __syncthreads();
     // exponent offsets of the batches present: v = exp2(c2 (1 - s) + log2 pen)
@@ -493,7 +504,8 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
       if (v != 0.f) atomicAdd(&Oout[o_at], (double)v);
     }
     // carry the state forward (O_in - old(this block) - old(next block)), spread over the CTAs
-    for (int e = carry0 + tid; e < carry1; e += NT) {
+    if (carry_mine && carry_s[tid] != 0.0) atomicAdd(&Oout[carry0 + tid], carry_s[tid]);
+    for (int e = carry0 + tid + NT; e < carry1; e += NT) {
       double v = Oin[e];
       if (Omc) v -= Omc[e];
       if (Omn) v -= Omn[e];

@@ -21,6 +21,7 @@
  *   hb_ridge_inverse      -> _harmony_correction_cuda.compute_inv_mat
  *                            (_cuda/harmony/correction/kernels_correction_fast.cuh:24-123)
  *   hb_lambda_kb          -> _compute_lambda_kb (preprocessing/_harmony/__init__.py:454-480)
+ *   hb_kmeans_init        -> the cuML KMeans fit in _initialize_centroids (__init__.py:290-323)
  *   hb_similarity         -> the similarity GEMM of clustering_loop_impl
  *                            (_cuda/harmony/clustering/clustering.cu:284-289)
  */
@@ -171,6 +172,20 @@ HB_API int hb_ridge_inverse(const double* O, const double* lambda_kb, double* in
 HB_API int hb_similarity(const void* Zn, int32_t ldz, const void* Yn, int32_t ldy, const int32_t* idx,
                   int64_t n, int32_t n_pcs, int32_t n_clusters, int32_t dtype, float* S,
                   int32_t* err, void* stream);
+
+/* Initial centroids by a seeded k-means on the L2-normalised rows of X (float32 [n, n_pcs],
+ * row-major): k-means++ seeding over a sample of min(n, 64 n_clusters, 16384) cells drawn
+ * from `seed`, then up to max_iter Lloyd iterations over all cells with tensor-core (bf16)
+ * assignment, stopping when |Y_new - Y_old|_F <= tol |Y_new|_F.  Y_out (float32
+ * [n_clusters, n_pcs], device) receives the centres (not normalised); *n_iter_out the Lloyd
+ * iterations run.  n_pcs <= 128, n_clusters <= 256 and <= n.  Synchronises the stream once
+ * per iteration.  Replaces the cuML KMeans(init="k-means||", max_iter=25) fit of the
+ * reference's _initialize_centroids (preprocessing/_harmony/__init__.py:290-323); cuML's
+ * random streams are not reproduced. */
+HB_API size_t hb_kmeans_workspace_bytes(int64_t n, int32_t n_pcs, int32_t n_clusters);
+HB_API int hb_kmeans_init(const float* X, int64_t n, int32_t n_pcs, int32_t n_clusters, int32_t max_iter,
+                          double tol, uint64_t seed, float* Y_out, int32_t* n_iter_out, void* workspace,
+                          size_t workspace_bytes, void* stream);
 
 HB_API const char* hb_last_error(void);
 HB_API const char* hb_version(void);

@@ -30,7 +30,8 @@ EXPORTED = (
     "hb_plan_create", "hb_plan_destroy", "hb_plan_workspace_bytes", "hb_harmonize",
     "hb_l2_normalize", "hb_block_lists_workspace_bytes", "hb_block_lists", "hb_block_lists_static",
     "hb_penalty",
-    "hb_lambda_kb", "hb_ridge_inverse", "hb_similarity", "hb_last_error", "hb_version",
+    "hb_lambda_kb", "hb_ridge_inverse", "hb_similarity", "hb_kmeans_workspace_bytes", "hb_kmeans_init",
+    "hb_last_error", "hb_version",
 )
 
 
@@ -135,6 +136,11 @@ def load() -> ctypes.CDLL:
     lib.hb_similarity.argtypes = [c_void_p, c_i32, c_void_p, c_i32, c_void_p, c_i64, c_i32, c_i32,
                                   c_i32, c_void_p, c_void_p, c_void_p]
     lib.hb_similarity.restype = c_int
+    lib.hb_kmeans_workspace_bytes.argtypes = [c_i64, c_i32, c_i32]
+    lib.hb_kmeans_workspace_bytes.restype = c_size
+    lib.hb_kmeans_init.argtypes = [c_void_p, c_i64, c_i32, c_i32, c_i32, ctypes.c_double, ctypes.c_uint64,
+                                   c_void_p, P(c_i32), c_void_p, c_size, c_void_p]
+    lib.hb_kmeans_init.restype = c_int
     lib.hb_last_error.argtypes = []
     lib.hb_last_error.restype = ctypes.c_char_p
     lib.hb_version.argtypes = []

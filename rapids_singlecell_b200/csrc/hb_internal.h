@@ -3,6 +3,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
+#include <utility>
+#include <vector>
 #include <cuda.h>
 #include "hb_common.cuh"
 
@@ -223,5 +226,48 @@ template <typename H>
 int launch_tc_apply(const float* X, int ldx, const H* R, int ldr, const float* W, const int32_t* cell_index,
                     const ApplyTile* tiles, int n_tiles, int K, int d, float* Zhat, int ldzh, H* Zn, int ldz,
                     int* err, cudaStream_t st);
+
+// ---- host helpers -------------------------------------------------------------
+// Pinned host buffers for read-backs, reused across runs and never freed.  Copies into
+// pageable memory are staged by the driver and serialised plans running at the same time
+// on other streams; cudaFreeHost would synchronise the device.
+class PinnedLease {
+ public:
+  explicit PinnedLease(size_t bytes) {
+    std::lock_guard<std::mutex> lock(mu());
+    auto& pool = free_list();
+    for (size_t i = 0; i < pool.size(); ++i)
+      if (pool[i].second >= bytes) {
+        ptr = pool[i].first;
+        size = pool[i].second;
+        pool.erase(pool.begin() + (long)i);
+        return;
+      }
+    size = std::max<size_t>(bytes, 4096);
+    if (cudaMallocHost(&ptr, size) != cudaSuccess) {
+      cudaGetLastError();
+      ptr = nullptr;
+    }
+  }
+  ~PinnedLease() {
+    if (!ptr) return;
+    std::lock_guard<std::mutex> lock(mu());
+    free_list().emplace_back(ptr, size);
+  }
+  PinnedLease(const PinnedLease&) = delete;
+  PinnedLease& operator=(const PinnedLease&) = delete;
+  void* ptr = nullptr;
+  size_t size = 0;
+
+ private:
+  static std::mutex& mu() {
+    static std::mutex m;
+    return m;
+  }
+  static std::vector<std::pair<void*, size_t>>& free_list() {
+    static std::vector<std::pair<void*, size_t>> v;
+    return v;
+  }
+};
 
 }  // namespace hb

@@ -1,0 +1,441 @@
+// Seeded k-means initialisation of the Harmony centroids on the GPU.
+//
+// The reference starts Harmony from cuML's KMeans (init="k-means||", n_init=1,
+// max_iter=25, random_state) fitted on the L2-normalised embedding, and then
+// L2-normalises the centres (preprocessing/_harmony/__init__.py:290-323).  cuML
+// is a third-party library whose random streams cannot be reproduced here; this
+// is the engine's own seeded k-means in the same role, with the same iteration
+// budget:
+//   seeding  k-means++ (Arthur & Vassilvitskii, 2007: each new centre is drawn
+//            with probability proportional to the squared distance to the
+//            nearest centre chosen so far) over a sample of m cells (all cells
+//            when n <= m, else m draws with replacement), in float64 with
+//            explicitly rounded operations and sequential sums, on one CTA; the
+//            draws come from splitmix64 (Steele, Lea & Flood, 2014) of (seed,
+//            counter), so a seed fixes the result bit for bit;
+//   Lloyd    up to max_iter iterations over all cells: the assignment is the
+//            tensor-core similarity of a 128-cell tile of bf16 Z_norm against the
+//            bf16 centres (fp32 in TMEM), argmax_k (z.y_k - |y_k|^2 / 2), which is
+//            the nearest centre for unit rows; each CTA adds its rows to their
+//            centre's sum in shared memory; the per-CTA sums are reduced per
+//            centre, and a centre that lost all its cells keeps its position.
+//            Stops when |Y_new - Y_old|_F <= tol |Y_new|_F.
+#include "hb_tc_tile.cuh"
+
+namespace hb {
+
+// ---- counter-based draws ------------------------------------------------------------
+__host__ __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+// draw `ctr` of stream `seed`
+__host__ __device__ __forceinline__ uint64_t km_draw(uint64_t seed, uint64_t ctr) {
+  return splitmix64(splitmix64(seed) ^ ctr);
+}
+// uniform in [0, 1) from the top 53 bits
+__host__ __device__ __forceinline__ double km_u01(uint64_t h) { return (double)(h >> 11) * (1.0 / 9007199254740992.0); }
+
+// counters: draw 0 picks the first centre, draw 1 + r the centre of round r, draw
+// kSampleBase + j the j-th sampled cell
+constexpr uint64_t kSampleBase = 1ull << 40;
+constexpr int kSeedThreads = 1024;
+
+// k-means++ over the sample.  S [m][d] (float64) receives the normalised sample rows,
+// D2 [m] the squared distance to the nearest chosen centre; Y [K][d] (float32) the
+// chosen centres.  Thread t owns the contiguous sample chunk [t c, (t + 1) c).
+__global__ void __launch_bounds__(kSeedThreads) k_km_seed(const float* __restrict__ X, int64_t n, int d, int K,
+                                                         int m, uint64_t seed, double* __restrict__ S,
+                                                         double* __restrict__ D2, float* __restrict__ Y) {
+  __shared__ double part[kSeedThreads];  // chunk sums, then their exclusive prefix
+  __shared__ double cen[128];
+  __shared__ int pick;
+  __shared__ double total;
+  const int t = threadIdx.x;
+  const int ch = (m + kSeedThreads - 1) / kSeedThreads;
+  const int j0 = min(m, t * ch), j1 = min(m, (t + 1) * ch);
+  // the sample rows, L2-normalised (inverse norm capped at 1e12, kernels_normalize.cuh:7-54)
+  for (int j = j0; j < j1; ++j) {
+    const int64_t cell = (int64_t)m == n ? j : (int64_t)(km_draw(seed, kSampleBase + (uint64_t)j) % (uint64_t)n);
+    const float* x = X + cell * d;
+    double ss = 0.0;
+    for (int c = 0; c < d; ++c) ss = __dadd_rn(ss, __dmul_rn((double)x[c], (double)x[c]));
+    double inv = __ddiv_rn(1.0, __dsqrt_rn(ss));
+    if (!(inv <= 1e12)) inv = 1e12;
+    for (int c = 0; c < d; ++c) S[(size_t)j * d + c] = __dmul_rn((double)x[c], inv);
+  }
+  if (t == 0) pick = (int)(km_draw(seed, 0) % (uint64_t)m);
+  __syncthreads();
+  for (int r = 0; r < K; ++r) {
+    // centre r = sample row `pick`
+    for (int c = t; c < d; c += kSeedThreads) {
+      cen[c] = S[(size_t)pick * d + c];
+      Y[(size_t)r * d + c] = (float)cen[c];
+    }
+    __syncthreads();
+    if (r == K - 1) break;
+    // nearest-centre distances and the chunk sums (sequential, in sample order)
+    double local = 0.0;
+    for (int j = j0; j < j1; ++j) {
+      double acc = 0.0;
+      for (int c = 0; c < d; ++c) {
+        const double df = __dsub_rn(S[(size_t)j * d + c], cen[c]);
+        acc = __dadd_rn(acc, __dmul_rn(df, df));
+      }
+      const double v = r == 0 ? acc : fmin(D2[j], acc);
+      D2[j] = v;
+      local = __dadd_rn(local, v);
+    }
+    part[t] = local;
+    __syncthreads();
+    if (t == 0) {  // exclusive prefix over the chunks, in order
+      double run = 0.0;
+      for (int q = 0; q < kSeedThreads; ++q) {
+        const double v = part[q];
+        part[q] = run;
+        run = __dadd_rn(run, v);
+      }
+      total = run;
+      pick = -1;
+    }
+    __syncthreads();
+    const uint64_t h = km_draw(seed, 1 + (uint64_t)(r + 1));
+    if (!(total > 0.0)) {  // every sample sits on a chosen centre: a uniform pick
+      if (t == 0) pick = (int)(h % (uint64_t)m);
+    } else {
+      const double target = __dmul_rn(km_u01(h), total);
+      const double lo = part[t], hi = t + 1 < kSeedThreads ? part[t + 1] : total;
+      if (lo <= target && target < hi) {
+        double acc = lo;
+        int got = -1, last = -1;
+        for (int j = j0; j < j1; ++j) {
+          if (D2[j] > 0.0) last = j;
+          acc = __dadd_rn(acc, D2[j]);
+          if (target < acc) {
+            got = j;
+            break;
+          }
+        }
+        pick = got >= 0 ? got : last;  // rounding left the target past the chunk's last sum
+      }
+    }
+    __syncthreads();
+    if (t == 0 && pick < 0) {  // the product rounded up to the total: the last sample with weight
+      for (int j = m - 1; j >= 0 && pick < 0; --j)
+        if (D2[j] > 0.0) pick = j;
+      if (pick < 0) pick = 0;
+    }
+    __syncthreads();
+  }
+}
+
+
+// ---- Lloyd iterations ------------------------------------------------------------------
+// Shared memory of the assignment kernel: the 128-cell bf16 tile, the resident centres,
+// the half squared norms, per-row labels, and the CTA's centre sums and counts.
+struct KmLayout {
+  TcLayout t;  // similarity tile geometry (dpad, kblk, npad, tcols)
+  uint32_t offA, offB, offHn, offCnt, offLab, offBest, offRows, offMisc, offAcc, bytes;
+  int acc_smem;  // 1: the CTA's centre sums in shared memory; 0: in its slice of the partials
+};
+
+inline KmLayout km_layout(int d, int K) {
+  KmLayout L{};
+  L.t.dpad = d <= 64 ? 64 : 128;
+  L.t.kblk = L.t.dpad / 64;
+  L.t.npad = (K + 15) / 16 * 16;
+  L.t.tcols = L.t.npad <= 128 ? 128 : 256;
+  auto al = [](uint32_t x, uint32_t a) { return (x + a - 1) / a * a; };
+  uint32_t o = 0;
+  L.offA = o; o += (uint32_t)L.t.kblk * 16384u;
+  L.offB = o; o += (uint32_t)L.t.kblk * (uint32_t)L.t.npad * 128u;
+  L.offHn = al(o, 16); o = L.offHn + (uint32_t)L.t.npad * 4u;
+  L.offCnt = al(o, 16); o = L.offCnt + (uint32_t)L.t.npad * 4u;
+  L.offLab = al(o, 16); o = L.offLab + 128u * 4u;
+  L.offBest = o; o += 2u * 128u * 8u;  // value and index per (half, row)
+  L.offRows = o; o += 2u * 128u * 4u;  // cell id and (unused) batch per row
+  L.offMisc = al(o, 16); o = L.offMisc + 64u;
+  L.offAcc = al(o, 16);
+  const uint32_t acc = (uint32_t)K * (uint32_t)d * 4u;
+  L.acc_smem = L.offAcc + acc + 1024u <= 220u * 1024u;
+  if (L.acc_smem) o = L.offAcc + acc;
+  L.bytes = o + 1024u;  // slack for the 1024-byte alignment of the base
+  return L;
+}
+
+// One Lloyd assignment pass: label = argmax_k (z . y_k - hn_k) of every cell (lowest k on
+// ties), and the CTA's sums P[cta][k][:] of its cells' bf16 rows and counts C[cta][k].
+template <typename H>
+__global__ void __launch_bounds__(256, 1) k_km_assign(const H* __restrict__ Zh, int ldz, const H* __restrict__ Yh,
+                                                      int ldy, const float* __restrict__ hn, int64_t n, int K, int d,
+                                                      KmLayout KL, float* __restrict__ P, float* __restrict__ C,
+                                                      int* err) {
+  extern __shared__ __align__(1024) unsigned char smem_dyn[];
+  unsigned char* sm = (unsigned char*)(((uintptr_t)smem_dyn + 1023) & ~(uintptr_t)1023);
+  const TcLayout& L = KL.t;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  float* hns = (float*)(sm + KL.offHn);
+  float* cnt = (float*)(sm + KL.offCnt);
+  int* lab = (int*)(sm + KL.offLab);
+  float* bestv = (float*)(sm + KL.offBest);  // [2][128]
+  int* besti = (int*)(bestv + 256);          // [2][128]
+  int* cid = (int*)(sm + KL.offRows);
+  int* ccat = cid + 128;
+  uint64_t* mbar = (uint64_t*)(sm + KL.offMisc);
+  uint32_t* tmem_slot = (uint32_t*)(sm + KL.offMisc + 8);
+  float* acc = KL.acc_smem ? (float*)(sm + KL.offAcc) : P + (size_t)blockIdx.x * K * d;
+  const unsigned char* smA = sm + KL.offA;
+  const uint32_t sA = tc::smem_u32(smA), sB = tc::smem_u32(sm + KL.offB);
+  if (warp == 0) {
+    tc::tmem_alloc(tmem_slot, (uint32_t)L.tcols);
+    tc::tmem_relinquish();
+    tc::fence_before_sync();
+  }
+  if (tid == 0) {
+    tc::mbar_init(mbar, 1);
+    tc::fence_mbar_init();
+  }
+  load_centroids_swizzled(Yh, ldy, K, sB, L);
+  for (int k = tid; k < L.npad; k += 256) hns[k] = k < K ? hn[k] : 0.f;
+  for (int e = tid; e < K * d; e += 256) acc[e] = 0.f;
+  for (int k = tid; k < K; k += 256) cnt[k] = 0.f;
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *tmem_slot;
+  const int64_t ntiles = (n + 127) / 128;
+  const uint32_t idesc = tc::idesc_f16(128, L.npad, is_bf16<H>::value, false, false);
+  const int half = warp >> 2, row = (warp & 3) * 32 + lane;
+  const int nh = (L.npad / 2 + 7) / 8 * 8;
+  const int c_lo = half * nh, c_hi = min(L.npad, c_lo + nh);
+  const uint32_t tl = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+  uint32_t phase = 0;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    __syncthreads();  // the previous tile's rows have been added
+    gather_rows_swizzled(Zh, ldz, nullptr, 0, n, tile, sA, L, cid, ccat, nullptr);
+    tc::cp_async_wait_all();
+    tc::fence_proxy_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) issue_similarity_mma(tmem, sA, sB, L, idesc, mbar);
+    if (!tc::mbar_wait(mbar, phase, kMaxPolls)) atomicExch(err, 9);
+    phase ^= 1u;
+    tc::fence_after_sync();
+    float best = -INFINITY;
+    int bi = 0;
+    for (int c = c_lo; c < c_hi; c += 8) {
+      float v[8];
+      tc::tmem_ld8(tl + (uint32_t)c, v);
+      tc::tmem_ld_wait();
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int k = c + i;
+        if (k < K) {
+          const float s = v[i] - hns[k];
+          if (s > best) {
+            best = s;
+            bi = k;
+          }
+        }
+      }
+    }
+    bestv[half * 128 + row] = best;
+    besti[half * 128 + row] = bi;
+    tc::fence_before_sync();
+    __syncthreads();
+    if (tid < 128) lab[tid] = bestv[128 + tid] > bestv[tid] ? besti[128 + tid] : besti[tid];
+    __syncthreads();
+    const int nvalid = (int)(n - tile * 128 < 128 ? n - tile * 128 : 128);
+    for (int e = tid; e < nvalid * d; e += 256) {
+      const int r = e / d, c = e - r * d;
+      const H z = *(const H*)(smA + (uint32_t)(c >> 6) * 16384u + tc::sw128_off((uint32_t)r, (uint32_t)((c >> 3) & 7)) +
+                              (uint32_t)(c & 7) * 2u);
+      atomicAdd(&acc[lab[r] * d + c], h2f(z));
+    }
+    if (tid < nvalid) atomicAdd(&cnt[lab[tid]], 1.f);
+  }
+  __syncthreads();
+  if (KL.acc_smem)
+    for (int e = tid; e < K * d; e += 256) P[(size_t)blockIdx.x * K * d + e] = acc[e];
+  for (int k = tid; k < K; k += 256) C[(size_t)blockIdx.x * K + k] = cnt[k];
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after_sync();
+    tc::tmem_dealloc(tmem, (uint32_t)L.tcols);
+  }
+}
+
+// New centre k = blockIdx.x: the mean of its cells over the G CTA partials (float64),
+// or the old centre when it has none; writes the float32 centre, its bf16 copy (zero
+// padded to ldy), hn_k = |bf16 centre|^2 / 2, and adds |shift|^2 and |new|^2 to shift[0..1].
+// With G = 0 it only derives the bf16 copy and hn from the current centres.
+template <typename H>
+__global__ void __launch_bounds__(256) k_km_update(const float* __restrict__ P, const float* __restrict__ C, int G,
+                                                   int K, int d, float* __restrict__ Yf, H* __restrict__ Yh, int ldy,
+                                                   float* __restrict__ hn, double* __restrict__ shift) {
+  __shared__ double part[8][128];
+  __shared__ double cpart[8];
+  __shared__ double red[32];
+  const int lane = threadIdx.x, y = threadIdx.y, t = y * 32 + lane;
+  const int k = blockIdx.x;
+  for (int c = lane; c < d; c += 32) {  // d <= 128
+    double s = 0.0;
+#pragma unroll 8
+    for (int g = y; g < G; g += 8) s += (double)__ldg(P + ((size_t)g * K + k) * d + c);
+    part[y][c] = s;
+  }
+  if (lane == 0) {
+    double cn = 0.0;
+    for (int g = y; g < G; g += 8) cn += (double)__ldg(C + (size_t)g * K + k);
+    cpart[y] = cn;
+  }
+  __syncthreads();
+  double count = 0.0;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) count += cpart[q];
+  double dsh = 0.0, nrm = 0.0, hsq = 0.0;
+  if (t < d) {
+    double s = 0.0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) s += part[q][t];
+    const double yold = (double)Yf[(size_t)k * d + t];
+    const float yf = count > 0.0 ? (float)(s / count) : (float)yold;
+    const H yh = from_f<H>(yf);
+    dsh = ((double)yf - yold) * ((double)yf - yold);
+    nrm = (double)yf * (double)yf;
+    hsq = (double)h2f(yh) * (double)h2f(yh);
+    Yf[(size_t)k * d + t] = yf;
+    Yh[(size_t)k * ldy + t] = yh;
+  } else if (t < ldy) {
+    Yh[(size_t)k * ldy + t] = from_f<H>(0.f);
+  }
+  dsh = block_sum(dsh, red);
+  nrm = block_sum(nrm, red);
+  hsq = block_sum(hsq, red);
+  if (t == 0) {
+    hn[k] = (float)(0.5 * hsq);
+    atomicAdd(&shift[0], dsh);
+    atomicAdd(&shift[1], nrm);
+  }
+}
+
+}  // namespace hb
+
+namespace hb {
+namespace {
+
+using Bf = __nv_bfloat16;
+
+// sample of the k-means++ seeding: every cell up to 64 K cells, at most 16384
+int64_t km_sample_size(int64_t n, int K) { return std::min<int64_t>(n, std::min<int64_t>(64LL * K, 16384)); }
+
+struct KmWork {
+  Bf* Zh;        // [n][ldz] bf16 L2-normalised rows
+  double* S;     // [m][d] seeding sample
+  double* D2;    // [m]
+  float* Yf;     // [K][d] centres
+  Bf* Yh;        // [K][ldy] bf16 centres
+  float* hn;     // [K] half squared norms of the bf16 centres
+  float* P;      // [G][K][d] per-CTA centre sums
+  float* C;      // [G][K] per-CTA counts
+  double* shift; // [2] |Y_new - Y_old|^2, |Y_new|^2
+  int* err;
+};
+
+size_t km_carve(Carver& cv, int64_t n, int d, int K, int G, KmWork& w) {
+  const int ld = (int)align_up((size_t)d, 8);
+  const int64_t m = km_sample_size(n, K);
+  w.Zh = cv.take<Bf>((size_t)n * ld);
+  w.S = cv.take<double>((size_t)m * d);
+  w.D2 = cv.take<double>((size_t)m);
+  w.Yf = cv.take<float>((size_t)K * d);
+  w.Yh = cv.take<Bf>((size_t)K * ld);
+  w.hn = cv.take<float>((size_t)K);
+  w.P = cv.take<float>((size_t)G * K * d);
+  w.C = cv.take<float>((size_t)G * K);
+  w.shift = cv.take<double>(2);
+  w.err = cv.take<int>(1);
+  return cv.off + 256;  // room to align the caller's base
+}
+
+}  // namespace
+}  // namespace hb
+
+using namespace hb;
+
+extern "C" {
+
+HB_API size_t hb_kmeans_workspace_bytes(int64_t n, int32_t n_pcs, int32_t n_clusters) {
+  if (n < 1 || n_pcs < 1 || n_clusters < 1) return 0;
+  Carver cv(nullptr, 0);
+  KmWork w;
+  return km_carve(cv, n, n_pcs, n_clusters, num_sms(), w);
+}
+
+HB_API int hb_kmeans_init(const float* X, int64_t n, int32_t n_pcs, int32_t n_clusters, int32_t max_iter,
+                          double tol, uint64_t seed, float* Y_out, int32_t* n_iter_out, void* workspace,
+                          size_t workspace_bytes, void* stream) {
+  const int d = n_pcs, K = n_clusters;
+  if (!X || !Y_out || !workspace || n < 1 || d < 1 || K < 1 || K > n || max_iter < 0 || !(tol >= 0.0)) {
+    set_error("hb_kmeans_init: bad argument");
+    return HB_ERR_INVALID;
+  }
+  if (d > 128 || K > 256) {
+    set_error("hb_kmeans_init: n_pcs=%d (at most 128) or n_clusters=%d (at most 256) out of range", d, K);
+    return HB_ERR_UNSUPPORTED;
+  }
+  const int G = num_sms();
+  if (workspace_bytes < hb_kmeans_workspace_bytes(n, d, K)) {
+    set_error("hb_kmeans_init: workspace too small");
+    return HB_ERR_WORKSPACE;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  Carver cv((void*)align_up((size_t)workspace, 256), workspace_bytes - 256);
+  KmWork w;
+  km_carve(cv, n, d, K, G, w);
+  const int ld = (int)align_up((size_t)d, 8);
+  const int m = (int)km_sample_size(n, K);
+  const KmLayout KL = km_layout(d, K);
+  PinnedLease host(4 * sizeof(double));
+  if (!host.ptr) {
+    set_error("hb_kmeans_init: cudaMallocHost failed");
+    return HB_ERR_CUDA;
+  }
+  double* h_shift = (double*)host.ptr;
+  int* h_err = (int*)(h_shift + 2);
+
+  HB_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
+  HB_TRY(launch_l2_normalize<float, Bf>(X, n, d, d, w.Zh, ld, st));
+  k_km_seed<<<1, kSeedThreads, 0, st>>>(X, n, d, K, m, seed, w.S, w.D2, w.Yf);
+  HB_LAUNCH_CHECK();
+  HB_CUDA(cudaMemsetAsync(w.shift, 0, 2 * sizeof(double), st));
+  k_km_update<Bf><<<K, dim3(32, 8), 0, st>>>(w.P, w.C, 0, K, d, w.Yf, w.Yh, ld, w.hn, w.shift);
+  HB_LAUNCH_CHECK();
+  const void* fn = (const void*)k_km_assign<Bf>;
+  HB_TRY(allow_max_dyn_smem(fn));
+  int iters = 0;
+  for (int it = 0; it < max_iter; ++it) {
+    HB_CUDA(cudaMemsetAsync(w.shift, 0, 2 * sizeof(double), st));
+    k_km_assign<Bf><<<G, 256, KL.bytes, st>>>(w.Zh, ld, w.Yh, ld, w.hn, n, K, d, KL, w.P, w.C, w.err);
+    HB_LAUNCH_CHECK();
+    k_km_update<Bf><<<K, dim3(32, 8), 0, st>>>(w.P, w.C, G, K, d, w.Yf, w.Yh, ld, w.hn, w.shift);
+    HB_LAUNCH_CHECK();
+    HB_CUDA(cudaMemcpyAsync(h_shift, w.shift, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    HB_CUDA(cudaStreamSynchronize(st));
+    ++iters;
+    if (h_shift[0] <= tol * tol * h_shift[1]) break;
+  }
+  HB_CUDA(cudaMemcpyAsync(Y_out, w.Yf, sizeof(float) * (size_t)K * d, cudaMemcpyDeviceToDevice, st));
+  HB_CUDA(cudaMemcpyAsync(h_err, w.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  HB_CUDA(cudaStreamSynchronize(st));
+  if (*h_err) {
+    set_error("hb_kmeans_init: tensor-core wait timed out (code %d)", *h_err);
+    return HB_ERR_TIMEOUT;
+  }
+  if (n_iter_out) *n_iter_out = iters;
+  return HB_OK;
+}
+
+}  // extern "C"

@@ -218,12 +218,39 @@ def default_n_clusters(n_cells: int) -> int:
 
 
 def seeded_centroids(Z: torch.Tensor, n_clusters: int, random_state: int) -> torch.Tensor:
-    """Initial centroids when none are given: ``n_clusters`` distinct cells chosen by
-    ``numpy.random.default_rng(random_state)``.  (The reference runs cuML k-means||,
-    a third-party library, here; pass ``init_centroids`` to reproduce a given start.)"""
+    """``n_clusters`` distinct cells chosen by ``numpy.random.default_rng(random_state)``:
+    the initial centroids when the k-means initialisation does not apply (more than 128
+    PCs or more than 256 clusters)."""
     rng = np.random.default_rng(random_state)
     idx = rng.choice(Z.shape[0], size=n_clusters, replace=False)
     return Z[torch.as_tensor(idx, device=Z.device)].contiguous()
+
+
+KMEANS_MAX_ITER = 25   # the reference's KMeans(max_iter=25) (_harmony/__init__.py:315-321)
+KMEANS_TOL = 1e-4
+
+
+def kmeans_centroids(X: torch.Tensor, n_clusters: int, random_state: int, *, max_iter: int = KMEANS_MAX_ITER,
+                     tol: float = KMEANS_TOL, return_iters: bool = False):
+    """Initial centroids by the engine's seeded k-means on the L2-normalised rows of ``X``
+    (``hb_kmeans_init``): k-means++ seeding on a sample drawn from ``random_state``, then up
+    to ``max_iter`` Lloyd iterations with tensor-core assignment.  This takes the place of
+    the reference's cuML ``KMeans(init="k-means||", n_init=1, max_iter=25)``
+    (_harmony/__init__.py:290-323); the centres are returned unnormalised, as cuML's are,
+    in the dtype of ``X``."""
+    lib = _lib.load()
+    X32 = X.to(torch.float32).contiguous()
+    n, d = X32.shape
+    ws_bytes = lib.hb_kmeans_workspace_bytes(n, d, n_clusters)
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device=X.device)
+    Y = torch.empty((n_clusters, d), dtype=torch.float32, device=X.device)
+    iters = ctypes.c_int32(0)
+    st = torch.cuda.current_stream(X.device).cuda_stream
+    _lib.check(lib.hb_kmeans_init(X32.data_ptr(), n, d, n_clusters, int(max_iter), float(tol),
+                                  int(random_state) & 0xFFFFFFFFFFFFFFFF, Y.data_ptr(), ctypes.byref(iters),
+                                  ws.data_ptr(), ws_bytes, st))
+    Y = Y.to(X.dtype)
+    return (Y, iters.value) if return_iters else Y
 
 
 def _resolve_precision(precision, dtype) -> str:
@@ -334,7 +361,10 @@ def harmonize(
     X = X.to(torch.float64 if prec == "fp64" else torch.float32).contiguous()
 
     if init_centroids is None:
-        Y0 = seeded_centroids(X, n_clusters, random_state)
+        if n_pcs <= 128 and n_clusters <= 256:
+            Y0 = kmeans_centroids(X, n_clusters, random_state)
+        else:
+            Y0 = seeded_centroids(X, n_clusters, random_state)
     else:
         Y0 = torch.as_tensor(init_centroids, device=device)
         if tuple(Y0.shape) != (n_clusters, n_pcs):

@@ -82,6 +82,7 @@ template <typename H>
 __global__ void __launch_bounds__(256, 1) k_tc_centroid_stream(CenStreamArgs a, CsLayout L,
                                                                const __grid_constant__ CUtensorMap tmZ,
                                                                const __grid_constant__ CUtensorMap tmR) {
+  if (a.stop && *(volatile const int*)a.stop) return;  // the k-means loop has stopped on the device
   extern __shared__ __align__(1024) unsigned char smem_dyn[];
   unsigned char* sm = (unsigned char*)(((uintptr_t)smem_dyn + 1023) & ~(uintptr_t)1023);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -259,7 +260,8 @@ __global__ void __launch_bounds__(256, 1) k_tc_centroid_stream(CenStreamArgs a, 
 template <typename H>
 __global__ void __launch_bounds__(256) k_cs_reduce(const float* __restrict__ P, const float* __restrict__ Opart, int G,
                                                    int K, int d, int nkeys, H* __restrict__ Yn, int ldy,
-                                                   double* __restrict__ Omin) {
+                                                   double* __restrict__ Omin, const int* stop) {
+  if (stop && *(volatile const int*)stop) return;  // the k-means loop has stopped on the device
   __shared__ double part[8][128];
   __shared__ double red[32];
   const int lane = threadIdx.x, y = threadIdx.y, t = y * 32 + lane;
@@ -349,7 +351,7 @@ int launch_tc_centroid_stream(const CenStreamArgs& a, const void* Zn, int ldz, c
   HB_LAUNCH_CHECK();
   const int64_t ne = (int64_t)a.nkeys * a.K;
   k_cs_reduce<H><<<(unsigned)(a.K + (ne + 31) / 32), dim3(32, 8), 0, st>>>(a.P, a.Opart, grid, a.K, a.d, a.nkeys,
-                                                                        (H*)a.Yn, a.ldy, Omin);
+                                                                        (H*)a.Yn, a.ldy, Omin, a.stop);
   HB_LAUNCH_CHECK();
   return HB_OK;
 }

@@ -179,6 +179,7 @@ struct RunAcc {
 
 template <typename H>
 __global__ void __launch_bounds__(256, 1) k_tc_centroid(CenArgs a, CenLayout L) {
+  if (a.stop && *(volatile const int*)a.stop) return;  // the k-means loop has stopped on the device
   extern __shared__ __align__(1024) unsigned char smem_dyn[];
   unsigned char* sm = (unsigned char*)(((uintptr_t)smem_dyn + 1023) & ~(uintptr_t)1023);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;

@@ -128,6 +128,7 @@ struct Work {
   float* Opart;     // per-CTA per-key sums of the streaming centroid pass
   int32_t* cell_index;  // cells sorted by batch (stable), built when the caller passes none
   int* err;
+  int* stop;  // device-side k-means stop: iterations run, 0 while running
   AccumChunk* cen_chunks;
   AccumChunk* m_chunks;
   int32_t* batch_chunk_off;
@@ -161,6 +162,7 @@ void carve(const hb_plan& P, Carver& cv, Work& w) {
   w.ckey = P.cen_stream ? cv.take<int32_t>((size_t)kMaxIterChunk * n) : nullptr;
   w.Opart = P.cen_stream ? cv.take<float>((size_t)P.cen_chunks * P.nkeys * K) : nullptr;
   w.err = cv.take<int>(4);
+  w.stop = cv.take<int>(1);
   w.cen_chunks = cv.take<AccumChunk>(P.cen_chunks);
   w.m_chunks = cv.take<AccumChunk>(P.max_m_chunks);
   w.batch_chunk_off = cv.take<int32_t>(B + 1);
@@ -401,6 +403,8 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
   double* obj_init = w.obj_out + std::max(p.max_iter_clustering, 1);
   constexpr bool tc_path = !std::is_same<S, float>::value && !std::is_same<S, double>::value;
   // one persistent sweep (16-bit path) over `nblk` blocks of `idx`, objective into obj_dst
+  int* sweep_stop = nullptr;  // device-side k-means stop passed to the next sweep launch, with sweep_it
+  int sweep_it = 0;
   auto sweep = [&](const int32_t* idx, const int32_t* lcat, int64_t bs, int nb, const double* Omin, int init,
                    double* obj_dst) -> int {
     if constexpr (tc_path) {
@@ -412,6 +416,7 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
       sa.sigma = p.sigma; sa.d = d; sa.K = K; sa.B = B; sa.stabilized = p.stabilized_penalty;
       sa.init_mode = init; sa.batch_sorted = P->ml.nsub > 1 || B <= 1;
       sa.max_ctas = p.max_sweep_ctas; sa.barrier = w.barrier; sa.err = w.err;
+      sa.stop = sweep_stop; sa.it = sweep_it; sa.tol = p.tol_clustering;
       HB_CUDA(cudaMemsetAsync(w.barrier, 0, sizeof(unsigned), st));
       HB_TRY(launch_tc_sweep<S>(sa, st));
       ring.cur = (ring.cur + nb) % 3;
@@ -452,6 +457,10 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
   // With tol_clustering = -inf no iteration can stop early, so the per-iteration
   // objective read-back (a host sync) is deferred to the end of the clustering call.
   const bool early_stop = !(std::isinf(p.tol_clustering) && p.tol_clustering < 0);
+  // 16-bit path: the window-3 test runs on the device (CTA 0 of the sweep sets a stop flag
+  // that the later launches of the outer iteration check at entry); the host reads the flag
+  // once per chunk of block lists instead of syncing after every k-means iteration
+  const bool dev_stop = tc_path && early_stop;
 
   // optional device-time profile: event pairs around block-update and centroid launches
   hb_profile* prof = out ? out->profile : nullptr;
@@ -483,6 +492,10 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
     const uint32_t seed = (uint32_t)((p.random_state + (uint64_t)outer * 1000003ull) & 0xffffffffull);
     kobj.clear();
     bool stop = false;
+    const int ring0 = ring.cur;
+    int done = p.max_iter_clustering;  // k-means iterations run (set by the device stop)
+    if (dev_stop) HB_CUDA(cudaMemsetAsync(w.stop, 0, sizeof(int), st));
+    int* const dstop = dev_stop ? w.stop : nullptr;
     for (int it0 = 0; it0 < p.max_iter_clustering && !stop; it0 += kMaxIterChunk) {
       const int C = std::min(kMaxIterChunk, p.max_iter_clustering - it0);
       HB_TRY(membership_build_dev(ml, w.mb, nullptr, seed + (uint32_t)it0, C, cats, w.idx, st, w.lcat,
@@ -503,10 +516,11 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
         if constexpr (tc_path) {
           if (P->cen_stream) {
             CenStreamArgs ca{n, (int)((P->rows_alloc - 8) / 128), w.ckey + (size_t)c * n, d, K, P->nkeys,
-                             (float*)w.Ypart, w.Opart, w.err, Yn, P->ldy};
+                             (float*)w.Ypart, w.Opart, w.err, Yn, P->ldy, dstop};
             HB_TRY(launch_tc_centroid_stream<S>(ca, Zn, P->ldz, R, P->ldr, P->rows_alloc, P->cen_chunks, w.Omin, st));
           } else {
-            CenArgs ca{Zn, P->ldz, R, P->ldr, cats, idx, lcat, n, ml.bs, d, K, B, (float*)w.Ypart, w.Omin, w.err};
+            CenArgs ca{Zn, P->ldz, R, P->ldr, cats, idx, lcat, n, ml.bs, d, K, B, (float*)w.Ypart, w.Omin, w.err,
+                       dstop};
             HB_TRY(launch_tc_centroid<S>(ca, P->cen_chunks, st));
           }
         } else {
@@ -515,12 +529,16 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
         }
         bool reduced = false;  // the cell-order pass reduces its partials itself
         if constexpr (tc_path) reduced = P->cen_stream;
-        if (!reduced) HB_TRY(launch_centroid_reduce<TA, S>((TA*)w.Ypart, P->cen_chunks, K, d, Yn, P->ldy, st));
+        if (!reduced)
+          HB_TRY(launch_centroid_reduce<TA, S>((TA*)w.Ypart, P->cen_chunks, K, d, Yn, P->ldy, st, dstop));
         span_end(sp);
         // sweep the blocks (clustering.cu:308-372)
         if constexpr (tc_path) {
           sp = span_begin(0, (double)n * (zb + rb + 8));
+          sweep_stop = dstop;
+          sweep_it = it;
           HB_TRY(sweep(idx, lcat, ml.bs, nblk, w.Omin, 0, w.obj_out + it));
+          sweep_stop = nullptr;
           span_end(sp);
         } else {
         for (int j = 0; j < nblk; ++j) {
@@ -537,7 +555,7 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
         HB_TRY(launch_objective_finalize(ring.state(), w.Pr, w.theta, p.sigma, B, K,
                                          p.stabilized_penalty, w.obj_acc, w.obj_out + it, st));
         }
-        if (early_stop) {
+        if (early_stop && !dev_stop) {
           HB_CUDA(cudaMemcpyAsync(h_dbl, w.obj_out + it, sizeof(double), cudaMemcpyDeviceToHost, st));
           HB_CUDA(cudaStreamSynchronize(st));
           h_obj = h_dbl[0];
@@ -551,17 +569,29 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
           }
         }
       }
+      if (dev_stop) {
+        HB_CUDA(cudaMemcpyAsync(h_err + 3, w.stop, sizeof(int), cudaMemcpyDeviceToHost, st));
+        HB_CUDA(cudaStreamSynchronize(st));
+        if (h_err[3] > 0) {
+          done = h_err[3];
+          stop = true;
+        }
+      }
     }
-    const bool read_kobj = !early_stop && p.max_iter_clustering > 0;
+    // the launches after the device stop returned at once: the state buffer advanced only
+    // through the iterations that ran
+    if (dev_stop) ring.cur = (int)((ring0 + (int64_t)done * nblk) % 3);
+    const int n_kobj = !early_stop ? p.max_iter_clustering : (dev_stop ? done : 0);
+    const bool read_kobj = n_kobj > 0;
     if (read_kobj)
-      HB_CUDA(cudaMemcpyAsync(h_dbl + 1, w.obj_out, sizeof(double) * p.max_iter_clustering,
+      HB_CUDA(cudaMemcpyAsync(h_dbl + 1, w.obj_out, sizeof(double) * n_kobj,
                               cudaMemcpyDeviceToHost, st));
     {
       int* err = h_err;
       HB_CUDA(cudaMemcpyAsync(&err[0], w.mb.err, sizeof(int), cudaMemcpyDeviceToHost, st));
       HB_CUDA(cudaMemcpyAsync(&err[1], w.err, sizeof(int), cudaMemcpyDeviceToHost, st));
       HB_CUDA(cudaStreamSynchronize(st));
-      if (read_kobj) kobj.assign(h_dbl + 1, h_dbl + 1 + p.max_iter_clustering);
+      if (read_kobj) kobj.assign(h_dbl + 1, h_dbl + 1 + n_kobj);
       if (err[0]) { set_error("block splitter candidate buffer overflow"); return HB_ERR_INTERNAL; }
       if (err[1] == 7) { set_error("fp16 correction: |X| or |W| reaches 65504, outside the fp16 range; use bf16"); return HB_ERR_UNSUPPORTED; }
       if (err[1]) { set_error("tensor-core wait timed out (code %d)", err[1]); return HB_ERR_TIMEOUT; }

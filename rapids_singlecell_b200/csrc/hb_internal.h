@@ -77,7 +77,7 @@ int launch_accum(const TS* W, int ldw, const TV* V, int ldv, const int32_t* cell
 // Y_norm[k] = l2norm(sum_chunks P[chunk][k]); optional 16-bit copy.
 template <typename TA, typename TY>
 int launch_centroid_reduce(const TA* P, int n_chunks, int K, int d, TY* Yn, int ldy,
-                           cudaStream_t st);
+                           cudaStream_t st, const int* stop = nullptr);
 
 struct BlockArgs {
   const void* Zn;
@@ -149,6 +149,11 @@ struct SweepArgs {
   int max_ctas;            // 0: one CTA per SM; otherwise at most this many CTAs
   unsigned* barrier;       // zero on entry
   int* err;
+  // device-side k-means stop (nullptr: none): the launch returns at once when *stop is set;
+  // otherwise CTA 0 applies the window-3 test to obj_out[-it .. 0] and sets *stop = it + 1
+  int* stop;
+  int it;
+  double tol;
 };
 
 template <typename H>
@@ -167,6 +172,7 @@ struct CenArgs {
   float* P;             // [G][K][d] partial sums
   double* Omin;         // [nblk][B+1][K]
   int* err;
+  const int* stop;      // nullptr, or the device-side k-means stop: return at once when set
 };
 
 template <typename H>
@@ -184,6 +190,7 @@ struct CenStreamArgs {
   int* err;
   void* Yn;              // [K][ldy] 16-bit normalised centroids (written by the reduction)
   int ldy;
+  const int* stop;       // nullptr, or the device-side k-means stop: return at once when set
 };
 bool cs_supported(int d, int K, int nkeys, int ldz);
 int make_tile_map4(CUtensorMap* tm, const void* base, int64_t rows, int ld, int blocks, bool bf16);

@@ -231,7 +231,8 @@ __device__ __forceinline__ void reduce_rows_into(const TA* __restrict__ P, int q
 
 template <typename TA, typename TY>
 __global__ void k_centroid_reduce(const TA* __restrict__ P, int n_chunks, int K, int d,
-                                  TY* __restrict__ Yn, int ldy) {
+                                  TY* __restrict__ Yn, int ldy, const int* stop) {
+  if (stop && *(volatile const int*)stop) return;  // the k-means loop has stopped on the device
   extern __shared__ double sm[];
   double* part = sm;              // [RED_Y][d]
   double* ys = sm + RED_Y * d;    // [d]
@@ -249,15 +250,17 @@ __global__ void k_centroid_reduce(const TA* __restrict__ P, int n_chunks, int K,
 }
 
 template <typename TA, typename TY>
-int launch_centroid_reduce(const TA* P, int n_chunks, int K, int d, TY* Yn, int ldy, cudaStream_t st) {
-  k_centroid_reduce<TA, TY><<<K, dim3(32, RED_Y), sizeof(double) * (RED_Y + 1) * d, st>>>(P, n_chunks, K, d, Yn, ldy);
+int launch_centroid_reduce(const TA* P, int n_chunks, int K, int d, TY* Yn, int ldy, cudaStream_t st,
+                           const int* stop) {
+  k_centroid_reduce<TA, TY><<<K, dim3(32, RED_Y), sizeof(double) * (RED_Y + 1) * d, st>>>(P, n_chunks, K, d, Yn,
+                                                                                        ldy, stop);
   HB_LAUNCH_CHECK();
   return HB_OK;
 }
-template int launch_centroid_reduce<float, float>(const float*, int, int, int, float*, int, cudaStream_t);
-template int launch_centroid_reduce<double, double>(const double*, int, int, int, double*, int, cudaStream_t);
-template int launch_centroid_reduce<float, __half>(const float*, int, int, int, __half*, int, cudaStream_t);
-template int launch_centroid_reduce<float, __nv_bfloat16>(const float*, int, int, int, __nv_bfloat16*, int, cudaStream_t);
+template int launch_centroid_reduce<float, float>(const float*, int, int, int, float*, int, cudaStream_t, const int*);
+template int launch_centroid_reduce<double, double>(const double*, int, int, int, double*, int, cudaStream_t, const int*);
+template int launch_centroid_reduce<float, __half>(const float*, int, int, int, __half*, int, cudaStream_t, const int*);
+template int launch_centroid_reduce<float, __nv_bfloat16>(const float*, int, int, int, __nv_bfloat16*, int, cudaStream_t, const int*);
 
 // ---------------------------------------------------------------------------
 // Fused block update (plain path).

@@ -216,6 +216,8 @@ __device__ __forceinline__ void tile_runs(const int* cc, int nvalid, int* runs, 
 
 template <typename H, int NG>
 __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayout SL) {
+  // the k-means loop has stopped on the device (set by an earlier launch: every CTA sees it)
+  if (a.stop && *(volatile const int*)a.stop) return;
   constexpr int NT = 256 * NG;
   extern __shared__ __align__(1024) unsigned char smem_dyn[];
   unsigned char* sm = (unsigned char*)(((uintptr_t)smem_dyn + 1023) & ~(uintptr_t)1023);
@@ -555,8 +557,17 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
     }
     acc = block_sum(acc, red);
     if (tid == 0) {
-      *a.obj_out = *a.obj_acc + a.sigma * acc;
+      const double obj = *a.obj_acc + a.sigma * acc;
+      *a.obj_out = obj;
       *a.obj_acc = 0.0;
+      // window-3 convergence over this outer iteration's objectives (clustering.cu:380-387),
+      // the same expressions as the host test
+      if (a.stop && a.it >= 3) {
+        const double* h = a.obj_out - a.it;
+        const double o = h[a.it - 1] + h[a.it - 2] + h[a.it - 3];
+        const double nw = obj + h[a.it - 1] + h[a.it - 2];
+        if ((o - nw) < a.tol * fabs(o)) *a.stop = a.it + 1;
+      }
     }
   }
   tc::bulk_wait_all();

@@ -126,3 +126,38 @@ def test_bf16_wide_shapes_vs_plain_fp32():
           f"{info.objectives_harmony} vs {ref_info.objectives_harmony}")
     np.testing.assert_allclose(info.objectives_harmony, ref_info.objectives_harmony, rtol=5e-3)
     assert err < 5e-3
+
+
+def _window_stop(objs, tol):
+    """First k-means iteration count at which the reference's window-3 test holds
+    (clustering.cu:380-387), or None."""
+    for m in range(4, len(objs) + 1):
+        o = objs[m - 2] + objs[m - 3] + objs[m - 4]
+        nw = objs[m - 1] + objs[m - 2] + objs[m - 3]
+        if (o - nw) < tol * abs(o):
+            return m
+    return None
+
+
+def test_device_kmeans_stop_follows_the_window_rule():
+    """With a finite tol_clustering the 16-bit path decides the k-means stop on the device
+    (launches after it return at once); each outer iteration must stop exactly where the
+    window-3 test first holds on its objectives, and the result must match the plain fp32
+    path, which decides on the host."""
+    cfg = make_config("C2", seed=8, n_cells=120_000)
+    tol = 1e-3
+    kw = dict(n_clusters=100, max_iter_harmony=3, max_iter_clustering=20, tol_harmony=-np.inf,
+              tol_clustering=tol)
+    labels = pd.Categorical.from_codes(cfg["cats"], categories=[f"b{i}" for i in range(cfg["n_batches"])])
+    Z = torch.as_tensor(cfg["Z"], device="cuda")
+    out, info = harmonize(Z, labels, None, init_centroids=cfg["Y0"], precision="bf16", return_info=True, **kw)
+    ref, ref_info = harmonize(Z, labels, None, init_centroids=cfg["Y0"], precision="fp32", return_info=True, **kw)
+    its = [len(k) for k in info.kmeans_objectives]
+    print(f"k-means iterations bf16 {its}, fp32 {[len(k) for k in ref_info.kmeans_objectives]}")
+    for outer, objs in enumerate(info.kmeans_objectives):
+        m = _window_stop(objs, tol)
+        assert m == len(objs) or (m is None and len(objs) == kw["max_iter_clustering"])
+        assert info.objectives_harmony[outer + 1] == objs[-1]
+    assert its == [len(k) for k in ref_info.kmeans_objectives]
+    assert min(its) < kw["max_iter_clustering"]  # the stop was exercised
+    assert rel_maxabs(out.cpu().numpy(), ref.cpu().numpy()) < 5e-3

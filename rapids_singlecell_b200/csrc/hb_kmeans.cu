@@ -10,9 +10,10 @@
 //            with probability proportional to the squared distance to the
 //            nearest centre chosen so far) over a sample of m cells (all cells
 //            when n <= m, else m draws with replacement), in float64 with
-//            explicitly rounded operations and sequential sums, on one CTA; the
-//            draws come from splitmix64 (Steele, Lea & Flood, 2014) of (seed,
-//            counter), so a seed fixes the result bit for bit;
+//            explicitly rounded operations in a fixed order (one thread per sample
+//            for the distances, one CTA for each draw); the draws come from
+//            splitmix64 (Steele, Lea & Flood, 2014) of (seed, counter), so a seed
+//            fixes the result bit for bit;
 //   Lloyd    up to max_iter iterations over all cells: the assignment is the
 //            tensor-core similarity of a 128-cell tile of bf16 Z_norm against the
 //            bf16 centres (fp32 in TMEM), argmax_k (z.y_k - |y_k|^2 / 2), which is
@@ -43,51 +44,59 @@ __host__ __device__ __forceinline__ double km_u01(uint64_t h) { return (double)(
 constexpr uint64_t kSampleBase = 1ull << 40;
 constexpr int kSeedThreads = 1024;
 
-// k-means++ over the sample.  S [m][d] (float64) receives the normalised sample rows,
-// D2 [m] the squared distance to the nearest chosen centre; Y [K][d] (float32) the
-// chosen centres.  Thread t owns the contiguous sample chunk [t c, (t + 1) c).
-__global__ void __launch_bounds__(kSeedThreads) k_km_seed(const float* __restrict__ X, int64_t n, int d, int K,
-                                                         int m, uint64_t seed, double* __restrict__ S,
-                                                         double* __restrict__ D2, float* __restrict__ Y) {
-  __shared__ double part[kSeedThreads];  // chunk sums, then their exclusive prefix
-  __shared__ double cen[128];
-  __shared__ int pick;
-  __shared__ double total;
-  const int t = threadIdx.x;
-  const int ch = (m + kSeedThreads - 1) / kSeedThreads;
-  const int j0 = min(m, t * ch), j1 = min(m, (t + 1) * ch);
-  // the sample rows, L2-normalised (inverse norm capped at 1e12, kernels_normalize.cuh:7-54)
-  for (int j = j0; j < j1; ++j) {
-    const int64_t cell = (int64_t)m == n ? j : (int64_t)(km_draw(seed, kSampleBase + (uint64_t)j) % (uint64_t)n);
-    const float* x = X + cell * d;
-    double ss = 0.0;
-    for (int c = 0; c < d; ++c) ss = __dadd_rn(ss, __dmul_rn((double)x[c], (double)x[c]));
-    double inv = __ddiv_rn(1.0, __dsqrt_rn(ss));
-    if (!(inv <= 1e12)) inv = 1e12;
-    for (int c = 0; c < d; ++c) S[(size_t)j * d + c] = __dmul_rn((double)x[c], inv);
+// k-means++ over the sample, in three kernels with the sample rows column-major in S
+// [d][m] (float64), so that the per-sample loops of a warp read consecutive addresses.
+// The arithmetic is fixed for reproducibility: sums over columns in column order, the
+// 1024 chunks of ceil(m / 1024) consecutive samples each summed in order, then the chunk
+// sums in order.
+
+// S[:, j] = the L2-normalised row of sampled cell j (inverse norm capped at 1e12,
+// kernels_normalize.cuh:7-54); every cell in order when m == n.
+__global__ void __launch_bounds__(256) k_km_sample(const float* __restrict__ X, int64_t n, int d, int m,
+                                                  uint64_t seed, double* __restrict__ S) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  const int64_t cell = (int64_t)m == n ? j : (int64_t)(km_draw(seed, kSampleBase + (uint64_t)j) % (uint64_t)n);
+  const float* x = X + cell * d;
+  double ss = 0.0;
+  for (int c = 0; c < d; ++c) ss = __dadd_rn(ss, __dmul_rn((double)x[c], (double)x[c]));
+  double inv = __ddiv_rn(1.0, __dsqrt_rn(ss));
+  if (!(inv <= 1e12)) inv = 1e12;
+  for (int c = 0; c < d; ++c) S[(size_t)c * m + j] = __dmul_rn((double)x[c], inv);
+}
+
+// D2[j] = squared distance of sample j to the last chosen centre (sample *pick), or the
+// smaller of that and D2[j] after the first centre.
+__global__ void __launch_bounds__(256) k_km_dist(const double* __restrict__ S, int m, int d,
+                                                const int* __restrict__ pick, int first, double* __restrict__ D2) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  const int p = *pick;
+  double acc = 0.0;
+  for (int c = 0; c < d; ++c) {
+    const double df = __dsub_rn(S[(size_t)c * m + j], S[(size_t)c * m + p]);
+    acc = __dadd_rn(acc, __dmul_rn(df, df));
   }
-  if (t == 0) pick = (int)(km_draw(seed, 0) % (uint64_t)m);
-  __syncthreads();
-  for (int r = 0; r < K; ++r) {
-    // centre r = sample row `pick`
-    for (int c = t; c < d; c += kSeedThreads) {
-      cen[c] = S[(size_t)pick * d + c];
-      Y[(size_t)r * d + c] = (float)cen[c];
-    }
-    __syncthreads();
-    if (r == K - 1) break;
-    // nearest-centre distances and the chunk sums (sequential, in sample order)
+  D2[j] = first ? acc : fmin(D2[j], acc);
+}
+
+// Centre r: sample draw(seed, 0) % m for r = 0, else the sample at which the running sum
+// of D2 first exceeds u * total (u from draw(seed, 1 + r)); a uniform draw when every
+// sample sits on a chosen centre.  Writes *pick and Y[r] (float32).
+__global__ void __launch_bounds__(kSeedThreads) k_km_pick(const double* __restrict__ S, const double* __restrict__ D2,
+                                                         int m, int d, int r, uint64_t seed, int* __restrict__ pick,
+                                                         float* __restrict__ Y) {
+  __shared__ double part[kSeedThreads];  // chunk sums, then their exclusive prefix
+  __shared__ double total;
+  __shared__ int sel;
+  const int t = threadIdx.x;
+  if (r == 0) {
+    if (t == 0) sel = (int)(km_draw(seed, 0) % (uint64_t)m);
+  } else {
+    const int ch = (m + kSeedThreads - 1) / kSeedThreads;
+    const int j0 = min(m, t * ch), j1 = min(m, (t + 1) * ch);
     double local = 0.0;
-    for (int j = j0; j < j1; ++j) {
-      double acc = 0.0;
-      for (int c = 0; c < d; ++c) {
-        const double df = __dsub_rn(S[(size_t)j * d + c], cen[c]);
-        acc = __dadd_rn(acc, __dmul_rn(df, df));
-      }
-      const double v = r == 0 ? acc : fmin(D2[j], acc);
-      D2[j] = v;
-      local = __dadd_rn(local, v);
-    }
+    for (int j = j0; j < j1; ++j) local = __dadd_rn(local, D2[j]);
     part[t] = local;
     __syncthreads();
     if (t == 0) {  // exclusive prefix over the chunks, in order
@@ -98,12 +107,12 @@ __global__ void __launch_bounds__(kSeedThreads) k_km_seed(const float* __restric
         run = __dadd_rn(run, v);
       }
       total = run;
-      pick = -1;
+      sel = -1;
     }
     __syncthreads();
-    const uint64_t h = km_draw(seed, 1 + (uint64_t)(r + 1));
+    const uint64_t h = km_draw(seed, 1 + (uint64_t)r);
     if (!(total > 0.0)) {  // every sample sits on a chosen centre: a uniform pick
-      if (t == 0) pick = (int)(h % (uint64_t)m);
+      if (t == 0) sel = (int)(h % (uint64_t)m);
     } else {
       const double target = __dmul_rn(km_u01(h), total);
       const double lo = part[t], hi = t + 1 < kSeedThreads ? part[t + 1] : total;
@@ -118,27 +127,32 @@ __global__ void __launch_bounds__(kSeedThreads) k_km_seed(const float* __restric
             break;
           }
         }
-        pick = got >= 0 ? got : last;  // rounding left the target past the chunk's last sum
+        sel = got >= 0 ? got : last;  // rounding left the target past the chunk's last sum
       }
     }
     __syncthreads();
-    if (t == 0 && pick < 0) {  // the product rounded up to the total: the last sample with weight
-      for (int j = m - 1; j >= 0 && pick < 0; --j)
-        if (D2[j] > 0.0) pick = j;
-      if (pick < 0) pick = 0;
+    if (t == 0 && sel < 0) {  // the product rounded up to the total: the last sample with weight
+      for (int j = m - 1; j >= 0 && sel < 0; --j)
+        if (D2[j] > 0.0) sel = j;
+      if (sel < 0) sel = 0;
     }
-    __syncthreads();
   }
+  __syncthreads();
+  const int p = sel;
+  for (int c = t; c < d; c += kSeedThreads) Y[(size_t)r * d + c] = (float)S[(size_t)c * m + p];
+  if (t == 0) *pick = p;
 }
 
-
 // ---- Lloyd iterations ------------------------------------------------------------------
-// Shared memory of the assignment kernel: the 128-cell bf16 tile, the resident centres,
-// the half squared norms, per-row labels, and the CTA's centre sums and counts.
+// Shared memory of the assignment kernel: two 128-cell bf16 tiles (the next tile's rows
+// are gathered while the current one is assigned), the resident centres, the one-hot
+// operand of the tile's labels, the half squared norms, per-row choices and counts.
+// TMEM: the similarity tile (L.tcols columns) and the CTA's centre sums (npad columns).
 struct KmLayout {
-  TcLayout t;  // similarity tile geometry (dpad, kblk, npad, tcols)
-  uint32_t offA, offB, offHn, offCnt, offLab, offBest, offRows, offMisc, offAcc, bytes;
-  int acc_smem;  // 1: the CTA's centre sums in shared memory; 0: in its slice of the partials
+  TcLayout t;     // similarity tile geometry (dpad, kblk, npad, tcols)
+  int nbK;        // 64-cluster blocks of the one-hot operand
+  int tcols_all;  // TMEM columns allocated
+  uint32_t offA, offB, offH, offHn, offCnt, offBest, offRows, offMisc, bytes;
 };
 
 inline KmLayout km_layout(int d, int K) {
@@ -147,26 +161,28 @@ inline KmLayout km_layout(int d, int K) {
   L.t.kblk = L.t.dpad / 64;
   L.t.npad = (K + 15) / 16 * 16;
   L.t.tcols = L.t.npad <= 128 ? 128 : 256;
+  L.nbK = (L.t.npad + 63) / 64;
+  L.tcols_all = 2 * L.t.tcols;
   auto al = [](uint32_t x, uint32_t a) { return (x + a - 1) / a * a; };
   uint32_t o = 0;
-  L.offA = o; o += (uint32_t)L.t.kblk * 16384u;
+  L.offA = o; o += 2u * (uint32_t)L.t.kblk * 16384u;
   L.offB = o; o += (uint32_t)L.t.kblk * (uint32_t)L.t.npad * 128u;
+  L.offH = al(o, 1024); o = L.offH + (uint32_t)L.nbK * 16384u;
   L.offHn = al(o, 16); o = L.offHn + (uint32_t)L.t.npad * 4u;
   L.offCnt = al(o, 16); o = L.offCnt + (uint32_t)L.t.npad * 4u;
-  L.offLab = al(o, 16); o = L.offLab + 128u * 4u;
   L.offBest = o; o += 2u * 128u * 8u;  // value and index per (half, row)
-  L.offRows = o; o += 2u * 128u * 4u;  // cell id and (unused) batch per row
+  L.offRows = o; o += 4u * 128u * 4u;  // cell id and (unused) batch per row, per tile buffer
   L.offMisc = al(o, 16); o = L.offMisc + 64u;
-  L.offAcc = al(o, 16);
-  const uint32_t acc = (uint32_t)K * (uint32_t)d * 4u;
-  L.acc_smem = L.offAcc + acc + 1024u <= 220u * 1024u;
-  if (L.acc_smem) o = L.offAcc + acc;
   L.bytes = o + 1024u;  // slack for the 1024-byte alignment of the base
   return L;
 }
 
-// One Lloyd assignment pass: label = argmax_k (z . y_k - hn_k) of every cell (lowest k on
-// ties), and the CTA's sums P[cta][k][:] of its cells' bf16 rows and counts C[cta][k].
+// One Lloyd assignment pass over the CTA's tiles: label = argmax_k (z . y_k - hn_k) of every
+// cell (lowest k on ties); the CTA's sums P[cta][k][:] of its cells' bf16 rows and counts
+// C[cta][k].  The sums are a second MMA per tile, D[c][k] += sum_r Z[r][c] H[r][k] with H
+// the one-hot of the tile's labels, accumulated in TMEM: A = Z_tile^T is the gathered tile
+// read MN-major (64-value blocks 16 KB apart, 8-cell groups 1 KB apart); M = 128 always
+// (with 64 PCs the upper rows read the next buffer and are discarded).
 template <typename H>
 __global__ void __launch_bounds__(256, 1) k_km_assign(const H* __restrict__ Zh, int ldz, const H* __restrict__ Yh,
                                                       int ldy, const float* __restrict__ hn, int64_t n, int K, int d,
@@ -177,19 +193,19 @@ __global__ void __launch_bounds__(256, 1) k_km_assign(const H* __restrict__ Zh, 
   const TcLayout& L = KL.t;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   float* hns = (float*)(sm + KL.offHn);
-  float* cnt = (float*)(sm + KL.offCnt);
-  int* lab = (int*)(sm + KL.offLab);
+  int* cnt = (int*)(sm + KL.offCnt);
   float* bestv = (float*)(sm + KL.offBest);  // [2][128]
   int* besti = (int*)(bestv + 256);          // [2][128]
-  int* cid = (int*)(sm + KL.offRows);
-  int* ccat = cid + 128;
+  int* cid = (int*)(sm + KL.offRows);        // [2][128]
+  int* ccat = cid + 256;                     // [2][128]
   uint64_t* mbar = (uint64_t*)(sm + KL.offMisc);
   uint32_t* tmem_slot = (uint32_t*)(sm + KL.offMisc + 8);
-  float* acc = KL.acc_smem ? (float*)(sm + KL.offAcc) : P + (size_t)blockIdx.x * K * d;
-  const unsigned char* smA = sm + KL.offA;
-  const uint32_t sA = tc::smem_u32(smA), sB = tc::smem_u32(sm + KL.offB);
+  unsigned char* oh = sm + KL.offH;
+  const uint32_t atile = (uint32_t)L.kblk * 16384u;
+  const uint32_t sA0 = tc::smem_u32(sm + KL.offA), sB = tc::smem_u32(sm + KL.offB), sH = tc::smem_u32(oh);
+  const int nbK = KL.nbK;
   if (warp == 0) {
-    tc::tmem_alloc(tmem_slot, (uint32_t)L.tcols);
+    tc::tmem_alloc(tmem_slot, (uint32_t)KL.tcols_all);
     tc::tmem_relinquish();
     tc::fence_before_sync();
   }
@@ -198,30 +214,48 @@ __global__ void __launch_bounds__(256, 1) k_km_assign(const H* __restrict__ Zh, 
     tc::fence_mbar_init();
   }
   load_centroids_swizzled(Yh, ldy, K, sB, L);
-  for (int k = tid; k < L.npad; k += 256) hns[k] = k < K ? hn[k] : 0.f;
-  for (int e = tid; e < K * d; e += 256) acc[e] = 0.f;
-  for (int k = tid; k < K; k += 256) cnt[k] = 0.f;
+  for (int k = tid; k < L.npad; k += 256) {
+    hns[k] = k < K ? hn[k] : 0.f;
+    cnt[k] = 0;
+  }
+  for (uint32_t e = (uint32_t)tid * 16u; e < (uint32_t)nbK * 16384u; e += 256u * 16u)
+    *(uint4*)(oh + e) = make_uint4(0u, 0u, 0u, 0u);
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t tmem = *tmem_slot;
+  const uint32_t tacc = tmem + (uint32_t)L.tcols;  // centre sums: lane = PC, column = cluster
   const int64_t ntiles = (n + 127) / 128;
-  const uint32_t idesc = tc::idesc_f16(128, L.npad, is_bf16<H>::value, false, false);
+  const uint32_t idesc1 = tc::idesc_f16(128, L.npad, is_bf16<H>::value, false, false);
+  const uint32_t idesc2 = tc::idesc_f16(128, L.npad, is_bf16<H>::value, true, true);
   const int half = warp >> 2, row = (warp & 3) * 32 + lane;
   const int nh = (L.npad / 2 + 7) / 8 * 8;
   const int c_lo = half * nh, c_hi = min(L.npad, c_lo + nh);
   const uint32_t tl = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+  // one-hot element (cell r, cluster k): MN-major [8-cell group][64-cluster block][8 x 128 B]
+  auto oh_off = [&](int r, int k) -> uint32_t {
+    return (uint32_t)(r >> 3) * (uint32_t)nbK * 1024u + (uint32_t)(k >> 6) * 1024u + (uint32_t)(r & 7) * 128u +
+           ((((uint32_t)(k & 63) >> 3) ^ (uint32_t)(r & 7)) << 4) + (uint32_t)(k & 7) * 2u;
+  };
+  const H one = from_f<H>(1.f), zero = from_f<H>(0.f);
+  int old_lab = -1;  // the one-hot entry this thread's row set (threads < 128)
   uint32_t phase = 0;
-  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    __syncthreads();  // the previous tile's rows have been added
-    gather_rows_swizzled(Zh, ldz, nullptr, 0, n, tile, sA, L, cid, ccat, nullptr);
-    tc::cp_async_wait_all();
+  if ((int64_t)blockIdx.x < ntiles) gather_rows_swizzled(Zh, ldz, nullptr, 0, n, blockIdx.x, sA0, L, cid, ccat, nullptr);
+  int buf = 0, it = 0;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, buf ^= 1, ++it) {
+    tc::cp_async_wait_all();  // this tile's rows have landed
     tc::fence_proxy_async_smem();
     tc::fence_before_sync();
     __syncthreads();
-    if (tid == 0) issue_similarity_mma(tmem, sA, sB, L, idesc, mbar);
+    if (tid == 0) issue_similarity_mma(tmem, sA0 + (uint32_t)buf * atile, sB, L, idesc1, mbar);
     if (!tc::mbar_wait(mbar, phase, kMaxPolls)) atomicExch(err, 9);
     phase ^= 1u;
     tc::fence_after_sync();
+    // the commit also covers the previous tile's sum MMA: its tile buffer and the one-hot
+    // are free; the next tile's rows land while this one is assigned
+    const int64_t nxt = tile + gridDim.x;
+    if (nxt < ntiles)
+      gather_rows_swizzled(Zh, ldz, nullptr, 0, n, nxt, sA0 + (uint32_t)(buf ^ 1) * atile, L, cid + (buf ^ 1) * 128,
+                           ccat + (buf ^ 1) * 128, nullptr);
     float best = -INFINITY;
     int bi = 0;
     for (int c = c_lo; c < c_hi; c += 8) {
@@ -244,26 +278,56 @@ __global__ void __launch_bounds__(256, 1) k_km_assign(const H* __restrict__ Zh, 
     besti[half * 128 + row] = bi;
     tc::fence_before_sync();
     __syncthreads();
-    if (tid < 128) lab[tid] = bestv[128 + tid] > bestv[tid] ? besti[128 + tid] : besti[tid];
-    __syncthreads();
     const int nvalid = (int)(n - tile * 128 < 128 ? n - tile * 128 : 128);
-    for (int e = tid; e < nvalid * d; e += 256) {
-      const int r = e / d, c = e - r * d;
-      const H z = *(const H*)(smA + (uint32_t)(c >> 6) * 16384u + tc::sw128_off((uint32_t)r, (uint32_t)((c >> 3) & 7)) +
-                              (uint32_t)(c & 7) * 2u);
-      atomicAdd(&acc[lab[r] * d + c], h2f(z));
+    if (tid < 128) {  // this row's one-hot entry and count
+      if (old_lab >= 0) *(H*)(oh + oh_off(tid, old_lab)) = zero;
+      old_lab = -1;
+      if (tid < nvalid) {
+        const int l = bestv[128 + tid] > bestv[tid] ? besti[128 + tid] : besti[tid];
+        *(H*)(oh + oh_off(tid, l)) = one;
+        atomicAdd(&cnt[l], 1);
+        old_lab = l;
+      }
     }
-    if (tid < nvalid) atomicAdd(&cnt[lab[tid]], 1.f);
+    tc::fence_proxy_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after_sync();
+      const uint32_t sA = sA0 + (uint32_t)buf * atile;
+      for (int k = 0; k < 8; ++k) {  // 8 steps of 16 cells
+        const uint64_t ad = tc::sdesc_sw128(sA + (uint32_t)k * 2048u, 16384u, 1024u);
+        const uint64_t bd = tc::sdesc_sw128(sH + (uint32_t)k * 2u * (uint32_t)nbK * 1024u, 1024u, (uint32_t)nbK * 1024u);
+        tc::mma_f16(tacc, ad, bd, idesc2, (it > 0 || k > 0) ? 1u : 0u);
+      }
+    }
   }
-  __syncthreads();
-  if (KL.acc_smem)
-    for (int e = tid; e < K * d; e += 256) P[(size_t)blockIdx.x * K * d + e] = acc[e];
-  for (int k = tid; k < K; k += 256) C[(size_t)blockIdx.x * K + k] = cnt[k];
+  // the sums out of TMEM: warp w reads PCs 32 (w % 4) .. + 31, its half of the clusters
+  if (it > 0) {
+    if (tid == 0) tc::mma_commit(mbar);
+    if (!tc::mbar_wait(mbar, phase, kMaxPolls)) atomicExch(err, 9);
+    tc::fence_after_sync();
+  }
+  {
+    const int c = (warp & 3) * 32 + lane;
+    const uint32_t ta = tacc + ((uint32_t)((warp & 3) * 32) << 16);
+    float* out = P + (size_t)blockIdx.x * K * d;
+    for (int k0 = c_lo; k0 < c_hi; k0 += 8) {
+      float v[8];
+      tc::tmem_ld8(ta + (uint32_t)k0, v);
+      tc::tmem_ld_wait();
+      if (c < d)
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+          if (k0 + i < K) out[(size_t)(k0 + i) * d + c] = it > 0 ? v[i] : 0.f;
+    }
+  }
+  for (int k = tid; k < K; k += 256) C[(size_t)blockIdx.x * K + k] = (float)cnt[k];
   tc::fence_before_sync();
   __syncthreads();
   if (warp == 0) {
     tc::fence_after_sync();
-    tc::tmem_dealloc(tmem, (uint32_t)L.tcols);
+    tc::tmem_dealloc(tmem, (uint32_t)KL.tcols_all);
   }
 }
 
@@ -342,6 +406,7 @@ struct KmWork {
   float* C;      // [G][K] per-CTA counts
   double* shift; // [2] |Y_new - Y_old|^2, |Y_new|^2
   int* err;
+  int* pick;     // sample index of the last chosen seed
 };
 
 size_t km_carve(Carver& cv, int64_t n, int d, int K, int G, KmWork& w) {
@@ -357,6 +422,7 @@ size_t km_carve(Carver& cv, int64_t n, int d, int K, int G, KmWork& w) {
   w.C = cv.take<float>((size_t)G * K);
   w.shift = cv.take<double>(2);
   w.err = cv.take<int>(1);
+  w.pick = cv.take<int>(1);
   return cv.off + 256;  // room to align the caller's base
 }
 
@@ -408,8 +474,17 @@ HB_API int hb_kmeans_init(const float* X, int64_t n, int32_t n_pcs, int32_t n_cl
 
   HB_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
   HB_TRY(launch_l2_normalize<float, Bf>(X, n, d, d, w.Zh, ld, st));
-  k_km_seed<<<1, kSeedThreads, 0, st>>>(X, n, d, K, m, seed, w.S, w.D2, w.Yf);
+  const unsigned sgrid = (unsigned)((m + 255) / 256);
+  k_km_sample<<<sgrid, 256, 0, st>>>(X, n, d, m, seed, w.S);
   HB_LAUNCH_CHECK();
+  for (int r = 0; r < K; ++r) {
+    if (r > 0) {
+      k_km_dist<<<sgrid, 256, 0, st>>>(w.S, m, d, w.pick, r == 1, w.D2);
+      HB_LAUNCH_CHECK();
+    }
+    k_km_pick<<<1, kSeedThreads, 0, st>>>(w.S, w.D2, m, d, r, seed, w.pick, w.Yf);
+    HB_LAUNCH_CHECK();
+  }
   HB_CUDA(cudaMemsetAsync(w.shift, 0, 2 * sizeof(double), st));
   k_km_update<Bf><<<K, dim3(32, 8), 0, st>>>(w.P, w.C, 0, K, d, w.Yf, w.Yh, ld, w.hn, w.shift);
   HB_LAUNCH_CHECK();

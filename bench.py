@@ -389,6 +389,23 @@ def run_sections(args, dev):
     return out
 
 
+def max_over_ranks_of(x, dist, device):
+    """The largest `x` over the ranks of the process group (the step time of a job is its
+    slowest rank's); `x` itself without a process group."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(units_per_rank, world, ms_per_step):
+    """Whole-job rate: the units all ranks processed per step / the max-over-ranks step time."""
+    return units_per_rank * world / (ms_per_step / 1e3)
+
+
 def run_ours(args):
     import torch
 
@@ -416,11 +433,7 @@ def run_ours(args):
             dist.barrier()
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks_of(x, dist, dev)
 
     def timed(fn, steps, warmup):
         for _ in range(warmup):
@@ -460,7 +473,7 @@ def run_ours(args):
     ms, per = timed(step_resident, args.steps, args.warmup)
     clk = clocks.stop() if clocks else None
     prof = last["info"].profile
-    value = cell_iters * world / (ms / 1e3)
+    value = job_throughput(cell_iters, world, ms)
 
     # ---- end to end through the public API from pinned host memory ------------
     Z_pin = torch.from_numpy(Z).pin_memory()
@@ -477,7 +490,7 @@ def run_ours(args):
 
     warnings.simplefilter("ignore")
     ms_e2e, per_e2e = timed(step_e2e, args.steps, args.warmup)
-    e2e_value = cell_iters * world / (ms_e2e / 1e3)
+    e2e_value = job_throughput(cell_iters, world, ms_e2e)
 
     # ---- plain float32 path (the drop-in for dtype=np.float32) -----------------
     plain = None

@@ -62,3 +62,20 @@ def test_kmeans_rejects_sizes_out_of_range():
     ws = torch.empty(1 << 20, dtype=torch.uint8, device="cuda")
     st = lib.hb_kmeans_init(X.data_ptr(), 10, 4, 20, 5, 1e-4, 0, Y.data_ptr(), None, ws.data_ptr(), 1 << 20, None)
     assert st == _lib.HB_ERR_INVALID  # more clusters than cells
+
+
+@pytest.mark.parametrize("n,d,K", [(1000, 5, 7), (2500, 128, 256), (129, 64, 3), (4100, 33, 129)])
+def test_odd_shapes(n, d, K):
+    """Few and many PCs and clusters, a last tile of one cell, clusters just past a 64-block:
+    the seeding bit for bit, and Lloyd within the oracle's inertia."""
+    from rapids_singlecell_b200.synthetic import MixtureSpec, make_mixture
+
+    Z, _, _ = make_mixture(MixtureSpec(n, d, 5, 2, "given", (0.6, 0.4), 0.5), 40 + d)
+    X = torch.as_tensor(Z, device="cuda")
+    Y0 = kmeans_centroids(X, K, 5, max_iter=0).cpu().numpy()
+    assert np.array_equal(Y0, ko.seed_centres(Z, K, 5))
+    Y = kmeans_centroids(X, K, 5).cpu().numpy()
+    Yr, _ = ko.lloyd(Z, ko.seed_centres(Z, K, 5), 25, 1e-4)
+    i_gpu, i_ref = ko.inertia(Z, Y), ko.inertia(Z, Yr)
+    assert np.isfinite(Y).all() and i_gpu <= ko.inertia(Z, Y0)
+    assert abs(i_gpu - i_ref) / max(i_ref, 1e-9) < 1e-2

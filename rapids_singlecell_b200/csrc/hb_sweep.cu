@@ -68,9 +68,9 @@ __device__ __forceinline__ void grid_wait(unsigned* ctr, unsigned target, int* e
   __syncthreads();
 }
 
-// barrier of the 256 threads of thread group g (named barrier 1 + g)
-__device__ __forceinline__ void group_sync(int g) {
-  asm volatile("bar.sync %0, 256;" ::"r"(1 + g) : "memory");
+// barrier of the `nthreads` threads of thread group g (named barrier 1 + g)
+__device__ __forceinline__ void group_sync(int g, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(nthreads) : "memory");
 }
 
 // Shared memory of the sweep: NG groups, each with one or two A tiles, a staging
@@ -101,7 +101,7 @@ inline SweepLayout sweep_layout(int d, int K, int B, int ldr, int ng, int nbuf) 
   S.offPen = al(o, 16); o = S.offPen + (uint32_t)B * S.t.npad * 4u;  // rows padded to npad
   S.osmBytes = al((uint32_t)B * K * 4u, 16);
   S.offOsm = al(o, 16); o = S.offOsm + (uint32_t)ng * S.osmBytes;
-  S.offRows = al(o, 16); o = S.offRows + (uint32_t)ng * 3u * 256u * 4u;  // cid, ccat, rsp: [2][128] each
+  S.offRows = al(o, 16); o = S.offRows + (uint32_t)ng * 4096u;  // cid, ccat [2][128]; rsp [<= 4][128]
   S.offMisc = al(o, 16); o = S.offMisc + 64u + 32u * 8u;
   S.bytes = o + 1024u;  // slack for 1024-byte alignment of the base
   return S;
@@ -164,10 +164,10 @@ __device__ __forceinline__ TileIds load_tile_ids(const SweepArgs& a, int64_t pos
 
 // Copies of the tile's normalised embedding rows into the 128B-swizzled K-major
 // A tile (zero fill past the PCs and for missing rows).  gt = thread index in the
-// group: it owns row gt % 128 and every other 16-byte chunk of it.
+// group of 128 nparts threads: it owns row gt % 128 and every nparts-th 16-byte chunk of it.
 template <typename H>
 __device__ __forceinline__ void stage_tile(const SweepArgs& a, TileIds t, int gt, uint32_t sA, int dpad,
-                                           int* cid, int* ccat) {
+                                           int* cid, int* ccat, int nparts) {
   const int r = gt & 127, part = gt >> 7;
   if (part == 0) {
     cid[r] = t.cell;
@@ -176,7 +176,7 @@ __device__ __forceinline__ void stage_tile(const SweepArgs& a, TileIds t, int gt
   const H* Zn = (const H*)a.Zn;
   const H* src = t.cell >= 0 ? Zn + (int64_t)t.cell * a.ldz : Zn;
   const int nch = dpad / 8;
-  for (int ch = part; ch < nch; ch += 2) {
+  for (int ch = part; ch < nch; ch += nparts) {
     const bool ok = t.cell >= 0 && ch * 8 < a.ldz;
     const uint32_t dst = sA + (uint32_t)(ch >> 3) * 16384u + tc::sw128_off(r, ch & 7);
     tc::cp_async16(dst, ok ? (const void*)(src + ch * 8) : (const void*)Zn, ok ? 16u : 0u);
@@ -214,24 +214,27 @@ __device__ __forceinline__ void tile_runs(const int* cc, int nvalid, int* runs, 
   }
 }
 
-template <typename H, int NG>
-__global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayout SL) {
+// NG thread groups of 128 QS threads per CTA; each row of a tile is split over QS threads
+// (column ranges), warps w, w + 4, ... of a group reading the same TMEM lanes.
+template <typename H, int NG, int QS>
+__global__ void __launch_bounds__(128 * QS * NG, 1) k_tc_sweep(SweepArgs a, SweepLayout SL) {
   // the k-means loop has stopped on the device (set by an earlier launch: every CTA sees it)
   if (a.stop && *(volatile const int*)a.stop) return;
-  constexpr int NT = 256 * NG;
+  constexpr int GS = 128 * QS;  // threads of a group
+  constexpr int NT = GS * NG;
   extern __shared__ __align__(1024) unsigned char smem_dyn[];
   unsigned char* sm = (unsigned char*)(((uintptr_t)smem_dyn + 1023) & ~(uintptr_t)1023);
   const TcLayout& L = SL.t;
   const int K = a.K, B = a.B;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int g = tid >> 8, gt = tid & 255, gw = gt >> 5;   // thread group, index and warp in it
+  const int g = tid / GS, gt = tid % GS, gw = gt >> 5;   // thread group, index and warp in it
   const int nvw = gridDim.x * NG;  // workers (thread groups) of the launch
   float* pen = (float*)(sm + SL.offPen);                     // [B][npad] exponent offsets
   float* osm = (float*)(sm + SL.offOsm + g * SL.osmBytes);   // [B][K] observed-count delta
   H* Rst = (H*)(sm + SL.offRst + g * SL.rstBytes);           // [128][ldst] staged rows
-  int* cid = (int*)(sm + SL.offRows + g * 3072);             // [2][128] cell per row
+  int* cid = (int*)(sm + SL.offRows + g * 4096);             // [2][128] cell per row
   int* ccat = cid + 256;                                     // [2][128] batch per row
-  float* rsp = (float*)(ccat + 256);                         // [2][128] row sums of the halves
+  float* rsp = (float*)(ccat + 256);                         // [QS][128] row sums of the column ranges
   uint64_t* mbar = (uint64_t*)(sm + SL.offMisc) + g;
   uint32_t* tmem_slot = (uint32_t*)(sm + SL.offMisc + 32);
   double* red = (double*)(sm + SL.offMisc + 64);
@@ -272,7 +275,7 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
   const int2* gsl = gslice[g];
   Cursor cu;
   bool have = cursor_first(a, 0, gsl, cu);
-  if (have) stage_tile<H>(a, load_tile_ids(a, cu.pos, tile_rows(cu), gt & 127), gt, sA[0], L.dpad, cid, ccat);
+  if (have) stage_tile<H>(a, load_tile_ids(a, cu.pos, tile_rows(cu), gt & 127), gt, sA[0], L.dpad, cid, ccat, QS);
   __syncthreads();
   if (have && gw == 0) tile_runs(ccat, tile_rows(cu), runs[0], &nruns[0]);
   tc::fence_after_sync();
@@ -282,10 +285,10 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
   const float c2 = (float)(-2.0 / a.sigma * 1.4426950408889634);  // exp(x) = exp2(x log2 e)
   const int ldp = L.npad;
   const float sig = (float)a.sigma;
-  const int half = gw >> 2;  // warps 0-3 / 4-7 of the group: the two column halves
+  const int half = gw >> 2;  // warps 4 half .. 4 half + 3 of the group: column range `half` of QS
   const int row = (gw & 3) * 32 + lane;
   const uint32_t tl = tmem + ((uint32_t)((warp & 3) * 32) << 16);
-  const int nh = (L.npad / 2 + 7) / 8 * 8;
+  const int nh = (L.npad / QS + 7) / 8 * 8;  // columns per range (a multiple of 8)
   const int c_lo = half * nh, c_hi = min(L.npad, c_lo + nh);
   double obj_local = 0.0;
   uint32_t phase = 0;
@@ -375,7 +378,7 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
         tc::cp_async_wait_all();
         tc::fence_proxy_async_smem();
         tc::fence_before_sync();
-        group_sync(g);
+        group_sync(g, GS);
         if (gt == 0) issue_similarity_mma(tmem, sA[buf], sB, L, idesc, mbar);
       }
       pre_issued = false;
@@ -425,8 +428,10 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
       const float km = 2.f * (rs - kx);  // sum v (2 (1 - s))
       tc::tmem_st_wait();
       rsp[half * 128 + row] = rs;
-      group_sync(g);
-      const float rsum = rsp[row] + rsp[128 + row];
+      group_sync(g, GS);
+      float rsum = 0.f;
+#pragma unroll
+      for (int q = 0; q < QS; ++q) rsum += rsp[q * 128 + row];
       const float rsafe = a.init_mode ? fmaxf(rsum, 1e-12f) : rsum;
       const float inv = 1.f / rsafe;
       // pass 2: normalise, round to 16 bits, stage the row (for the counts and the R store)
@@ -457,8 +462,8 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
         obj_local += (double)e;
       }
       // copies of the next tile (its ids have landed by now)
-      if (have_nx) stage_tile<H>(a, tn, gt, sA[buf ^ 1], L.dpad, cid + (buf ^ 1) * 128, ccat + (buf ^ 1) * 128);
-      group_sync(g);
+      if (have_nx) stage_tile<H>(a, tn, gt, sA[buf ^ 1], L.dpad, cid + (buf ^ 1) * 128, ccat + (buf ^ 1) * 128, QS);
+      group_sync(g, GS);
       // the new assignment rows: one bulk store per row (ldr 16-bit values).  The last
       // tile of the block stores its rows after the grid arrival, while the other CTAs
       // finish the block (nothing reads R during the sweep).
@@ -475,7 +480,7 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
       // observed-count delta: one thread per cluster column (warp 0 last), summed per batch run
       const int* rn = runs[buf];
       const int nrn = nruns[buf];
-      for (int kc = (gt + 224) & 255; kc < K; kc += 256) {
+      for (int kc = (gt + GS - 32) % GS; kc < K; kc += GS) {
         for (int q = 0; q < nrn; ++q) {
           const int r0 = rn[q], r1 = rn[q + 1];
           float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
@@ -520,7 +525,7 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
     grid_arrive(a.barrier);
     if (pend_rows > 0) {  // coalesced 16-byte stores: consecutive threads on consecutive chunks of a row
       const int nch = a.ldr / 8;
-      for (int e = gt; e < pend_rows * nch; e += 256) {
+      for (int e = gt; e < pend_rows * nch; e += GS) {
         const int r = e / nch, c = e - r * nch;
         *(uint4*)(R + (int64_t)cid[pend_buf * 128 + r] * a.ldr + c * 8) = *(const uint4*)(Rst + r * L.ldst + c * 8);
       }
@@ -532,7 +537,7 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
       tc::cp_async_wait_all();
       tc::fence_proxy_async_smem();
       tc::fence_before_sync();
-      group_sync(g);
+      group_sync(g, GS);
       if (gt == 0) issue_similarity_mma(tmem, sA[buf], sB, L, idesc, mbar);
       pre_issued = true;
     }
@@ -579,13 +584,13 @@ __global__ void __launch_bounds__(256 * NG, 1) k_tc_sweep(SweepArgs a, SweepLayo
   }
 }
 
-template <typename H, int NG>
+template <typename H, int NG, int QS>
 static int launch_sweep_ng(const SweepArgs& a, const SweepLayout& SL, cudaStream_t st) {
-  const void* fn = (const void*)k_tc_sweep<H, NG>;
+  const void* fn = (const void*)k_tc_sweep<H, NG, QS>;
   const size_t smem = SL.bytes;
   HB_TRY(allow_max_dyn_smem(fn));
   int occ = 0;
-  HB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 256 * NG, smem));
+  HB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 128 * QS * NG, smem));
   if (occ < 1) {
     set_error("tensor-core sweep: kernel does not fit on an SM");
     return HB_ERR_UNSUPPORTED;
@@ -598,16 +603,16 @@ static int launch_sweep_ng(const SweepArgs& a, const SweepLayout& SL, cudaStream
   SweepArgs args = a;
   SweepLayout lay = SL;
   void* kargs[] = {(void*)&args, (void*)&lay};
-  HB_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(256 * NG), kargs, smem, st));
+  HB_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(128 * QS * NG), kargs, smem, st));
   ++g_launches;
   return HB_OK;
 }
 
-// Dynamic plus static shared memory of k_tc_sweep<H, NG> fits in one CTA.
-template <typename H, int NG>
+// Dynamic plus static shared memory of k_tc_sweep<H, NG, QS> fits in one CTA.
+template <typename H, int NG, int QS>
 static int sweep_fits(const SweepLayout& SL, bool& fits) {
   cudaFuncAttributes fa;
-  HB_CUDA(cudaFuncGetAttributes(&fa, (const void*)k_tc_sweep<H, NG>));
+  HB_CUDA(cudaFuncGetAttributes(&fa, (const void*)k_tc_sweep<H, NG, QS>));
   int dev = 0, optin = 0;
   HB_CUDA(cudaGetDevice(&dev));
   HB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
@@ -615,19 +620,20 @@ static int sweep_fits(const SweepLayout& SL, bool& fits) {
   return HB_OK;
 }
 
-// Layout preference: two thread groups before one, two A tiles per group before one.
+// Layout preference: two thread groups (two threads per row) before one group (four threads
+// per row, so the CTA still runs 512 threads), two A tiles per group before one.
 template <typename H>
 int launch_tc_sweep(const SweepArgs& a, cudaStream_t st) {
   bool fits = false;
   for (int nbuf = 2; nbuf >= 1; --nbuf) {
     const SweepLayout S2 = sweep_layout(a.d, a.K, a.B, a.ldr, 2, nbuf);
-    HB_TRY(sweep_fits<H, 2>(S2, fits));
-    if (fits) return launch_sweep_ng<H, 2>(a, S2, st);
+    HB_TRY((sweep_fits<H, 2, 2>(S2, fits)));
+    if (fits) return launch_sweep_ng<H, 2, 2>(a, S2, st);
   }
   for (int nbuf = 2; nbuf >= 1; --nbuf) {
     const SweepLayout S1 = sweep_layout(a.d, a.K, a.B, a.ldr, 1, nbuf);
-    HB_TRY(sweep_fits<H, 1>(S1, fits));
-    if (fits) return launch_sweep_ng<H, 1>(a, S1, st);
+    HB_TRY((sweep_fits<H, 1, 4>(S1, fits)));
+    if (fits) return launch_sweep_ng<H, 1, 4>(a, S1, st);
   }
   set_error("tensor-core sweep: shared-memory tables too large (B=%d K=%d d=%d)", a.B, a.K, a.d);
   return HB_ERR_UNSUPPORTED;

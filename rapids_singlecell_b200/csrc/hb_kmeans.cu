@@ -17,9 +17,10 @@
 //   Lloyd    up to max_iter iterations over all cells: the assignment is the
 //            tensor-core similarity of a 128-cell tile of bf16 Z_norm against the
 //            bf16 centres (fp32 in TMEM), argmax_k (z.y_k - |y_k|^2 / 2), which is
-//            the nearest centre for unit rows; each CTA adds its rows to their
-//            centre's sum in shared memory; the per-CTA sums are reduced per
-//            centre, and a centre that lost all its cells keeps its position.
+//            the nearest centre for unit rows; the tile's rows are added to their
+//            centre's sum by a second MMA (Z_tile^T times the one-hot of the labels,
+//            accumulated in TMEM); the per-CTA sums are reduced per centre in float64,
+//            and a centre that lost all its cells keeps its position.
 //            Stops when |Y_new - Y_old|_F <= tol |Y_new|_F.
 #include "hb_tc_tile.cuh"
 

@@ -251,18 +251,19 @@ __global__ void __launch_bounds__(256, 1) k_tc_centroid_stream(CenStreamArgs a, 
   }
 }
 
-// Both reductions of the per-CTA partials in one launch (one wave), 32 x 8 threads per CTA;
-// threadIdx.y takes every 8th CTA partial and the eight float64 sums are combined in shared
-// memory:
+// Both reductions of the per-CTA partials in one launch (one wave), 32 x kRedY threads per
+// CTA; threadIdx.y takes every kRedY-th CTA partial and the float64 sums are combined in
+// shared memory:
 //   CTAs 0 .. K-1: centroid row k = blockIdx.x, Y[k] = sum_g P[g][k][:], written L2-normalised
 //                  as 16-bit Y_norm (inverse norm capped at 1e12, kernels_normalize.cuh:7-54);
 //   the others:    32 consecutive (key, cluster) entries e, Omin[e] = sum_g Opart[g][e].
+constexpr int kRedY = 16;
 template <typename H>
-__global__ void __launch_bounds__(256) k_cs_reduce(const float* __restrict__ P, const float* __restrict__ Opart, int G,
+__global__ void __launch_bounds__(32 * kRedY) k_cs_reduce(const float* __restrict__ P, const float* __restrict__ Opart, int G,
                                                    int K, int d, int nkeys, H* __restrict__ Yn, int ldy,
                                                    double* __restrict__ Omin, const int* stop) {
   if (stop && *(volatile const int*)stop) return;  // the k-means loop has stopped on the device
-  __shared__ double part[8][128];
+  __shared__ double part[kRedY][128];
   __shared__ double red[32];
   const int lane = threadIdx.x, y = threadIdx.y, t = y * 32 + lane;
   if ((int)blockIdx.x < K) {
@@ -271,7 +272,7 @@ __global__ void __launch_bounds__(256) k_cs_reduce(const float* __restrict__ P, 
       for (int c = c0 + lane; c < min(d, c0 + 128); c += 32) {
         double s = 0.0;
 #pragma unroll 8
-        for (int g = y; g < G; g += 8) s += (double)__ldg(P + ((size_t)g * K + k) * d + c);
+        for (int g = y; g < G; g += kRedY) s += (double)__ldg(P + ((size_t)g * K + k) * d + c);
         part[y][c - c0] = s;
       }
     }
@@ -279,13 +280,13 @@ __global__ void __launch_bounds__(256) k_cs_reduce(const float* __restrict__ P, 
     double v = 0.0, ss = 0.0;
     if (t < d) {
 #pragma unroll
-      for (int q = 0; q < 8; ++q) v += part[q][t];
+      for (int q = 0; q < kRedY; ++q) v += part[q][t];
       ss = v * v;
     }
     ss = block_sum(ss, red);
     double inv = rsqrt(ss);
     if (inv > 1e12) inv = 1e12;
-    for (int c = t; c < ldy; c += 256) Yn[(size_t)k * ldy + c] = from_f<H>(c < d ? (float)(v * inv) : 0.f);
+    for (int c = t; c < ldy; c += 32 * kRedY) Yn[(size_t)k * ldy + c] = from_f<H>(c < d ? (float)(v * inv) : 0.f);
     return;
   }
   const int64_t ne = (int64_t)nkeys * K;
@@ -293,14 +294,14 @@ __global__ void __launch_bounds__(256) k_cs_reduce(const float* __restrict__ P, 
   double s = 0.0;
   if (e < ne) {
 #pragma unroll 8
-    for (int g = y; g < G; g += 8) s += (double)__ldg(Opart + (size_t)g * ne + e);
+    for (int g = y; g < G; g += kRedY) s += (double)__ldg(Opart + (size_t)g * ne + e);
   }
   part[y][lane] = s;
   __syncthreads();
   if (y == 0 && e < ne) {
     double tot = 0.0;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) tot += part[q][lane];
+    for (int q = 0; q < kRedY; ++q) tot += part[q][lane];
     Omin[e] = tot;
   }
 }
@@ -350,7 +351,7 @@ int launch_tc_centroid_stream(const CenStreamArgs& a, const void* Zn, int ldz, c
   k_tc_centroid_stream<H><<<grid, 256, smem, st>>>(a, L, tmZ, tmR);
   HB_LAUNCH_CHECK();
   const int64_t ne = (int64_t)a.nkeys * a.K;
-  k_cs_reduce<H><<<(unsigned)(a.K + (ne + 31) / 32), dim3(32, 8), 0, st>>>(a.P, a.Opart, grid, a.K, a.d, a.nkeys,
+  k_cs_reduce<H><<<(unsigned)(a.K + (ne + 31) / 32), dim3(32, kRedY), 0, st>>>(a.P, a.Opart, grid, a.K, a.d, a.nkeys,
                                                                         (H*)a.Yn, a.ldy, Omin, a.stop);
   HB_LAUNCH_CHECK();
   return HB_OK;

@@ -72,7 +72,7 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* m, uint32_t byte
                : "memory");
 }
 
-// ---- TMA row gather (no multicast): 4 rows x one 64-element box of a 2-D
+// ---- TMA row gather (this CTA only): 4 rows x one 64-element box of a 2-D
 // tensor map (box one row high) into 512 contiguous bytes of shared memory; the
 // tensor map's 128B swizzle is applied from the destination address.  Rows at or
 // beyond the tensor's height read the zero fill.  Completion is counted on mbar.
@@ -101,7 +101,7 @@ __device__ __forceinline__ void bulk_wait_read_all() {
 // wait until all committed bulk stores of this thread are complete
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
-// ---- TMA tile load (no multicast) of a 4-D tensor map box at {x0, x1, x2, x3} ------
+// ---- TMA tile load (this CTA only) of a 4-D tensor map box at {x0, x1, x2, x3} ----
 __device__ __forceinline__ void tma_load4d(uint32_t dst, const CUtensorMap* tm, int x0, int x1, int x2, int x3,
                                            uint64_t* mbar) {
   asm volatile(

@@ -161,10 +161,21 @@ class HarmonyProblem:
             pass
 
 
+def from_dlpack(x):
+    """Arrays of other libraries that export DLPack (``__dlpack__``: CuPy, JAX, ...) as torch
+    tensors sharing their memory (no copy); torch tensors, NumPy arrays, pandas objects and
+    lists pass through unchanged.  The corrected embedding is returned as a torch tensor,
+    which exports DLPack itself (``cupy.from_dlpack(Z_hat)`` takes it without a copy)."""
+    if isinstance(x, (torch.Tensor, np.ndarray)) or not hasattr(x, "__dlpack__"):
+        return x
+    return torch.from_dlpack(x)
+
+
 def _integer_codes(labels):
     """Categorical codes of plain non-negative integer labels without pandas:
     the categories are the sorted distinct values, as ``astype("category")``
     gives them.  Returns (None, 0) for anything else."""
+    labels = from_dlpack(labels)
     if isinstance(labels, torch.Tensor):
         labels = labels.detach().cpu().numpy()
     if not isinstance(labels, np.ndarray) or labels.ndim != 1 or labels.dtype.kind not in "iu":
@@ -331,8 +342,10 @@ def harmonize(
     ``precision`` is one of "fp32", "fp64" (plain paths) or "bf16"/"fp16"
     (tensor-core paths); by default it follows the dtype of ``Z``.
     Returns the corrected embedding as a torch tensor on the GPU (and a
-    ``HarmonyInfo`` when ``return_info``).
+    ``HarmonyInfo`` when ``return_info``).  ``Z`` and integer ``batch_mat`` labels may
+    be arrays of any library that exports DLPack; device arrays are used in place.
     """
+    Z = from_dlpack(Z)
     n_cells, n_pcs = (int(v) for v in Z.shape)
     cats_np, n_batches = _integer_codes(batch_mat) if batch_key is None else (None, 0)
     if cats_np is None:

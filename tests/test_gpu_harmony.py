@@ -134,3 +134,29 @@ def test_engine_cell_index_matches_caller_sorted():
     b.cell_index = torch.as_tensor(np.argsort(cats, kind="stable").astype(np.int32), device="cuda")
     zb = b.run()[0]
     assert rel_maxabs(za.cpu().numpy(), zb.cpu().numpy()) < 1e-5
+
+
+def test_dlpack_device_input_runs_in_place():
+    """An array of another library on the device (seen only through DLPack) is integrated
+    without a copy to the host and gives the result of the equivalent torch tensor."""
+    import torch
+
+    class Exporter:
+        def __init__(self, t):
+            self._t = t
+
+        def __dlpack__(self, *args, **kwargs):
+            return self._t.__dlpack__(*args, **kwargs)
+
+        def __dlpack_device__(self):
+            return self._t.__dlpack_device__()
+
+    cfg = make_config("C1", seed=12, n_cells=3000)
+    Zt = torch.as_tensor(cfg["Z"], device="cuda")
+    codes = torch.as_tensor(cfg["cats"].astype(np.int64), device="cuda")
+    kw = dict(n_clusters=20, max_iter_harmony=2, max_iter_clustering=4, tol_harmony=-np.inf,
+              tol_clustering=-np.inf, init_centroids=cfg["Y0"][:20], precision="fp32")
+    a = harmonize(Exporter(Zt), Exporter(codes), None, **kw)
+    b = harmonize(Zt, cfg["cats"].astype(np.int64), None, **kw)
+    assert a.device.type == "cuda"
+    assert (a - b).abs().max().item() <= 1e-5 * b.abs().max().item()

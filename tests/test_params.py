@@ -94,3 +94,30 @@ def test_request_bytes_counts_workspace_and_tensors():
     ws = HarmonyProblem.workspace_bytes(make_params(1000, 50, 30, 3, precision="bf16",
                                                     max_iter_harmony=2, max_iter_clustering=5))
     assert request_bytes(r) == ws + 2 * 1000 * 50 * 4 + 30 * 50 * 4 + 1000 * 4
+
+
+class _Exporter:
+    """An array of another library: it exposes only the DLPack protocol."""
+
+    def __init__(self, t):
+        self._t = t
+
+    def __dlpack__(self, *args, **kwargs):
+        return self._t.__dlpack__(*args, **kwargs)
+
+    def __dlpack_device__(self):
+        return self._t.__dlpack_device__()
+
+
+def test_dlpack_inputs_share_memory():
+    import torch
+
+    from rapids_singlecell_b200.harmony import _integer_codes, from_dlpack
+
+    t = torch.arange(12, dtype=torch.float32).reshape(4, 3)
+    z = from_dlpack(_Exporter(t))
+    assert isinstance(z, torch.Tensor) and z.data_ptr() == t.data_ptr()
+    codes, nb = _integer_codes(_Exporter(torch.tensor([5, 2, 5, 9], dtype=torch.int64)))
+    assert nb == 3 and codes.tolist() == [1, 0, 1, 2]
+    a = np.zeros(3)
+    assert from_dlpack(a) is a and from_dlpack([1, 2]) == [1, 2]

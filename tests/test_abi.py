@@ -52,3 +52,22 @@ def test_struct_layout():
     assert ctypes.sizeof(_lib.HbParams) == 112
     assert ctypes.sizeof(_lib.HbOutputs) == 6 * ctypes.sizeof(ctypes.c_void_p)
     assert ctypes.sizeof(_lib.HbProfile) == 56
+
+
+def test_kmeans_init_validation_without_gpu():
+    """hb_kmeans_init checks its arguments before touching the device."""
+    lib = _lib.load()
+    ws = lib.hb_kmeans_workspace_bytes(10_000, 50, 100)
+    assert ws > 10_000 * 56 * 2  # at least the bf16 copy of the rows
+    assert lib.hb_kmeans_workspace_bytes(0, 50, 100) == 0
+    it = ctypes.c_int32(0)
+    fake = ctypes.c_void_p(256)  # never dereferenced: every case fails before any device work
+    def call(n, d, K, max_iter=25, tol=1e-4, ws_bytes=1 << 30):
+        return lib.hb_kmeans_init(fake, n, d, K, max_iter, tol, 0, fake, ctypes.byref(it), fake, ws_bytes, None)
+    assert call(100, 10, 200) == _lib.HB_ERR_INVALID        # more clusters than cells
+    assert call(100, 10, 5, max_iter=-1) == _lib.HB_ERR_INVALID
+    assert call(100, 10, 5, tol=float("nan")) == _lib.HB_ERR_INVALID
+    assert call(1000, 129, 5) == _lib.HB_ERR_UNSUPPORTED    # more than 128 PCs
+    assert call(1000, 10, 257) == _lib.HB_ERR_UNSUPPORTED   # more than 256 clusters
+    assert call(1000, 10, 5, ws_bytes=16) == _lib.HB_ERR_WORKSPACE
+    assert b"workspace" in lib.hb_last_error()

@@ -32,6 +32,11 @@ import numpy as np
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
+# 32 hardware work queues instead of CUDA's default 8, set before CUDA starts in this process:
+# the batched section runs 32 streams, and with 8 queues streams share queues and serialise
+# (256 problems: 32 streams measured 1.1e9-1.3e9 cell-iters/s, 8 streams 0.7e9-0.9e9).  The
+# single-stream measurements are unaffected.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 OUTER, INNER = 10, 20
 WORKLOAD = "C2"
@@ -261,12 +266,12 @@ def wide_section(dev):
     return out
 
 
-def batched_section(dev, n_problems=256, streams=8):
+def batched_section(dev, n_problems=256, streams=32):
     """Independent problems of uneven sizes on one GPU: cells log-uniform in
     [2k, 200k], d in {30, 50}, B uniform in [2, 12], K = min(100, n / 30), each
     from the mixture generator with its own seed (10 types, Dirichlet(1)
     batches); 10 outer x 20 k-means iterations fixed; inputs resident on the
-    device.  All problems go through one HarmonyServer (8 streams); bf16 and
+    device.  All problems go through one HarmonyServer (32 streams); bf16 and
     plain fp32 runs of the same set, and the per-problem bf16 vs fp32 error."""
     import torch
 

@@ -12,6 +12,11 @@ GIL.
 Admission is by an HBM budget: a problem starts only when its workspace, inputs
 and output fit into what the running problems leave of the budget.
 
+CUDA gives a process 8 hardware work queues unless CUDA_DEVICE_MAX_CONNECTIONS is
+set before CUDA starts; beyond 8 streams the streams share queues and partly
+serialise.  With the variable at 32, 32 streams ran 256 small problems about 1.4x
+faster than 8.
+
 The persistent sweep of each problem is a cooperative launch whose CTAs wait
 for each other at a grid barrier (one CTA per SM).  Two such grids that are both
 only partly resident could each wait for SMs the other holds, so SMs are a second

@@ -65,3 +65,27 @@ def test_reference_arm_runs_on_rank_zero_only(monkeypatch, capsys):
 
     assert bench.run_reference(A()) is None
     assert capsys.readouterr().out == ""
+
+
+def test_reference_arm_prints_the_contract_line(monkeypatch, capsys):
+    """The CPU reference arm: one JSON line with the metric, its unit and direction, the
+    CPU baseline it measured and an e2e entry that moves no bytes."""
+    import json
+
+    sys.path.insert(0, ROOT)
+    import bench
+
+    monkeypatch.setenv("RANK", "0")
+    monkeypatch.setenv("WORLD_SIZE", "1")
+
+    class A:
+        steps, warmup, gpus = 1, 0, 1
+
+    bench.run_reference(A())
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["metric"] == bench.METRIC
+    assert line["unit"] == "cell-iters/s" and line["higher_is_better"] is True and line["value"] > 0
+    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
+    assert line["cpu_baseline"]["value"] == line["value"]
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+    assert line["config"]["workload"].startswith("C2: 500000 cells")

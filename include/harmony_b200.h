@@ -145,7 +145,9 @@ HB_API int hb_block_lists(int64_t n, int64_t block_size, const uint32_t* seeds, 
  * synchronises the device and can fail under memory pressure), or a C host with no allocator.
  * Returns HB_ERR_WORKSPACE when hb_block_lists_workspace_bytes() exceeds the limit.  The first
  * call on a device looks up the array (cudaGetSymbolAddress) and should come before any stream
- * capture.  Calls that overlap in time race on the array; it keeps the last call's contents. */
+ * capture; the looked-up address is kept for the life of the process, so the entry point must not
+ * be called again on a device after cudaDeviceReset().  Calls that overlap in time race on the
+ * array; it keeps the last call's contents.  n_iters == 0 returns HB_OK without device work. */
 #define HB_BLOCK_LISTS_STATIC_MAX_BYTES ((size_t)16 << 20)
 HB_API int hb_block_lists_static(int64_t n, int64_t block_size, const uint32_t* seeds, int32_t n_iters,
                                  const int32_t* cats, int32_t n_batches, int32_t* idx, void* stream);

@@ -289,23 +289,22 @@ int hb_similarity(const void* Zn, int32_t ldz, const void* Yn, int32_t ldy, cons
 
 namespace {
 
+// block update of the plain paths (the 16-bit path runs the persistent sweep instead)
 template <typename S>
-int block_update(const BlockArgs& a, const double* in, double* out, double* zero, int* err,
-                 cudaStream_t st) {
+int block_update(const BlockArgs& a, const double* in, double* out, double* zero, cudaStream_t st) {
+  static_assert(std::is_same<S, double>::value || std::is_same<S, float>::value, "plain paths only");
   if constexpr (std::is_same<S, double>::value) return launch_block_update_f64(a, in, out, zero, st);
-  else if constexpr (std::is_same<S, float>::value) return launch_block_update_f32(a, in, out, zero, st);
-  else return launch_tc_block_update<S>(a, in, out, zero, err, st);
+  else return launch_block_update_f32(a, in, out, zero, st);
 }
 
 struct ORing {
   double* buf[3];
-  int* err;
   int cur = 0;
   // launch a block update that reads the current state and produces the next
   template <typename S>
   int step(const BlockArgs& a, cudaStream_t st) {
     const int out = (cur + 1) % 3, zero = (cur + 2) % 3;
-    HB_TRY(block_update<S>(a, buf[cur], buf[out], buf[zero], err, st));
+    HB_TRY(block_update<S>(a, buf[cur], buf[out], buf[zero], st));
     cur = out;
     return HB_OK;
   }
@@ -383,11 +382,13 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
   for (int i = 0; i < 3; ++i) HB_CUDA(cudaMemsetAsync(w.O[i], 0, sizeof(double) * (B + 1) * K, st));
   HB_CUDA(cudaMemsetAsync(w.obj_acc, 0, sizeof(double), st));
   HB_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
+  // the splitter's overflow flag is read once per outer iteration: cleared once per run
+  HB_TRY(membership_clear_err(w.mb, st));
 
   S* Zn = (S*)w.Zn;
   S* R = (S*)w.R;
   S* Yn = (S*)w.Yn;
-  ORing ring{{w.O[0], w.O[1], w.O[2]}, w.err, 0};
+  ORing ring{{w.O[0], w.O[1], w.O[2]}, 0};
 
   BlockArgs base{};
   base.Zn = Zn; base.ldz = P->ldz; base.R = R; base.ldr = P->ldr; base.cats = cats;
@@ -708,7 +709,11 @@ size_t hb_block_lists_workspace_bytes(int64_t n, int64_t block_size, int32_t n_b
 int hb_block_lists(int64_t n, int64_t block_size, const uint32_t* seeds, int32_t n_iters,
                    const int32_t* cats, int32_t n_batches, int32_t* idx, void* workspace,
                    size_t workspace_bytes, void* stream) {
-  if (n < 1 || block_size < 1 || !seeds || !idx) { set_error("hb_block_lists: bad argument"); return HB_ERR_INVALID; }
+  if (n < 1 || block_size < 1 || !seeds || !idx || n_iters < 0) {
+    set_error("hb_block_lists: bad argument");
+    return HB_ERR_INVALID;
+  }
+  if (n_iters == 0) return HB_OK;
   MembershipLayout L = membership_layout(n, block_size, cats ? n_batches : 1);
   if (L.nblk > kMaxBlocks) { set_error("too many blocks"); return HB_ERR_UNSUPPORTED; }
   if (L.cap > 16384) { set_error("n too large"); return HB_ERR_UNSUPPORTED; }
@@ -720,6 +725,7 @@ int hb_block_lists(int64_t n, int64_t block_size, const uint32_t* seeds, int32_t
   MembershipBufs B;
   membership_carve(cv, L, B);
   cudaStream_t st = (cudaStream_t)stream;
+  HB_TRY(membership_clear_err(B, st));
   for (int c0 = 0; c0 < n_iters; c0 += kMaxIterChunk) {
     const int C = std::min(kMaxIterChunk, n_iters - c0);
     HB_TRY(membership_build(L, B, seeds + c0, C, cats, idx + (size_t)c0 * n, st));

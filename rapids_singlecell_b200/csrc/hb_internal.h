@@ -41,6 +41,8 @@ void membership_carve(Carver& cv, const MembershipLayout& L, MembershipBufs& B);
 int membership_build(const MembershipLayout& L, const MembershipBufs& B, const uint32_t* h_seeds,
                      int n_iters, const int32_t* cats, int32_t* idx, cudaStream_t st,
                      int32_t* lcat = nullptr, int32_t* ckey = nullptr, int n_batches = 0);
+// B.err (candidate overflow) is set by the builds and cleared only by membership_clear_err
+int membership_clear_err(const MembershipBufs& B, cudaStream_t st);
 int membership_build_dev(const MembershipLayout& L, const MembershipBufs& B, const uint32_t* seeds,
                          uint32_t seed0, int n_iters, const int32_t* cats, int32_t* idx,
                          cudaStream_t st, int32_t* lcat = nullptr, int32_t* ckey = nullptr,
@@ -114,9 +116,6 @@ int launch_objective_finalize(const double* O, const double* Pr, const double* t
 // 2-D tensor map over a row-major 16-bit matrix [rows][ld] for row gathers:
 // box = 64 elements x 1 row, 128-byte swizzle, zero fill out of bounds.
 int make_row_gather_map(CUtensorMap* tm, const void* base, int64_t rows, int ld, bool bf16);
-template <typename H>
-int launch_tc_block_update(const BlockArgs& a, const double* O_in, double* O_out, double* O_zero,
-                           int* err, cudaStream_t st);
 template <typename H>
 int launch_tc_similarity(const H* Zn, int ldz, const H* Yn, int ldy, const int32_t* idx,
                          const int32_t* cats, int64_t n, int d, int K, float* S, int* err,

@@ -368,8 +368,16 @@ int membership_build(const MembershipLayout& L, const MembershipBufs& B, const u
   return membership_build_dev(L, B, B.seeds, 0, n_iters, cats, idx, st, lcat, ckey, n_batches);
 }
 
+// Clears the candidate-overflow flag.  The build functions only ever set it, so a caller
+// clears it once before its first chunk and reads it once after the last one.
+int membership_clear_err(const MembershipBufs& B, cudaStream_t st) {
+  HB_CUDA(cudaMemsetAsync(B.err, 0, sizeof(int), st));
+  return HB_OK;
+}
+
 // Block lists for the consecutive seeds seed0 .. seed0+n_iters-1 (no host copy),
-// or for the device list `seeds` when it is not null.
+// or for the device list `seeds` when it is not null.  Sets B.err on a candidate
+// overflow and never clears it (membership_clear_err).
 int membership_build_dev(const MembershipLayout& L, const MembershipBufs& B, const uint32_t* seeds,
                          uint32_t seed0, int n_iters, const int32_t* cats, int32_t* idx,
                          cudaStream_t st, int32_t* lcat, int32_t* ckey, int n_batches) {
@@ -378,7 +386,6 @@ int membership_build_dev(const MembershipLayout& L, const MembershipBufs& B, con
   const int nsub = cats ? L.nsub : 1;
   const int nbk = L.nblk * nsub;
   HB_CUDA(cudaMemsetAsync(B.hist, 0, sizeof(uint32_t) * (size_t)n_iters * kNumBins, st));
-  HB_CUDA(cudaMemsetAsync(B.err, 0, sizeof(int), st));
   int g = std::min(div_up(L.n, 256 * 8), 2 * sms);
   if (g < 1) g = 1;
   if (nb > 0) {

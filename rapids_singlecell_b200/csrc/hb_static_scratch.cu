@@ -14,11 +14,14 @@
 //     HB_ERR_WORKSPACE and a message naming both sizes;
 //   * the first call on a device (with that device current) looks up the
 //     array's device address with cudaGetSymbolAddress, which may load this
-//     module; make that first call before any stream capture;
+//     module; make that first call before any stream capture.  The address is
+//     cached per device for the life of the process: after cudaDeviceReset()
+//     it is stale, so do not call this entry point again after a reset;
 //   * the array is shared by every call on the device: calls that overlap in
 //     time (other streams or host threads) race on it, and it keeps the last
 //     call's contents.  The parts that must start at zero (the key histogram
-//     and the overflow flag) are cleared on the stream by every call.
+//     and the overflow flag) are cleared on the stream by every call that
+//     writes lists; n_iters == 0 returns at once without touching the device.
 #include <mutex>
 
 #include "hb_internal.h"
@@ -70,6 +73,7 @@ HB_API int hb_block_lists_static(int64_t n, int64_t block_size, const uint32_t* 
     set_error("hb_block_lists_static: bad argument");
     return HB_ERR_INVALID;
   }
+  if (n_iters == 0) return HB_OK;  // no lists to write: the device is not touched
   const MembershipLayout L = membership_layout(n, block_size, cats ? n_batches : 1);
   if (L.nblk > kMaxBlocks) { set_error("hb_block_lists_static: too many blocks"); return HB_ERR_UNSUPPORTED; }
   if (L.cap > 16384) { set_error("hb_block_lists_static: n too large"); return HB_ERR_UNSUPPORTED; }
@@ -86,6 +90,7 @@ HB_API int hb_block_lists_static(int64_t n, int64_t block_size, const uint32_t* 
   MembershipBufs B;
   membership_carve(cv, L, B);
   cudaStream_t st = (cudaStream_t)stream;
+  HB_TRY(membership_clear_err(B, st));  // the flag covers every chunk of this call
   for (int c0 = 0; c0 < n_iters; c0 += kMaxIterChunk) {
     const int C = std::min(kMaxIterChunk, n_iters - c0);
     HB_TRY(membership_build(L, B, seeds + c0, C, cats, idx + (size_t)c0 * n, st));

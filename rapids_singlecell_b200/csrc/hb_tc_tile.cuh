@@ -49,14 +49,6 @@ inline TcLayout tc_layout(int d, int K, int B, int ldr, int elem_bytes_pen) {
   return L;
 }
 
-struct TcArgs {
-  BlockArgs a;
-  const double* O_in;
-  double* O_out;
-  double* O_zero;
-  int* err;
-};
-
 template <typename H> struct is_bf16 { static constexpr bool value = false; };
 template <> struct is_bf16<__nv_bfloat16> { static constexpr bool value = true; };
 

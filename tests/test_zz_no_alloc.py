@@ -32,14 +32,15 @@ def test_static_block_lists_rejects_sizes_beyond_the_scratch():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("n_seeds", [3, 9, 17])  # one, two and three chunks of eight k-means iterations
 @pytest.mark.parametrize("B", [0, 5])
-def test_static_block_lists_match_workspace_entry(B):
+def test_static_block_lists_match_workspace_entry(B, n_seeds):
     import torch
 
     from tests._gpu import dev, lib, ptr, stream
 
     n, bs = 120_000, 6_000
-    seeds = [3, 77, 1000003]
+    seeds = [3, 77, 1000003, 0xFFFFFFFF, 11, 12, 500, 501, 9, 1, 2, 4, 8, 16, 32, 64, 128][:n_seeds]
     cats = np.random.default_rng(9).integers(0, max(B, 1), n).astype(np.int32)
     dcats = dev(cats)
     arr = (ctypes.c_uint32 * len(seeds))(*seeds)
@@ -55,3 +56,24 @@ def test_static_block_lists_match_workspace_entry(B):
                                                ptr(out), stream()))
         torch.cuda.synchronize()
         assert torch.equal(out, ref)
+
+
+@pytest.mark.gpu
+def test_static_block_lists_zero_iterations_is_a_no_op():
+    """n_iters == 0 writes nothing and reports success, even right after a call that used
+    the shared scratch."""
+    import torch
+
+    from tests._gpu import lib, ptr, stream
+
+    n, bs = 50_000, 2_500
+    seeds = (ctypes.c_uint32 * 2)(5, 6)
+    out = torch.full((2 * n,), -1, dtype=torch.int32, device="cuda")
+    _lib.check(lib().hb_block_lists_static(n, bs, seeds, 2, None, 0, ptr(out), stream()))
+    untouched = torch.full((n,), -7, dtype=torch.int32, device="cuda")
+    assert lib().hb_block_lists_static(n, bs, seeds, 0, None, 0, ptr(untouched), stream()) == _lib.HB_OK
+    torch.cuda.synchronize()
+    assert bool((untouched == -7).all())
+    # the workspace entry point agrees on both cases, and rejects a negative count
+    assert lib().hb_block_lists(n, bs, seeds, 0, None, 0, ptr(untouched), None, 0, stream()) == _lib.HB_OK
+    assert lib().hb_block_lists(n, bs, seeds, -1, None, 0, ptr(untouched), None, 0, stream()) == _lib.HB_ERR_INVALID

@@ -79,6 +79,12 @@ typedef struct hb_params {
                                    must together stay within the SM count, or their grid barriers
                                    can wait on each other */
   uint64_t random_state;
+  int64_t sweep_wait_ns;        /* bound of each grid-barrier wait of the persistent sweep (16-bit path):
+                                   after this long the wait gives up and the run returns HB_ERR_TIMEOUT;
+                                   0 means 2 s */
+  int32_t test_unmet_arrivals;  /* test hook, 0 in normal use: the sweep's grid barrier waits for this many
+                                   arrivals more than its CTAs make, so every wait runs out (bounded by
+                                   sweep_wait_ns) and the run must return HB_ERR_TIMEOUT */
 } hb_params;
 
 typedef struct hb_plan hb_plan;

@@ -340,8 +340,18 @@ def harmonize(Z, cats, n_batches, Y0, *, n_clusters=None, max_iter_harmony=10,
               ridge_lambda=1.0, sigma=0.1, block_proportion=0.05, theta=2.0, tau=0,
               random_state=0, stabilized_penalty=True, dynamic_lambda=True, alpha=0.2,
               batch_prune_threshold=1e-5, correction_method="batched",
-              dtype=np.float64) -> OracleResult:
-    """Restatement of ``harmonize`` (_harmony/__init__.py:41-289) with injected Y0."""
+              dtype=np.float64, timings=None) -> OracleResult:
+    """Restatement of ``harmonize`` (_harmony/__init__.py:41-289) with injected Y0.
+
+    ``timings`` (a dict, optional) receives the wall seconds of the phases: ``init`` (input
+    normalisation and the initial R / E / O / objective), ``clustering`` (all k-means
+    iterations, objective included) and ``correction`` (lambda, ridge correction and the
+    renormalisation), summed over the outer iterations."""
+    import time
+
+    clock = time.perf_counter
+    tm = {"init": 0.0, "clustering": 0.0, "correction": 0.0}
+    t0 = clock()
     dt = np.dtype(dtype)
     X = np.ascontiguousarray(Z, dtype=dt)
     cats = np.asarray(cats, dtype=np.int64)
@@ -357,12 +367,14 @@ def harmonize(Z, cats, n_batches, Y0, *, n_clusters=None, max_iter_harmony=10,
     R, E, O, obj0 = init_state(Z_norm, np.asarray(Y0), cats, n_batches, Pr_b, th, sigma,
                                stabilized_penalty)
     objs = [obj0]
+    tm["init"] = clock() - t0
     km_objs = []
     converged = False
     Z_hat = X
     Yn = None
     n_outer = 0
     for i in range(max_iter_harmony):
+        t0 = clock()
         km, Yn = clustering(Z_norm, R, E, O, Pr_b, cats, th, n_batches=n_batches, sigma=sigma,
                             block_size=block_size, max_iter=max_iter_clustering,
                             tol=tol_clustering,
@@ -370,6 +382,8 @@ def harmonize(Z, cats, n_batches, Y0, *, n_clusters=None, max_iter_harmony=10,
                             stabilized=stabilized_penalty)
         km_objs.append(km)
         objs.append(km[-1])
+        tm["clustering"] += clock() - t0
+        t0 = clock()
         lam = compute_lambda_kb(E, O, N_b, alpha=alpha, threshold=batch_prune_threshold,
                                 ridge_lambda=ridge_lambda, dynamic_lambda=dynamic_lambda)
         if correction_method == "original":
@@ -377,9 +391,12 @@ def harmonize(Z, cats, n_batches, Y0, *, n_clusters=None, max_iter_harmony=10,
         else:
             Z_hat = correction_batched(X, R, O, lam, cats, n_batches)
         Z_norm = l2_normalize(Z_hat)
+        tm["correction"] += clock() - t0
         n_outer = i + 1
         if len(objs) >= 2 and (objs[-2] - objs[-1]) < tol_harmony * abs(objs[-2]):
             converged = True
             break
+    if timings is not None:
+        timings.update(tm)
     return OracleResult(Z_hat=Z_hat, objectives_harmony=objs, kmeans_objectives=km_objs,
                         R=R, O=O, E=E, Y_norm=Yn, converged=converged, n_outer=n_outer)

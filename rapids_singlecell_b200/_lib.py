@@ -56,6 +56,8 @@ class HbParams(ctypes.Structure):
         ("dynamic_lambda", ctypes.c_int32),
         ("max_sweep_ctas", ctypes.c_int32),
         ("random_state", ctypes.c_uint64),
+        ("sweep_wait_ns", ctypes.c_int64),
+        ("test_unmet_arrivals", ctypes.c_int32),
     ]
 
 

@@ -181,6 +181,14 @@ int validate(const hb_params& p) {
   if (p.max_iter_harmony < 1) { set_error("max_iter_harmony must be >= 1"); return HB_ERR_INVALID; }
   if (p.max_iter_clustering < 0) { set_error("max_iter_clustering must be >= 0"); return HB_ERR_INVALID; }
   if (!(p.sigma > 0)) { set_error("sigma must be > 0"); return HB_ERR_INVALID; }
+  if (p.sweep_wait_ns < 0 || p.sweep_wait_ns > 60000000000LL) {
+    set_error("sweep_wait_ns must be in [0, 60 s]");
+    return HB_ERR_INVALID;
+  }
+  if (p.test_unmet_arrivals < 0 || p.test_unmet_arrivals > 1) {
+    set_error("test_unmet_arrivals must be 0 or 1");
+    return HB_ERR_INVALID;
+  }
   const int64_t nblk = (p.n_cells + p.block_size - 1) / p.block_size;
   if (nblk > kMaxBlocks) {
     set_error("block_proportion too small: %lld blocks per iteration (max %d)", (long long)nblk, kMaxBlocks);
@@ -417,6 +425,8 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
       sa.sigma = p.sigma; sa.d = d; sa.K = K; sa.B = B; sa.stabilized = p.stabilized_penalty;
       sa.init_mode = init; sa.batch_sorted = P->ml.nsub > 1 || B <= 1;
       sa.max_ctas = p.max_sweep_ctas; sa.barrier = w.barrier; sa.err = w.err;
+      sa.wait_ns = p.sweep_wait_ns > 0 ? (uint64_t)p.sweep_wait_ns : 2000000000ull;
+      sa.unmet = (unsigned)p.test_unmet_arrivals;
       sa.stop = sweep_stop; sa.it = sweep_it; sa.tol = p.tol_clustering;
       HB_CUDA(cudaMemsetAsync(w.barrier, 0, sizeof(unsigned), st));
       HB_TRY(launch_tc_sweep<S>(sa, st));

@@ -147,6 +147,8 @@ struct SweepArgs {
   int batch_sorted;        // the list is ordered by batch within each block
   int max_ctas;            // 0: one CTA per SM; otherwise at most this many CTAs
   unsigned* barrier;       // zero on entry
+  uint64_t wait_ns;        // bound of each grid-barrier wait
+  unsigned unmet;          // arrivals the barrier waits for beyond the grid's (test hook; 0)
   int* err;
   // device-side k-means stop (nullptr: none): the launch returns at once when *stop is set;
   // otherwise CTA 0 applies the window-3 test to obj_out[-it .. 0] and sets *stop = it + 1

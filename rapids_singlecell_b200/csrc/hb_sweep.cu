@@ -36,8 +36,9 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
 // Grid-wide barrier of a cooperative launch, split in two: arrive once this
 // CTA's writes of the block are issued, wait before the next block's counts are
 // read; work that does not depend on the other CTAs goes in between.  The wait
-// is bounded: after 2 s (or once any CTA has given up) the CTA records error 3
-// and proceeds (the host reports a timeout).
+// is bounded: after `limit_ns` (2 s unless the plan says otherwise), or once any
+// CTA has given up, the CTA records error 3 and proceeds (the host reports a
+// timeout).
 __device__ __forceinline__ void grid_arrive(unsigned* ctr) {
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -50,14 +51,14 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-__device__ __forceinline__ void grid_wait(unsigned* ctr, unsigned target, int* err) {
+__device__ __forceinline__ void grid_wait(unsigned* ctr, unsigned target, int* err, uint64_t limit_ns) {
   if (threadIdx.x == 0) {
     const uint64_t t0 = globaltimer_ns();
     unsigned spins = 0;
     while (ld_acquire_u32(ctr) < target) {
-      // give up after 2 s, or at once when another CTA has already given up
+      // give up after limit_ns, or at once when another CTA has already given up
       if ((++spins & 255u) == 0 &&
-          (globaltimer_ns() - t0 > 2000000000ull || *(volatile int*)err != 0)) {
+          (globaltimer_ns() - t0 > limit_ns || *(volatile int*)err != 0)) {
         atomicExch(err, 3);
         break;
       }
@@ -541,7 +542,7 @@ __global__ void __launch_bounds__(128 * QS * NG, 1) k_tc_sweep(SweepArgs a, Swee
       if (gt == 0) issue_similarity_mma(tmem, sA[buf], sB, L, idesc, mbar);
       pre_issued = true;
     }
-    grid_wait(a.barrier, (unsigned)(j + 1) * gridDim.x, a.err);
+    grid_wait(a.barrier, (unsigned)(j + 1) * (gridDim.x + a.unmet), a.err, a.wait_ns);
   }
 
   // ---- objective: diversity term from the final state (kernels_clustering.cuh:68-103)

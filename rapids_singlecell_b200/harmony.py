@@ -36,8 +36,11 @@ class HarmonyInfo:
 def make_params(n_cells, n_pcs, n_clusters, n_batches, *, precision="fp32", max_iter_harmony=10,
                 max_iter_clustering=200, tol_harmony=1e-4, tol_clustering=1e-5, ridge_lambda=1.0,
                 sigma=0.1, block_proportion=0.05, random_state=0, stabilized_penalty=True,
-                dynamic_lambda=True, alpha=0.2, batch_prune_threshold=1e-5, max_sweep_ctas=0) -> HbParams:
-    """The engine's plan parameters (``hb_params``) for one problem."""
+                dynamic_lambda=True, alpha=0.2, batch_prune_threshold=1e-5, max_sweep_ctas=0,
+                sweep_wait_ns=0, test_unmet_arrivals=0) -> HbParams:
+    """The engine's plan parameters (``hb_params``) for one problem.  ``sweep_wait_ns`` bounds each
+    grid-barrier wait of the 16-bit sweep (0: 2 s); ``test_unmet_arrivals`` is a test hook that
+    makes those waits run out (0 in normal use)."""
     p = HbParams()
     p.n_cells = int(n_cells)
     p.n_pcs = int(n_pcs)
@@ -58,6 +61,8 @@ def make_params(n_cells, n_pcs, n_clusters, n_batches, *, precision="fp32", max_
     p.dynamic_lambda = int(bool(dynamic_lambda))
     p.random_state = int(random_state) & 0xFFFFFFFFFFFFFFFF
     p.max_sweep_ctas = int(max_sweep_ctas)
+    p.sweep_wait_ns = int(sweep_wait_ns)
+    p.test_unmet_arrivals = int(test_unmet_arrivals)
     return p
 
 
@@ -76,7 +81,8 @@ class HarmonyProblem:
                  max_iter_harmony=10, max_iter_clustering=200, tol_harmony=1e-4,
                  tol_clustering=1e-5, ridge_lambda=1.0, sigma=0.1, block_proportion=0.05,
                  random_state=0, stabilized_penalty=True, dynamic_lambda=True, alpha=0.2,
-                 batch_prune_threshold=1e-5, stream=None, max_sweep_ctas=0):
+                 batch_prune_threshold=1e-5, stream=None, max_sweep_ctas=0, sweep_wait_ns=0,
+                 test_unmet_arrivals=0):
         self.lib = _lib.load()
         self.device = X.device
         self.X = X.contiguous()
@@ -103,7 +109,8 @@ class HarmonyProblem:
                         tol_harmony=tol_harmony, tol_clustering=tol_clustering, ridge_lambda=ridge_lambda,
                         sigma=sigma, block_proportion=block_proportion, random_state=random_state,
                         stabilized_penalty=stabilized_penalty, dynamic_lambda=dynamic_lambda, alpha=alpha,
-                        batch_prune_threshold=batch_prune_threshold, max_sweep_ctas=max_sweep_ctas)
+                        batch_prune_threshold=batch_prune_threshold, max_sweep_ctas=max_sweep_ctas,
+                        sweep_wait_ns=sweep_wait_ns, test_unmet_arrivals=test_unmet_arrivals)
         self.params = p
         self.plan = ctypes.c_void_p()
         _lib.check(self.lib.hb_plan_create(ctypes.byref(p), ctypes.byref(self.plan)))

@@ -45,11 +45,19 @@ def test_plan_validation_without_gpu():
     p.block_size = 50
     p.n_clusters = 300
     assert lib.hb_plan_create(ctypes.byref(p), ctypes.byref(plan)) == _lib.HB_ERR_UNSUPPORTED
+    p.n_clusters = 10
+    p.sweep_wait_ns = -1  # the grid-barrier wait bound must be in [0, 60 s]
+    assert lib.hb_plan_create(ctypes.byref(p), ctypes.byref(plan)) == _lib.HB_ERR_INVALID
+    assert b"sweep_wait_ns" in lib.hb_last_error()
+    p.sweep_wait_ns, p.test_unmet_arrivals = 0, 2  # the test hook takes 0 or 1
+    assert lib.hb_plan_create(ctypes.byref(p), ctypes.byref(plan)) == _lib.HB_ERR_INVALID
+    assert b"test_unmet_arrivals" in lib.hb_last_error()
 
 
 def test_struct_layout():
-    # hb_params: 8+4*4+8+4*2+8*6+4*4+8 = 112 bytes
-    assert ctypes.sizeof(_lib.HbParams) == 112
+    # hb_params: 8+4*4+8+4*2+8*6+4*4+8 = 112 bytes, then the wait bound (8) and the test hook
+    # (4, padded to 8)
+    assert ctypes.sizeof(_lib.HbParams) == 128
     assert ctypes.sizeof(_lib.HbOutputs) == 6 * ctypes.sizeof(ctypes.c_void_p)
     assert ctypes.sizeof(_lib.HbProfile) == 56
 

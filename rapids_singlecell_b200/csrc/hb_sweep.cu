@@ -39,12 +39,11 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
 // is bounded: after `limit_ns` (2 s unless the plan says otherwise), or once any
 // CTA has given up, the CTA records error 3 and proceeds (the host reports a
 // timeout).
+// The arrival is a release reduction: the CTA's writes of the block (ordered before it by the
+// CTA barrier) are visible to every CTA whose acquire load sees the count.
 __device__ __forceinline__ void grid_arrive(unsigned* ctr) {
   __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    atomicAdd(ctr, 1u);
-  }
+  if (threadIdx.x == 0) asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(ctr) : "memory");
 }
 __device__ __forceinline__ uint64_t globaltimer_ns() {
   uint64_t t;
@@ -62,12 +61,33 @@ __device__ __forceinline__ void grid_wait(unsigned* ctr, unsigned target, int* e
         atomicExch(err, 3);
         break;
       }
-      __nanosleep(32);
     }
-    __threadfence();
   }
+  // the acquire load above and this CTA barrier order the block's loads after every
+  // arrival's release (no further fence; polls back to back, each is an L2 round trip)
   __syncthreads();
 }
+
+// Profiling build only (-DHB_SWEEP_TRACE): per-phase timestamps of thread 0 of every CTA for
+// every block of the last sweep launch, %globaltimer (ns, comparable across SMs) and clock64
+// (cycles, this SM), read back with hb_debug_sweep_trace().  Compiled out otherwise.
+#ifdef HB_SWEEP_TRACE
+constexpr int kTraceCtas = 160, kTraceBlocks = 64, kTracePts = 12;
+__device__ uint64_t g_sweep_trace_ns[kTraceCtas * kTraceBlocks * kTracePts];
+__device__ uint64_t g_sweep_trace_clk[kTraceCtas * kTraceBlocks * kTracePts];
+#define HB_TRACE(j, pt)                                                                              \
+  do {                                                                                               \
+    if (threadIdx.x == 0 && blockIdx.x < kTraceCtas && (j) < kTraceBlocks) {                         \
+      const size_t at_ = ((size_t)blockIdx.x * kTraceBlocks + (j)) * kTracePts + (pt);               \
+      g_sweep_trace_ns[at_] = globaltimer_ns();                                                      \
+      g_sweep_trace_clk[at_] = (uint64_t)clock64();                                                  \
+    }                                                                                                \
+  } while (0)
+#else
+#define HB_TRACE(j, pt) \
+  do {                  \
+  } while (0)
+#endif
 
 // barrier of the `nthreads` threads of thread group g (named barrier 1 + g)
 __device__ __forceinline__ void group_sync(int g, int nthreads) {
@@ -84,7 +104,7 @@ struct SweepLayout {
   int ng;
   int nbuf;          // A tiles per group (2, or 1 when two do not fit)
   uint32_t atile;    // bytes of one A tile
-  uint32_t offA, offB, offRst, rstBytes, offPen, offOsm, osmBytes, offRows, offMisc, bytes;
+  uint32_t offA, offB, offRst, rstBytes, offPen, offOsm, osmBytes, offRows, offMisc, offBt, bytes;
 };
 
 inline SweepLayout sweep_layout(int d, int K, int B, int ldr, int ng, int nbuf) {
@@ -104,6 +124,7 @@ inline SweepLayout sweep_layout(int d, int K, int B, int ldr, int ng, int nbuf) 
   S.offOsm = al(o, 16); o = S.offOsm + (uint32_t)ng * S.osmBytes;
   S.offRows = al(o, 16); o = S.offRows + (uint32_t)ng * 4096u;  // cid, ccat [2][128]; rsp [<= 4][128]
   S.offMisc = al(o, 16); o = S.offMisc + 64u + 32u * 8u;
+  S.offBt = al(o, 16); o = S.offBt + (uint32_t)B * 8u;  // Pr_b and theta_b (float32)
   S.bytes = o + 1024u;  // slack for 1024-byte alignment of the base
   return S;
 }
@@ -184,17 +205,19 @@ __device__ __forceinline__ void stage_tile(const SweepArgs& a, TileIds t, int gt
   }
 }
 
-// ocol[k] += sum over batches b of (O[b][k] - Om[b][k]) (ocol zeroed by the caller):
-// the rows are split over the threads, np threads per column.
+// ocol[k] += sum over batches b of (O[b][k] - Om[b][k]) (ocol zeroed by the caller).  The
+// loads of the first 2 nt entries are issued together (one L2 round trip when B K <= 2 nt),
+// then added into ocol.
 __device__ __forceinline__ void column_sums(const double* O, const double* Om, int B, int K, float* ocol,
                                             int nt) {
-  const int np = K < nt ? nt / K : 1;
-  for (int t = threadIdx.x; t < np * K; t += nt) {
-    const int k = t % K, p = t / K;
-    double s = 0.0;
-    for (int b = p; b < B; b += np) s += O[(size_t)b * K + k] - (Om ? Om[(size_t)b * K + k] : 0.0);
-    atomicAdd(&ocol[k], (float)s);
-  }
+  const int ne = B * K;
+  double v0 = 0.0, v1 = 0.0;
+  const int e0 = threadIdx.x, e1 = threadIdx.x + nt;
+  if (e0 < ne) v0 = O[e0] - (Om ? Om[e0] : 0.0);
+  if (e1 < ne) v1 = O[e1] - (Om ? Om[e1] : 0.0);
+  if (e0 < ne) atomicAdd(&ocol[e0 % K], (float)v0);
+  if (e1 < ne) atomicAdd(&ocol[e1 % K], (float)v1);
+  for (int e = threadIdx.x + 2 * nt; e < ne; e += nt) atomicAdd(&ocol[e % K], (float)(O[e] - (Om ? Om[e] : 0.0)));
 }
 
 // Starts of the runs of equal batch in a tile (rows are ordered by batch inside
@@ -239,6 +262,8 @@ __global__ void __launch_bounds__(128 * QS * NG, 1) k_tc_sweep(SweepArgs a, Swee
   uint64_t* mbar = (uint64_t*)(sm + SL.offMisc) + g;
   uint32_t* tmem_slot = (uint32_t*)(sm + SL.offMisc + 32);
   double* red = (double*)(sm + SL.offMisc + 64);
+  float* prb = (float*)(sm + SL.offBt);  // [B] Pr_b, then [B] theta_b: read every block, so kept here
+  float* thb = prb + B;
   __shared__ float ocol_s[2][256];         // column sums of the state (E / Pr_b), by block parity
   __shared__ int2 crange[kMaxBlocks];      // batch range of this CTA's slice, per block
   __shared__ int2 gslice[NG][kMaxBlocks];  // each group's slice of every block (list positions)
@@ -266,6 +291,10 @@ __global__ void __launch_bounds__(128 * QS * NG, 1) k_tc_sweep(SweepArgs a, Swee
     tc::fence_mbar_init();
   }
   load_centroids_swizzled((const H*)a.Yn, a.ldy, K, sB, L);
+  for (int b = tid; b < B; b += NT) {
+    prb[b] = (float)a.Pr[b];
+    thb[b] = (float)a.theta[b];
+  }
   for (int e = tid; e < NG * a.nblk; e += NT) {
     const int gg = e / a.nblk, jj = e % a.nblk;
     int64_t lo, hi;
@@ -312,6 +341,7 @@ __global__ void __launch_bounds__(128 * QS * NG, 1) k_tc_sweep(SweepArgs a, Swee
   for (int k = tid; k < 256; k += NT) ocol_s[0][k] = 0.f;
   __syncthreads();
   for (int j = 0; j < a.nblk; ++j) {
+    HB_TRACE(j, 0);
     const double* Oin = a.Obuf[(a.b0 + j) % 3];
     double* Oout = a.Obuf[(a.b0 + j + 1) % 3];
     double* Ozero = a.Obuf[(a.b0 + j + 2) % 3];
@@ -347,6 +377,7 @@ __global__ void __launch_bounds__(128 * QS * NG, 1) k_tc_sweep(SweepArgs a, Swee
     if (carry_mine) carry_s[tid] = c_in - c_mc - c_mn;  // read back by this thread at the flush
     for (int k = tid; k < K; k += NT) ocol_s[(j + 1) & 1][k] = 0.f;
     __syncthreads();
+    HB_TRACE(j, 1);
     // exponent offsets of the batches present: v = exp2(c2 (1 - s) + log2 pen)
     // = exp2(pc - c2 s) with pc = c2 + theta_b log2((E+1)/(O[+E]+1)) (kernels_pen.cuh:8-21);
     // padding columns get a large negative offset (v = 0).  Zero the delta rows.
@@ -364,15 +395,16 @@ __global__ void __launch_bounds__(128 * QS * NG, 1) k_tc_sweep(SweepArgs a, Swee
           for (int i = 0; i < kPre; ++i)
             if (q == i) o = opre[i];
           if (q >= kPre) o = (float)(Oin[o_at] - (Omc ? Omc[o_at] : 0.0));
-          const float E = (float)a.Pr[b] * ocol[k];
+          const float E = prb[b] * ocol[k];
           const float denom = a.stabilized ? (o + E + 1.f) : (o + 1.f);
-          lp = (float)a.theta[b] * log2f((E + 1.f) / denom);
+          lp = thb[b] * log2f((E + 1.f) / denom);
         }
         pc = c2 + lp;
       }
       pen[(size_t)b * ldp + k] = pc;
     }
     __syncthreads();
+    HB_TRACE(j, 2);
     // ---- this group's tiles of the block ------------------------------------------
     while (have && cu.j == j) {
       if (!pre_issued) {
@@ -390,6 +422,7 @@ __global__ void __launch_bounds__(128 * QS * NG, 1) k_tc_sweep(SweepArgs a, Swee
       if (!tc::mbar_wait(mbar, phase, kMaxPolls)) atomicExch(a.err, 2);
       phase ^= 1u;
       tc::fence_after_sync();
+      HB_TRACE(j, 3);
       const int nvalid = tile_rows(cu);
       const int cell = cid[buf * 128 + row];
       const int cat = ccat[buf * 128 + row];
@@ -430,6 +463,7 @@ __global__ void __launch_bounds__(128 * QS * NG, 1) k_tc_sweep(SweepArgs a, Swee
       tc::tmem_st_wait();
       rsp[half * 128 + row] = rs;
       group_sync(g, GS);
+      HB_TRACE(j, 4);
       float rsum = 0.f;
 #pragma unroll
       for (int q = 0; q < QS; ++q) rsum += rsp[q * 128 + row];
@@ -465,6 +499,7 @@ __global__ void __launch_bounds__(128 * QS * NG, 1) k_tc_sweep(SweepArgs a, Swee
       // copies of the next tile (its ids have landed by now)
       if (have_nx) stage_tile<H>(a, tn, gt, sA[buf ^ 1], L.dpad, cid + (buf ^ 1) * 128, ccat + (buf ^ 1) * 128, QS);
       group_sync(g, GS);
+      HB_TRACE(j, 5);
       // the new assignment rows: one bulk store per row (ldr 16-bit values).  The last
       // tile of the block stores its rows after the grid arrival, while the other CTAs
       // finish the block (nothing reads R during the sweep).
@@ -503,6 +538,7 @@ __global__ void __launch_bounds__(128 * QS * NG, 1) k_tc_sweep(SweepArgs a, Swee
       cu = nx;
     }
     // ---- flush the CTA's deltas and carry the state ------------------------------
+    HB_TRACE(j, 6);
     __syncthreads();
     for (int e = tid; e < (cmax - cmin + 1) * K; e += NT) {
       const size_t o_at = (size_t)cmin * K + e;
@@ -523,7 +559,9 @@ __global__ void __launch_bounds__(128 * QS * NG, 1) k_tc_sweep(SweepArgs a, Swee
       const double tot = block_sum(obj_local, red);
       if (tid == 0 && tot != 0.0) atomicAdd(a.obj_acc, tot);
     }
+    HB_TRACE(j, 7);
     grid_arrive(a.barrier);
+    HB_TRACE(j, 8);
     if (pend_rows > 0) {  // coalesced 16-byte stores: consecutive threads on consecutive chunks of a row
       const int nch = a.ldr / 8;
       for (int e = gt; e < pend_rows * nch; e += GS) {
@@ -542,7 +580,9 @@ __global__ void __launch_bounds__(128 * QS * NG, 1) k_tc_sweep(SweepArgs a, Swee
       if (gt == 0) issue_similarity_mma(tmem, sA[buf], sB, L, idesc, mbar);
       pre_issued = true;
     }
+    HB_TRACE(j, 9);
     grid_wait(a.barrier, (unsigned)(j + 1) * (gridDim.x + a.unmet), a.err, a.wait_ns);
+    HB_TRACE(j, 10);
   }
 
   // ---- objective: diversity term from the final state (kernels_clustering.cuh:68-103)
@@ -643,3 +683,14 @@ template int launch_tc_sweep<__half>(const SweepArgs&, cudaStream_t);
 template int launch_tc_sweep<__nv_bfloat16>(const SweepArgs&, cudaStream_t);
 
 }  // namespace hb
+
+#ifdef HB_SWEEP_TRACE
+// [kTraceCtas][kTraceBlocks][kTracePts] timestamps of the last sweep (profiling build only)
+extern "C" __attribute__((visibility("default"))) int hb_debug_sweep_trace(uint64_t* ns, uint64_t* clk,
+                                                                           size_t count) {
+  const size_t n = std::min(count, (size_t)hb::kTraceCtas * hb::kTraceBlocks * hb::kTracePts);
+  if (cudaMemcpyFromSymbol(ns, hb::g_sweep_trace_ns, n * sizeof(uint64_t)) != cudaSuccess) return 4;
+  if (cudaMemcpyFromSymbol(clk, hb::g_sweep_trace_clk, n * sizeof(uint64_t)) != cudaSuccess) return 4;
+  return 0;
+}
+#endif

@@ -195,6 +195,48 @@ HB_API int hb_kmeans_init(const float* X, int64_t n, int32_t n_pcs, int32_t n_cl
                           double tol, uint64_t seed, float* Y_out, int32_t* n_iter_out, void* workspace,
                           size_t workspace_bytes, void* stream);
 
+/* ---- PCA by the covariance eigendecomposition (preprocessing/_pca.py:339-353 ->
+ * preprocessing/_sparse_pca/_sparse_pca.py:26-127): Gram matrix and column sums on the tensor
+ * core, covariance, and the projection onto the leading components.  The eigendecomposition of
+ * the n_genes x n_genes covariance is left to the caller (the reference calls cp.linalg.eigh,
+ * _sparse_pca.py:47). ---- */
+
+/* gram[i][j] = sum_r X[r][i] X[r][j] (float64 [n_genes][n_genes], both triangles) and
+ * col_sums[i] = sum_r X[r][i] (float64 [n_genes]) of a dense float32 X [n][ldx] (device).  Each
+ * float32 value enters the bf16 tensor-core products as hi + lo parts (about 16 significant
+ * bits), accumulated in float32 per 128-row tile run and summed in float64.  Replaces the Gram
+ * build of _create_gram_matrix (_sparse_pca.py:202-248; gram_csr_upper_kernel,
+ * _cuda/spca/kernels_spca.cuh:5-28) and the column means of _get_mean_var
+ * (preprocessing/_utils.py:88-105).  n_genes <= 32768.  Synchronises the stream once. */
+HB_API size_t hb_pca_gram_workspace_bytes(int64_t n, int32_t n_genes);
+HB_API int hb_pca_gram(const float* X, int64_t n, int32_t n_genes, int64_t ldx, double* gram, double* col_sums,
+                       void* workspace, size_t workspace_bytes, void* stream);
+
+/* cov = gram / n - mean mean^T with mean = col_sums / n (zero_center != 0), or cov = gram
+ * (zero_center == 0, the reference's uncentred path); float64 [n_genes][n_genes]; mean
+ * (optional, float64 [n_genes]) receives the column means.  Replaces _compute_cov and
+ * cov_from_gram_kernel (_sparse_pca/_helper.py:21-32; _cuda/spca/kernels_spca.cuh:48-62). */
+HB_API int hb_pca_covariance(const double* gram, const double* col_sums, int64_t n, int32_t n_genes,
+                             int32_t zero_center, double* cov, double* mean, void* stream);
+
+/* X_pca[r][c] = sum_g X[r][g] components[c][g] - (mean ? sum_g mean[g] components[c][g] : 0),
+ * float32 [n][n_comps]; components float32 [n_comps][n_genes] (device), mean float64 [n_genes]
+ * or NULL.  X and the components enter the bf16 tensor-core products as hi + lo parts.
+ * n_comps <= 256.  Replaces PCA_sparse._transform_cupy (_sparse_pca.py:84-95).  Synchronises the
+ * stream once. */
+HB_API size_t hb_pca_project_workspace_bytes(int32_t n_genes, int32_t n_comps);
+HB_API int hb_pca_project(const float* X, int64_t n, int32_t n_genes, int64_t ldx, const float* components,
+                          int32_t n_comps, const double* mean, float* X_pca, void* workspace,
+                          size_t workspace_bytes, void* stream);
+
+/* Dense float32 copy out[r][c] (row stride ldo, zero where no entry is stored) of a CSR matrix
+ * (indptr int64 [n_rows + 1], indices int32, data float32; device).  *err (device int32, set
+ * to zero by the call) flags a column index outside [0, n_cols) -> HB_ERR_INVALID.  The sparse
+ * input of the reference's covariance PCA (csr_matrix, _sparse_pca.py:202-214) enters the
+ * dense Gram and projection kernels through this copy. */
+HB_API int hb_csr_to_dense(const int64_t* indptr, const int32_t* indices, const float* data, int64_t n_rows,
+                           int32_t n_cols, float* out, int64_t ldo, int32_t* err, void* stream);
+
 HB_API const char* hb_last_error(void);
 HB_API const char* hb_version(void);
 

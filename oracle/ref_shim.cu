@@ -2,8 +2,9 @@
 //
 // This file is compiled by oracle/Makefile together with rapids_singlecell's
 // kernel headers, read in place from the reference source tree
-// (src/rapids_singlecell/_cuda/harmony/*/kernels_*.cuh and
-// src/rapids_singlecell/_cuda/cublas_helpers.cuh), into oracle/_ref/libharmony_ref.so.
+// (src/rapids_singlecell/_cuda/harmony/*/kernels_*.cuh, _cuda/spca/kernels_spca.cuh,
+// _cuda/mean_var/kernels_mv.cuh and _cuda/cublas_helpers.cuh), into
+// oracle/_ref/libharmony_ref.so.
 // The reference's nanobind modules (*.cu) cannot be built here (nanobind is not
 // installed), so this shim replays their launch sequences -- grid and block
 // shapes, GEMM calls and kernel order -- around the unmodified kernels.  The
@@ -22,6 +23,9 @@
 //   ref_colsum              preprocessing/_harmony/_helper.py:310-361 with
 //                           _cuda/harmony/colsum/colsum.cu:14-55
 //   ref_outer               _cuda/harmony/outer/outer.cu:10-19
+//   ref_pca_cov_csr         preprocessing/_sparse_pca/_sparse_pca.py:138-199 (_cov_sparse) with
+//                           _cuda/spca/spca.cu:12-44, _cuda/mean_var/mean_var.cu:24-31 and
+//                           preprocessing/_utils.py:88-105 (the column means)
 //
 // Every entry point returns 0 on success or a CUDA / cuBLAS error code (negated
 // for cuBLAS); ref_last_error() gives the message.
@@ -46,6 +50,8 @@
 #include "harmony/outer/kernels_outer.cuh"
 #include "harmony/pen/kernels_pen.cuh"
 #include "harmony/scatter/kernels_scatter.cuh"
+#include "mean_var/kernels_mv.cuh"
+#include "spca/kernels_spca.cuh"
 
 namespace {
 
@@ -407,7 +413,56 @@ void colsum(const T* A, T* out, int rows, int cols, int algo, cudaStream_t st) {
   }
 }
 
+// _cov_sparse (_sparse_pca.py:138-199) of a float32 CSR matrix with int32 indices:
+// gram_csr_upper -> copy_upper_to_lower; the column means in float64 by mean_var_minor
+// (_utils.py:88-105) cast to float32; gram *= 1 / n; cov_from_gram.  return_gram: the raw
+// Gram (not scaled, no mean).  cov: float32 [ncols][ncols]; mean: float32 [ncols].
+void pca_cov_csr(const int* indptr, const int* indices, const float* data, int nrows, int ncols, long long nnz,
+                 int return_gram, float* cov, float* mean, cudaStream_t st) {
+  cuda_ok(cudaMemsetAsync(cov, 0, sizeof(float) * (size_t)ncols * ncols, st), "memset");
+  gram_csr_upper_kernel<float, int><<<strided_grid(nrows, 1), 128, 0, st>>>(indptr, indices, data, nrows, ncols, cov);
+  launched("gram_csr_upper_kernel");
+  const dim3 mb(32, 32), mg(strided_grid(ncols, 32), strided_grid(ncols, 32));
+  copy_upper_to_lower_kernel<float><<<mg, mb, 0, st>>>(cov, ncols);
+  launched("copy_upper_to_lower_kernel");
+  if (return_gram) {
+    cuda_ok(cudaStreamSynchronize(st), "sync");
+    return;
+  }
+  Scratch ws;
+  double* m64 = ws.get<double>(ncols);
+  double* v64 = ws.get<double>(ncols);
+  cuda_ok(cudaMemsetAsync(m64, 0, sizeof(double) * ncols, st), "memset");
+  cuda_ok(cudaMemsetAsync(v64, 0, sizeof(double) * ncols, st), "memset");
+  if (nnz > 0) {
+    mean_var_minor_kernel<float, int><<<strided_grid(nnz, 256), 256, 0, st>>>(indices, data, m64, v64, nnz);
+    launched("mean_var_minor_kernel");
+  }
+  std::vector<double> h(ncols);
+  cuda_ok(cudaMemcpyAsync(h.data(), m64, sizeof(double) * ncols, cudaMemcpyDeviceToHost, st), "D2H");
+  cuda_ok(cudaStreamSynchronize(st), "sync");
+  std::vector<float> hm(ncols);
+  for (int i = 0; i < ncols; ++i) hm[i] = (float)(h[i] / nrows);  // mean /= major; .astype(x.dtype)
+  cuda_ok(cudaMemcpyAsync(mean, hm.data(), sizeof(float) * ncols, cudaMemcpyHostToDevice, st), "H2D");
+  // gram_matrix *= 1 / x.shape[0] (float32 array times a Python float)
+  std::vector<float> g((size_t)ncols * ncols);
+  cuda_ok(cudaMemcpyAsync(g.data(), cov, sizeof(float) * g.size(), cudaMemcpyDeviceToHost, st), "D2H");
+  cuda_ok(cudaStreamSynchronize(st), "sync");
+  const float inv = (float)(1.0 / (double)nrows);
+  for (float& x : g) x *= inv;
+  cuda_ok(cudaMemcpyAsync(cov, g.data(), sizeof(float) * g.size(), cudaMemcpyHostToDevice, st), "H2D");
+  cov_from_gram_kernel<float><<<mg, mb, 0, st>>>(cov, cov, mean, mean, ncols);
+  launched("cov_from_gram_kernel");
+  cuda_ok(cudaStreamSynchronize(st), "sync");
+}
+
 }  // namespace
+
+extern "C" int ref_pca_cov_csr_f32(const int* indptr, const int* indices, const float* data, int nrows, int ncols,
+                                   long long nnz, int return_gram, float* cov, float* mean, void* stream) {
+  return guarded([&] { pca_cov_csr(indptr, indices, data, nrows, ncols, nnz, return_gram, cov, mean,
+                                   (cudaStream_t)stream); });
+}
 
 #define REF_BOTH(NAME, ARGS_T, CALL)                                                      \
   extern "C" int NAME##_f32 ARGS_T(float) { return guarded([&] { CALL(float); }); }       \

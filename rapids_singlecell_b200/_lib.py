@@ -31,6 +31,8 @@ EXPORTED = (
     "hb_l2_normalize", "hb_block_lists_workspace_bytes", "hb_block_lists", "hb_block_lists_static",
     "hb_penalty",
     "hb_lambda_kb", "hb_ridge_inverse", "hb_similarity", "hb_kmeans_workspace_bytes", "hb_kmeans_init",
+    "hb_pca_gram_workspace_bytes", "hb_pca_gram", "hb_pca_covariance", "hb_pca_project_workspace_bytes",
+    "hb_pca_project", "hb_csr_to_dense",
     "hb_last_error", "hb_version",
 )
 
@@ -143,6 +145,20 @@ def load() -> ctypes.CDLL:
     lib.hb_kmeans_init.argtypes = [c_void_p, c_i64, c_i32, c_i32, c_i32, ctypes.c_double, ctypes.c_uint64,
                                    c_void_p, P(c_i32), c_void_p, c_size, c_void_p]
     lib.hb_kmeans_init.restype = c_int
+    lib.hb_pca_gram_workspace_bytes.argtypes = [c_i64, c_i32]
+    lib.hb_pca_gram_workspace_bytes.restype = c_size
+    lib.hb_pca_gram.argtypes = [c_void_p, c_i64, c_i32, c_i64, c_void_p, c_void_p, c_void_p, c_size, c_void_p]
+    lib.hb_pca_gram.restype = c_int
+    lib.hb_pca_covariance.argtypes = [c_void_p, c_void_p, c_i64, c_i32, c_i32, c_void_p, c_void_p, c_void_p]
+    lib.hb_pca_covariance.restype = c_int
+    lib.hb_pca_project_workspace_bytes.argtypes = [c_i32, c_i32]
+    lib.hb_pca_project_workspace_bytes.restype = c_size
+    lib.hb_pca_project.argtypes = [c_void_p, c_i64, c_i32, c_i64, c_void_p, c_i32, c_void_p, c_void_p,
+                                   c_void_p, c_size, c_void_p]
+    lib.hb_pca_project.restype = c_int
+    lib.hb_csr_to_dense.argtypes = [c_void_p, c_void_p, c_void_p, c_i64, c_i32, c_void_p, c_i64, c_void_p,
+                                    c_void_p]
+    lib.hb_csr_to_dense.restype = c_int
     lib.hb_last_error.argtypes = []
     lib.hb_last_error.restype = ctypes.c_char_p
     lib.hb_version.argtypes = []

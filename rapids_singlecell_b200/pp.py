@@ -125,3 +125,6 @@ def harmony_integrate(
         init_centroids=init_centroids, precision=precision,
     )
     adata.obsm[adjusted_basis] = Z_hat.cpu().numpy()
+
+
+from .pca import pp_pca as pca  # noqa: E402  (``pp.pca``, the drop-in for rapids_singlecell.pp.pca)

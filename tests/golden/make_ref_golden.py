@@ -9,7 +9,8 @@ then checks the NumPy oracle against these outputs on any machine (no GPU).
     make -C oracle && python tests/golden/make_ref_golden.py [--out DIR]
 
 Inputs are seeded draws of the repository's mixture generator at small sizes, so the
-fixtures stay small (about 2 MB together).
+fixtures stay small (about 2 MB together).  The PCA cases (``ref_pca_*.npz``) run the
+reference's covariance PCA kernels on a seeded sparse matrix (``oracle/ref_pca.py``).
 """
 
 from __future__ import annotations
@@ -49,6 +50,43 @@ CASES = {
 }
 
 
+def pca_input(seed=5, n=3000, g=240, rank=8):
+    """A sparse, log-normalised-looking cells x genes matrix with a low-rank structure: Poisson
+    counts of a rank-`rank` factor model at low depth (about a quarter of the entries nonzero),
+    log1p; every gene expressed in at least one cell."""
+    import scipy.sparse as sp
+
+    rng = np.random.default_rng(seed)
+    F = rng.gamma(2.0, 1.0, (n, rank))
+    L = rng.gamma(0.6, 1.0, (rank, g)) * rng.uniform(0.2, 3.0, g)
+    lam = F @ L / rank
+    counts = rng.poisson(lam * rng.uniform(0.05, 0.3, (n, 1)))
+    counts[rng.integers(0, n, g), np.arange(g)] += 1  # no all-zero gene
+    X = sp.csr_matrix(np.log1p(counts).astype(np.float32))
+    X.sort_indices()
+    return X
+
+
+PCA_CASES = {"pca_center": dict(zero_center=True, n_comps=20), "pca_gram": dict(zero_center=False, n_comps=12)}
+
+
+def run_pca_case(name, out_dir: Path) -> Path:
+    from oracle import ref_pca
+
+    X = pca_input()
+    kw = PCA_CASES[name]
+    X_pca, comps, var, ratio, mean = ref_pca.pca_csr(X.indptr, X.indices, X.data, X.shape, kw["n_comps"],
+                                                      zero_center=kw["zero_center"])
+    arrays = dict(indptr=X.indptr.astype(np.int64), indices=X.indices.astype(np.int32), data=X.data,
+                  shape=np.asarray(X.shape), params=np.array(json.dumps(kw)), X_pca=X_pca, components=comps,
+                  variance=var, variance_ratio=ratio)
+    if mean is not None:
+        arrays["mean"] = mean
+    path = out_dir / f"ref_{name}.npz"
+    np.savez_compressed(path, **arrays)
+    return path
+
+
 def run_case(name, out_dir: Path) -> Path:
     from oracle import ref_harmony as rh
 
@@ -77,11 +115,16 @@ def run_case(name, out_dir: Path) -> Path:
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--out", default=str(Path(__file__).resolve().parent))
-    ap.add_argument("--cases", nargs="*", default=list(CASES))
+    ap.add_argument("--cases", nargs="*", default=list(CASES) + list(PCA_CASES))
     args = ap.parse_args()
     out = Path(args.out)
     out.mkdir(parents=True, exist_ok=True)
     for name in args.cases:
+        if name in PCA_CASES:
+            path = run_pca_case(name, out)
+            with np.load(path) as f:
+                print(f"{path.name}: variance={np.round(f['variance'][:6], 4).tolist()}")
+            continue
         path = run_case(name, out)
         with np.load(path) as f:
             print(f"{path.name}: n_outer={int(f['n_outer'])} kmeans_iters={f['kmeans_iters'].tolist()} "

@@ -237,6 +237,27 @@ HB_API int hb_pca_project(const float* X, int64_t n, int32_t n_genes, int64_t ld
 HB_API int hb_csr_to_dense(const int64_t* indptr, const int32_t* indices, const float* data, int64_t n_rows,
                            int32_t n_cols, float* out, int64_t ldo, int32_t* err, void* stream);
 
+/* ---- exact k nearest neighbours (the brute-force search of pp.neighbors,
+ * preprocessing/_neighbors/_algorithms/_brute.py:14-37, a cuML NearestNeighbors(algorithm="brute")
+ * call in the reference) ---- */
+#define HB_KNN_SQEUCLIDEAN 0
+#define HB_KNN_EUCLIDEAN 1     /* also "l2" */
+#define HB_KNN_COSINE 2        /* 1 - cosine similarity */
+#define HB_KNN_INNER_PRODUCT 3 /* similarity, largest first */
+
+/* For each of n_queries float32 rows (device, [n_queries][n_dims]) the k nearest of n_data rows
+ * (device, [n_data][n_dims]); indices int64 [n_queries][k] and distances float32 [n_queries][k]
+ * (device), ascending by distance then index.  Dot products run on the tensor core as bf16 hi + lo
+ * parts; each query's best candidates are re-ranked with exact float32 distances (difference form
+ * for the euclidean metrics).  Pass the same pointer and count for queries and data for a kNN
+ * graph (the call of pp.neighbors, _neighbors/__init__.py:223-230).  n_dims <= 128, k <= 56
+ * (k <= 24 above 64 dims).  Synchronises the stream once. */
+HB_API size_t hb_knn_workspace_bytes(int64_t n_queries, int64_t n_data, int32_t n_dims, int32_t same,
+                                     int32_t metric);
+HB_API int hb_knn(const float* queries, int64_t n_queries, const float* data, int64_t n_data, int32_t n_dims,
+                  int32_t k, int32_t metric, int64_t* indices, float* distances, void* workspace,
+                  size_t workspace_bytes, void* stream);
+
 HB_API const char* hb_last_error(void);
 HB_API const char* hb_version(void);
 

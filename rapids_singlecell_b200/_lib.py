@@ -23,6 +23,7 @@ HB_ERR_INTERNAL = 5
 HB_ERR_UNSUPPORTED = 6
 
 HB_FP32, HB_FP64, HB_BF16, HB_FP16 = 0, 1, 2, 3
+HB_KNN_SQEUCLIDEAN, HB_KNN_EUCLIDEAN, HB_KNN_COSINE, HB_KNN_INNER_PRODUCT = 0, 1, 2, 3
 PRECISIONS = {"fp32": HB_FP32, "fp64": HB_FP64, "bf16": HB_BF16, "fp16": HB_FP16}
 
 # every symbol include/harmony_b200.h declares
@@ -32,7 +33,7 @@ EXPORTED = (
     "hb_penalty",
     "hb_lambda_kb", "hb_ridge_inverse", "hb_similarity", "hb_kmeans_workspace_bytes", "hb_kmeans_init",
     "hb_pca_gram_workspace_bytes", "hb_pca_gram", "hb_pca_covariance", "hb_pca_project_workspace_bytes",
-    "hb_pca_project", "hb_csr_to_dense",
+    "hb_pca_project", "hb_csr_to_dense", "hb_knn_workspace_bytes", "hb_knn",
     "hb_last_error", "hb_version",
 )
 
@@ -159,6 +160,11 @@ def load() -> ctypes.CDLL:
     lib.hb_csr_to_dense.argtypes = [c_void_p, c_void_p, c_void_p, c_i64, c_i32, c_void_p, c_i64, c_void_p,
                                     c_void_p]
     lib.hb_csr_to_dense.restype = c_int
+    lib.hb_knn_workspace_bytes.argtypes = [c_i64, c_i64, c_i32, c_i32, c_i32]
+    lib.hb_knn_workspace_bytes.restype = c_size
+    lib.hb_knn.argtypes = [c_void_p, c_i64, c_void_p, c_i64, c_i32, c_i32, c_i32, c_void_p, c_void_p, c_void_p,
+                           c_size, c_void_p]
+    lib.hb_knn.restype = c_int
     lib.hb_last_error.argtypes = []
     lib.hb_last_error.restype = ctypes.c_char_p
     lib.hb_version.argtypes = []

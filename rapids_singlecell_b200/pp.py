@@ -128,3 +128,4 @@ def harmony_integrate(
 
 
 from .pca import pp_pca as pca  # noqa: E402  (``pp.pca``, the drop-in for rapids_singlecell.pp.pca)
+from .neighbors import pp_neighbors as neighbors  # noqa: E402  (``pp.neighbors``, the drop-in for rapids_singlecell.pp.neighbors)

@@ -51,10 +51,11 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="bf16", choices=["bf16", "fp16", "fp32"])
     ap.add_argument("--no-plain", action="store_true")
-    ap.add_argument("--sections", default="wide,batched,serving",
+    ap.add_argument("--sections", default="wide,batched,serving,pca,knn",
                     help="extra measurements on rank 0 beside the headline line: wide (the "
                          "2M-cell x 100-PC workload), batched (256 independent problems), "
-                         "serving (Poisson request stream); empty for none")
+                         "serving (Poisson request stream), pca (500k x 2000 covariance PCA), "
+                         "knn (500k x 50 exact kNN); empty for none")
     ap.add_argument("--profile-case", action="store_true",
                     help="one short run for ncu: the same workload for 1 outer x 2 k-means "
                          "iterations, then exit")
@@ -429,10 +430,130 @@ def serving_section(dev, n_requests=64, rates=(10.0, 100.0), fp32_rate=10.0, str
     return out
 
 
+def _events_ms(fn, reps=3):
+    """Median device time of fn() (CUDA events on the current stream) after one warm-up."""
+    import torch
+
+    fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return float(np.median(ts))
+
+
+def _tensor_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["bf16_tflops"]), "measured"
+    return 1590.0, "fallback"
+
+
+def pca_section(dev, n=500_000, g=2000, n_comps=50):
+    """PCA upstream of Harmony: a seeded 500,000-cell x 2,000-gene log-normalised-looking matrix
+    (rank-20 gamma factor model, Poisson counts, log1p; about 14 % nonzero) generated on the
+    device, dense float32 in HBM.  Times the Gram kernel (X^T X and column sums), the projection
+    onto 50 components, and the whole covariance PCA; the Gram against cuBLAS float32
+    (torch.matmul(X.T, X), the GEMM a dense float32 PCA runs) on the same matrix."""
+    import ctypes
+
+    import torch
+
+    from rapids_singlecell_b200 import _lib
+    from rapids_singlecell_b200.pca import pca_arrays
+
+    lib = _lib.load()
+    gen = torch.Generator(device=dev).manual_seed(11)
+    F = torch.distributions.Gamma(2.0, 1.0).sample((n, 20)).to(dev)
+    L = torch.rand((20, g), generator=gen, device=dev) ** 3 * 0.6
+    X = torch.log1p(torch.poisson(F @ L * 0.15, generator=gen)).contiguous()
+    del F, L
+    density = float((X != 0).float().mean().item())
+    st = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    ws_bytes = lib.hb_pca_gram_workspace_bytes(n, g)
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
+    G = torch.empty((g, g), dtype=torch.float64, device=dev)
+    cs = torch.empty(g, dtype=torch.float64, device=dev)
+
+    def gram():
+        _lib.check(lib.hb_pca_gram(ctypes.c_void_p(X.data_ptr()), n, g, g, ctypes.c_void_p(G.data_ptr()),
+                                   ctypes.c_void_p(cs.data_ptr()), ctypes.c_void_p(ws.data_ptr()), ws_bytes, st))
+
+    ms_gram = _events_ms(gram)
+    ms_cublas = _events_ms(lambda: torch.matmul(X.T, X))
+    G32 = torch.matmul(X.T.double(), X.double()) if n * g <= 2_000_000_000 else None
+    err = float(((G - G32).abs().max() / G32.abs().max()).item()) if G32 is not None else None
+    err32 = float(((torch.matmul(X.T, X).double() - G32).abs().max() / G32.abs().max()).item()) if G32 is not None else None
+    del G32, ws
+    res = {}
+    ms_pca = _events_ms(lambda: res.update(r=pca_arrays(X, n_comps)), reps=2)
+    comps = res["r"].components
+    pws_bytes = lib.hb_pca_project_workspace_bytes(g, n_comps)
+    pws = torch.empty(pws_bytes, dtype=torch.uint8, device=dev)
+    out = torch.empty((n, n_comps), dtype=torch.float32, device=dev)
+    mean = res["r"].mean
+
+    def project():
+        _lib.check(lib.hb_pca_project(ctypes.c_void_p(X.data_ptr()), n, g, g, ctypes.c_void_p(comps.data_ptr()),
+                                      n_comps, ctypes.c_void_p(mean.data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                                      ctypes.c_void_p(pws.data_ptr()), pws_bytes, st))
+
+    ms_proj = _events_ms(project)
+    peak_t, kind_t = _tensor_peak()
+    peak_h, kind_h = measured_peaks()
+    useful = float(n) * g * (g + 1)  # one multiply-add per (i <= j) entry and row
+    issued = 3.0 * 2.0 * n * (128 * 128) * ((g + 127) // 128) * ((g + 127) // 128 + 1) / 2  # bf16 MMA flops
+    proj_bytes = float(n) * g * 4 + float(n) * n_comps * 4
+    return {"workload": f"{n} cells x {g} genes float32 (density {density:.3f}), {n_comps} components, "
+                        "covariance eigendecomposition",
+            "pca_ms": ms_pca,
+            "gram": {"kernel": "k_pca_gram + k_pca_reduce", "ms": ms_gram,
+                     "useful_tflops": useful / ms_gram / 1e9, "issued_bf16_tflops": issued / ms_gram / 1e9,
+                     "roofline": {"bound": "tensor", "achieved": issued / ms_gram / 1e9, "peak": peak_t,
+                                  "unit": "TFLOP/s", "frac": issued / ms_gram / 1e9 / peak_t, "peak_kind": kind_t,
+                                  "note": "achieved = bf16 MMA flops issued (3 hi/lo products of the upper "
+                                          "triangle of 128 x 128 blocks)"},
+                     "rel_max_abs_err_vs_float64": err},
+            "cublas_fp32_gram_ms": ms_cublas, "cublas_fp32_rel_max_abs_err_vs_float64": err32,
+            "speedup_gram_vs_cublas_fp32": ms_cublas / ms_gram,
+            "project": {"kernel": "k_pca_project", "ms": ms_proj,
+                        "roofline": {"bound": "hbm", "achieved": proj_bytes / ms_proj / 1e6, "peak": peak_h,
+                                     "unit": "GB/s", "frac": proj_bytes / ms_proj / 1e6 / peak_h,
+                                     "peak_kind": kind_h, "algorithmic_bytes": proj_bytes}}}
+
+
+def knn_section(dev, n=500_000, d=50, k=15):
+    """kNN graph of the corrected embedding: the 500,000-cell x 50-PC mixture (the Harmony
+    workload's input), exact brute force, k = 15, euclidean."""
+    import torch
+
+    from rapids_singlecell_b200.neighbors import knn_arrays
+    from rapids_singlecell_b200.synthetic import make_config
+
+    Z = torch.as_tensor(make_config(WORKLOAD, seed=0)["Z"][:n, :d], device=dev)
+    ms = _events_ms(lambda: knn_arrays(Z, k), reps=2)
+    peak_t, kind_t = _tensor_peak()
+    dpad = 64 if d <= 64 else 128
+    tiles = (n + 127) // 128
+    issued = 3.0 * 2.0 * (tiles * 128.0) ** 2 * dpad
+    return {"workload": f"{n} x {d} float32, k={k}, euclidean, exact brute force", "ms": ms,
+            "queries_per_s": n / (ms / 1e3), "distances_per_s": float(n) * n / (ms / 1e3),
+            "roofline": {"bound": "tensor", "achieved": issued / ms / 1e9, "peak": peak_t, "unit": "TFLOP/s",
+                         "frac": issued / ms / 1e9 / peak_t, "peak_kind": kind_t,
+                         "note": "achieved = bf16 MMA flops issued (3 hi/lo products of every 128 x 128 "
+                                 "query-data tile pair over the padded 64 dimensions)"}}
+
+
 def run_sections(args, dev):
     out = {}
     for name in [s for s in args.sections.split(",") if s]:
-        fn = {"wide": wide_section, "batched": batched_section, "serving": serving_section}[name]
+        fn = {"wide": wide_section, "batched": batched_section, "serving": serving_section,
+              "pca": pca_section, "knn": knn_section}[name]
         t0 = time.perf_counter()
         try:
             out[name] = fn(dev)

@@ -73,112 +73,159 @@ __device__ __forceinline__ void list_insert(float* ld, int* li, float dist, int 
   thr = ld[(KC - 1) * 256];
 }
 
-template <int KC>
+// NB = 2: two data-tile buffers and two TMEM accumulators, so the MMA of data tile t+1 runs
+// while the epilogue of tile t reads its dot products (and tile t+2 loads); NB = 1 when shared
+// memory holds one data tile only (128 dimensions, or the 64-entry candidate lists).
+template <int KC, int NB>
 __global__ void __launch_bounds__(256, 1) k_knn_search(KnnArgs a) {
   extern __shared__ __align__(1024) unsigned char smem_dyn[];
   unsigned char* sm = (unsigned char*)(((uintptr_t)smem_dyn + 1023) & ~(uintptr_t)1023);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int kblk = a.dpad / 64;
-  const uint32_t atile = (uint32_t)kblk * 16384u;  // 128 rows x dpad bf16
-  const uint32_t oAh = 0, oAl = atile, oBh = 2 * atile, oBl = 3 * atile;
-  const uint32_t oNrm = 4 * atile;                  // [2][128] data-tile norms
-  const uint32_t oLd = oNrm + 1024, oLi = oLd + (uint32_t)KC * 256u * 4u;
-  const uint32_t oMisc = oLi + (uint32_t)KC * 256u * 4u;
+  const uint32_t atile = (uint32_t)kblk * 16384u;   // 128 rows x dpad bf16
+  const uint32_t oAh = 0, oAl = atile, oB = 2 * atile;  // data buffer b: hi at oB + 2 b atile, lo after
+  const uint32_t oNrm = oB + 2u * NB * atile;        // [4][128] data-tile norms (tile t in slot t & 3)
+  const uint32_t oLd = oNrm + 2048, oLi = oLd + (uint32_t)KC * 256u * 4u;
+  const uint32_t oSt = oLi + (uint32_t)KC * 256u * 4u;  // [8][256] staged distances, then ids
+  const uint32_t oMisc = oSt + 8u * 256u * 8u;
   float* nrm_s = (float*)(sm + oNrm);
   float* ld = (float*)(sm + oLd) + tid;
   int* li = (int*)(sm + oLi) + tid;
-  uint64_t* mbar = (uint64_t*)(sm + oMisc);
-  uint32_t* tmem_slot = (uint32_t*)(sm + oMisc + 8);
+  float* sd = (float*)(sm + oSt) + tid;
+  int* si = (int*)(sm + oSt + 8u * 256u * 4u) + tid;
+  uint64_t* mbar = (uint64_t*)(sm + oMisc);          // [NB]
+  uint32_t* tmem_slot = (uint32_t*)(sm + oMisc + 16);
   const uint32_t sm32 = tc::smem_u32(sm);
   const int64_t q0 = (int64_t)blockIdx.x * 128;
+  const int64_t ntiles = (a.nx + 127) / 128;
   if (warp == 0) {
-    tc::tmem_alloc(tmem_slot, 128u);
+    tc::tmem_alloc(tmem_slot, 128u * NB);
     tc::tmem_relinquish();
     tc::fence_before_sync();
   }
   if (tid == 0) {
-    tc::mbar_init(mbar, 1);
+    for (int b = 0; b < NB; ++b) tc::mbar_init(mbar + b, 1);
     tc::fence_mbar_init();
   }
-  // query tile (A) and the first data tile (B): rows of dpad bf16, K-major, 128B swizzle
+  // rows of dpad bf16, K-major, 128B swizzle; rows are padded to whole tiles
   const int nch = a.dpad / 8;
   auto load_rows = [&](uint32_t dst_h, uint32_t dst_l, const __nv_bfloat16* Sh, const __nv_bfloat16* Sl,
                        int64_t r0) {
     for (int e = tid; e < 128 * nch; e += 256) {
       const int r = e / nch, ch = e % nch;
       const uint32_t off = (uint32_t)(ch >> 3) * 16384u + tc::sw128_off((uint32_t)r, (uint32_t)(ch & 7));
-      const size_t src = (size_t)(r0 + r) * a.dpad + ch * 8;  // rows padded to whole tiles
+      const size_t src = (size_t)(r0 + r) * a.dpad + ch * 8;
       tc::cp_async16(sm32 + dst_h + off, Sh + src, 16u);
       tc::cp_async16(sm32 + dst_l + off, Sl + src, 16u);
     }
   };
+  auto load_tile = [&](int64_t tt) {  // data tile tt into buffer tt % NB, its norms into slot tt & 3
+    const uint32_t bh = oB + 2u * (uint32_t)(tt % NB) * atile;
+    load_rows(bh, bh + atile, a.Xh, a.Xl, tt * 128);
+    if (tid < 128) nrm_s[(tt & 3) * 128 + tid] = a.xn[tt * 128 + tid];
+  };
   load_rows(oAh, oAl, a.Qh, a.Ql, q0);
-  load_rows(oBh, oBl, a.Xh, a.Xl, 0);
-  if (tid < 128) nrm_s[tid] = a.xn[tid];
+  load_tile(0);
+  if (NB == 2 && ntiles > 1) load_tile(1);
   for (int i = 0; i < KC; ++i) {
     ld[i * 256] = INFINITY;
     li[i * 256] = -1;
   }
   float thr = INFINITY;
+  tc::cp_async_wait_all();
+  tc::fence_proxy_async_smem();
+  tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t tmem = *tmem_slot;
   const uint32_t idesc = tc::idesc_f16(128, 128, true, false, false);
-  const int row = (warp & 3) * 32 + lane, half = warp >> 2;
-  const uint32_t tl = tmem + ((uint32_t)((warp & 3) * 32) << 16);
-  const int64_t q = q0 + row;
-  const float qnorm = q < a.nq ? a.qn[q] : 0.f;
-  const bool dot_metric = a.metric == kKnnCosine || a.metric == kKnnInner;
-  const int64_t ntiles = (a.nx + 127) / 128;
-  for (int64_t t = 0; t < ntiles; ++t) {
+  auto issue = [&](int64_t tt) {  // thread 0: D[b] = Q . X_tile^T, three hi / lo products
+    const int b = (int)(tt % NB);
+    const uint32_t bh = sm32 + oB + 2u * (uint32_t)b * atile;
+    const int nks = a.dpad / 16;
+    for (int s = 0; s < nks; ++s) {
+      const uint32_t o = (uint32_t)(s >> 2) * 16384u + (uint32_t)(s & 3) * 32u;
+      const uint64_t ah = tc::sdesc_sw128(sm32 + oAh + o, 16, 1024), al = tc::sdesc_sw128(sm32 + oAl + o, 16, 1024);
+      const uint64_t xh = tc::sdesc_sw128(bh + o, 16, 1024), xl = tc::sdesc_sw128(bh + atile + o, 16, 1024);
+      const uint32_t d = tmem + (uint32_t)(b * 128);
+      tc::mma_f16(d, ah, xh, idesc, s > 0 ? 1u : 0u);
+      tc::mma_f16(d, ah, xl, idesc, 1u);
+      tc::mma_f16(d, al, xh, idesc, 1u);
+    }
+    tc::mma_commit(mbar + b);
+  };
+  auto join = [&]() {  // loads landed, the epilogue's TMEM reads done, then the next MMA may run
     tc::cp_async_wait_all();
     tc::fence_proxy_async_smem();
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
-    if (tid == 0) {
-      const int nks = a.dpad / 16;
-      for (int s = 0; s < nks; ++s) {
-        const uint32_t o = (uint32_t)(s >> 2) * 16384u + (uint32_t)(s & 3) * 32u;
-        const uint64_t ah = tc::sdesc_sw128(sm32 + oAh + o, 16, 1024), al = tc::sdesc_sw128(sm32 + oAl + o, 16, 1024);
-        const uint64_t bh = tc::sdesc_sw128(sm32 + oBh + o, 16, 1024), bl = tc::sdesc_sw128(sm32 + oBl + o, 16, 1024);
-        tc::mma_f16(tmem, ah, bh, idesc, s > 0 ? 1u : 0u);
-        tc::mma_f16(tmem, ah, bl, idesc, 1u);
-        tc::mma_f16(tmem, al, bh, idesc, 1u);
-      }
-      tc::mma_commit(mbar);
-    }
-    if (!tc::mbar_wait(mbar, (uint32_t)(t & 1), kMaxPolls)) atomicExch(a.err, 8);
+  };
+  const int row = (warp & 3) * 32 + lane, half = warp >> 2;
+  const uint32_t tl = tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(half * 64);
+  const int64_t q = q0 + row;
+  const bool live = q < a.nq;
+  const float qnorm = live ? a.qn[q] : 0.f;
+  const bool dot_metric = a.metric == kKnnCosine || a.metric == kKnnInner;
+  if (tid == 0) issue(0);
+  for (int64_t t = 0; t < ntiles; ++t) {
+    const int b = (int)(t % NB);
+    if (!tc::mbar_wait(mbar + b, (uint32_t)((t / NB) & 1), kMaxPolls)) atomicExch(a.err, 8);
     tc::fence_after_sync();
-    // the data tile's operands are free: load the next one while this epilogue runs
-    const float* nrm_cur = nrm_s + (t & 1) * 128;
-    if (t + 1 < ntiles) {
-      load_rows(oBh, oBl, a.Xh, a.Xl, (t + 1) * 128);
-      if (tid < 128) nrm_s[((t + 1) & 1) * 128 + tid] = a.xn[(t + 1) * 128 + tid];
+    if (NB == 2) {
+      if (t + 1 < ntiles) {  // its operands loaded during the previous epilogue: start its MMA
+        join();
+        if (tid == 0) issue(t + 1);
+      }
+      if (t + 2 < ntiles) load_tile(t + 2);  // into the buffer tile t has finished with
+    } else if (t + 1 < ntiles) {
+      load_tile(t + 1);
     }
+    // epilogue: the thread's 64 columns in one wait (tcgen05.ld is warp-collective: every lane
+    // loads, lanes past the last query skip the lists)
+    float v[8][8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) tc::tmem_ld8(tl + (uint32_t)(b * 128 + 8 * c), v[c]);
+    tc::tmem_ld_wait();
+    // fast pass, eight candidates at a time: the ones below the thread's threshold are staged
+    // (no branch); the sorted lists are only touched when some lane of the warp staged one
     {
-      // tcgen05.ld is warp-collective: every lane loads, lanes past the last query skip the lists
-      const int64_t base = t * 128 + half * 64;
-      const bool live = q < a.nq;
-      for (int c0 = 0; c0 < 64; c0 += 8) {
-        float v[8];
-        tc::tmem_ld8(tl + (uint32_t)(half * 64 + c0), v);
-        tc::tmem_ld_wait();
-        if (!live) continue;
+      const float* nr = nrm_s + (t & 3) * 128 + half * 64;
+      const int base = (int)(t * 128) + half * 64;
+      const int nvalid = (int)min((int64_t)64, a.nx - (int64_t)base);  // candidates of this half
+      // dist < thr  <=>  key < thr - |q|^2 with key = |x|^2 - 2 q.x (euclidean), -q.x (dot)
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        const float4 n0 = *(const float4*)(nr + 8 * c), n1 = *(const float4*)(nr + 8 * c + 4);
+        const float nn[8] = {n0.x, n0.y, n0.z, n0.w, n1.x, n1.y, n1.z, n1.w};
+        const float lim = dot_metric ? thr : thr - qnorm;
+        int cnt = 0;
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
-          const int64_t cand = base + c0 + i;
-          if (cand >= a.nx) break;
-          const float dist = dot_metric ? -v[i] : fmaf(-2.f, v[i], qnorm + nrm_cur[half * 64 + c0 + i]);
-          if (dist < thr) list_insert<KC>(ld, li, dist, (int)cand, thr);
+          const float key = dot_metric ? -v[c][i] : fmaf(-2.f, v[c][i], nn[i]);
+          const bool take = live && key < lim && 8 * c + i < nvalid;
+          if (take) {
+            sd[cnt * 256] = dot_metric ? key : key + qnorm;
+            si[cnt * 256] = base + 8 * c + i;
+          }
+          cnt += take ? 1 : 0;
         }
+        if (__any_sync(0xffffffffu, cnt > 0))
+          for (int e = 0; e < cnt; ++e) {
+            const float dd = sd[e * 256];
+            if (dd < thr) list_insert<KC>(ld, li, dd, si[e * 256], thr);
+          }
       }
     }
     tc::fence_before_sync();
+    if (NB == 1 && t + 1 < ntiles) {
+      join();
+      if (tid == 0) issue(t + 1);
+    }
   }
   __syncthreads();
   // exact re-rank: thread `row` (half 0) takes both halves' candidates of its query
-  if (half == 0 && q < a.nq) {
+  if (half == 0 && live) {
     float bd[64];
     int bi[64];
     const int kk = a.k;
@@ -188,12 +235,10 @@ __global__ void __launch_bounds__(256, 1) k_knn_search(KnnArgs a) {
     }
     const float* qrow = a.Q + q * a.d;
     for (int h = 0; h < 2; ++h) {
-      const float* cd = (const float*)(sm + oLd) + h * 128 + row;
       const int* ci = (const int*)(sm + oLi) + h * 128 + row;
       for (int i = 0; i < KC; ++i) {
         const int id = ci[i * 256];
         if (id < 0) continue;
-        (void)cd;
         const float* xr = a.X + (int64_t)id * a.d;
         float acc = 0.f;
         if (dot_metric) {
@@ -230,7 +275,7 @@ __global__ void __launch_bounds__(256, 1) k_knn_search(KnnArgs a) {
   __syncthreads();
   if (warp == 0) {
     tc::fence_after_sync();
-    tc::tmem_dealloc(tmem, 128u);
+    tc::tmem_dealloc(tmem, 128u * NB);
   }
 }
 
@@ -325,16 +370,16 @@ HB_API int hb_knn(const float* queries, int64_t n_queries, const float* data, in
   KnnArgs a{cosine ? Qc : queries, cosine ? Xc : data, Qh, Ql, Xh, Xl, qn, xn, n_queries, n_data, n_dims,
             P.dpad, k, metric, indices, distances, err};
   const int KC = k <= 24 ? 32 : 64;
+  const int NB = (KC == 32 && P.dpad == 64) ? 2 : 1;  // two data tiles fit beside the 32-entry lists
   const uint32_t atile = (uint32_t)(P.dpad / 64) * 16384u;
-  const size_t smem = 4 * (size_t)atile + 1024 + 2 * (size_t)KC * 256 * 4 + 64 + 1024;
+  const size_t smem = (2 + 2 * (size_t)NB) * atile + 2048 + 2 * (size_t)KC * 256 * 4 + 8 * 256 * 8 + 64 + 1024;
   const unsigned grid = (unsigned)((n_queries + 127) / 128);
-  if (KC == 32) {
-    HB_TRY(allow_max_dyn_smem((const void*)k_knn_search<32>));
-    k_knn_search<32><<<grid, 256, smem, st>>>(a);
-  } else {
-    HB_TRY(allow_max_dyn_smem((const void*)k_knn_search<64>));
-    k_knn_search<64><<<grid, 256, smem, st>>>(a);
-  }
+  const void* fn = KC == 64 ? (const void*)k_knn_search<64, 1>
+                            : (NB == 2 ? (const void*)k_knn_search<32, 2> : (const void*)k_knn_search<32, 1>);
+  HB_TRY(allow_max_dyn_smem(fn));
+  if (KC == 64) k_knn_search<64, 1><<<grid, 256, smem, st>>>(a);
+  else if (NB == 2) k_knn_search<32, 2><<<grid, 256, smem, st>>>(a);
+  else k_knn_search<32, 1><<<grid, 256, smem, st>>>(a);
   HB_LAUNCH_CHECK();
   int h_err = 0;
   HB_CUDA(cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, st));

@@ -10,8 +10,12 @@
 //                  128-row tiles of X read once, split into bf16 hi + lo parts
 //                  (x = hi + lo to ~16 significant bits) and staged MN-major;
 //                  D[i][j] += hi_i hi_j + hi_i lo_j + lo_i hi_j on tcgen05 with the
-//                  float32 accumulator in TMEM over the CTA's rows; diagonal blocks
-//                  also sum their columns in float64 (the means).
+//                  float32 accumulator in TMEM, drained into the CTA's float64 partial
+//                  every kDrainTiles row tiles: the tensor core's float32 accumulation
+//                  rounds with a bias, so its error grows with the length of the chain
+//                  (one chain over 100,000 rows measured 9e-4 relative; 2,048 rows keep it
+//                  near the hi/lo split's 1e-5); diagonal blocks also sum their columns in
+//                  float64 (the means).
 //   k_pca_reduce   float64 sum of the row-split partials into the full symmetric
 //                  Gram matrix and the column sums.
 //   k_pca_cov      cov = G / n - mean mean^T in float64.
@@ -24,7 +28,8 @@
 namespace hb {
 namespace {
 
-constexpr int kGB = 128;  // genes per Gram block (M = N = 128)
+constexpr int kGB = 128;          // genes per Gram block (M = N = 128)
+constexpr int kDrainTiles = 16;   // 128-row tiles per float32 accumulation chain in TMEM
 
 // byte offset of 16-byte chunk c8 of 64-element block nb in row r of an MN-major,
 // 128-byte-swizzled tile with `nblocks` 64-element blocks per 8-row group
@@ -59,7 +64,7 @@ struct GramArgs {
   int64_t n, ldx;
   int g, nI, T, S;
   int vec;          // rows 16-byte aligned: float4 loads
-  float* Gpart;     // [S][T][128][128]
+  double* Gpart;    // [S][T][128][128] float64 partials
   double* Cpart;    // [S][nI][128] column sums (written by the diagonal blocks)
   int* err;
 };
@@ -112,6 +117,22 @@ __global__ void __launch_bounds__(256, 1) k_pca_gram(GramArgs a) {
   double cs[8];
 #pragma unroll
   for (int i = 0; i < 8; ++i) cs[i] = 0.0;
+  // D[i][j] -> Gpart[s][t][i][j] (float64): warps 0-3 columns 0..63, warps 4-7 columns 64..127
+  const int dm = (warp & 3) * 32 + lane, dc_lo = (warp >> 2) * 64;
+  const uint32_t dtl = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+  double* dout = a.Gpart + ((size_t)s * a.T + t) * (kGB * kGB) + (size_t)dm * kGB;
+  auto drain = [&](bool add) {
+    for (int c0 = dc_lo; c0 < dc_lo + 64; c0 += 8) {
+      float v[8];
+      tc::tmem_ld8(dtl + (uint32_t)c0, v);
+      tc::tmem_ld_wait();
+#pragma unroll
+      for (int i = 0; i < 8; ++i) dout[c0 + i] = add ? dout[c0 + i] + (double)v[i] : (double)v[i];
+    }
+  };
+  auto zero_partial = [&]() {
+    for (int c0 = dc_lo; c0 < dc_lo + 64; ++c0) dout[c0] = 0.0;
+  };
   int it = 0;
   for (int64_t base = r0; base < r1; base += 128, ++it) {
 #pragma unroll 2
@@ -147,7 +168,7 @@ __global__ void __launch_bounds__(256, 1) k_pca_gram(GramArgs a) {
         const uint32_t o = (uint32_t)ks * 2u * 2u * 1024u;
         const uint64_t ah = tc::sdesc_sw128(ah0 + o, 1024, 2048), al = tc::sdesc_sw128(al0 + o, 1024, 2048);
         const uint64_t bh = tc::sdesc_sw128(bh0 + o, 1024, 2048), bl = tc::sdesc_sw128(bl0 + o, 1024, 2048);
-        tc::mma_f16(tmem, ah, bh, idesc, (it > 0 || ks > 0) ? 1u : 0u);
+        tc::mma_f16(tmem, ah, bh, idesc, (it % kDrainTiles > 0 || ks > 0) ? 1u : 0u);
         tc::mma_f16(tmem, ah, bl, idesc, 1u);
         tc::mma_f16(tmem, al, bh, idesc, 1u);
       }
@@ -156,24 +177,11 @@ __global__ void __launch_bounds__(256, 1) k_pca_gram(GramArgs a) {
     // the operands are rewritten by the next row tile: wait for the MMAs
     if (!tc::mbar_wait(mbar, (uint32_t)(it & 1), kMaxPolls)) atomicExch(a.err, 8);
     tc::fence_after_sync();
+    // end of a chain (or of the rows): D is added into the float64 partial and the next
+    // tile's first MMA starts a new chain (the loop-top barrier orders these loads before it)
+    if (it % kDrainTiles == kDrainTiles - 1 || base + 128 >= r1) drain(it >= kDrainTiles);
   }
-  // D[i][j] -> Gpart[s][t][i][j]: warps 0-3 columns 0..63, warps 4-7 columns 64..127
-  {
-    const int m = (warp & 3) * 32 + lane;
-    const int c_lo = (warp >> 2) * 64;
-    const uint32_t tl = tmem + ((uint32_t)((warp & 3) * 32) << 16);
-    float* out = a.Gpart + ((size_t)s * a.T + t) * (kGB * kGB) + (size_t)m * kGB;
-    for (int c0 = c_lo; c0 < c_lo + 64; c0 += 8) {
-      float v[8];
-      tc::tmem_ld8(tl + (uint32_t)c0, v);
-      tc::tmem_ld_wait();
-      if (it == 0)
-#pragma unroll
-        for (int i = 0; i < 8; ++i) v[i] = 0.f;
-      *(float4*)(out + c0) = make_float4(v[0], v[1], v[2], v[3]);
-      *(float4*)(out + c0 + 4) = make_float4(v[4], v[5], v[6], v[7]);
-    }
-  }
+  if (it == 0) zero_partial();
   if (diag) {  // column sums of block I: 16 threads per 8-gene chunk
     double* red = (double*)(sm + kGramRed);
 #pragma unroll
@@ -194,7 +202,7 @@ __global__ void __launch_bounds__(256, 1) k_pca_gram(GramArgs a) {
 }
 
 // G[i][j] = G[j][i] = sum over splits of the partial of the upper block pair (float64)
-__global__ void k_pca_reduce(const float* __restrict__ Gpart, const double* __restrict__ Cpart, int g, int nI,
+__global__ void k_pca_reduce(const double* __restrict__ Gpart, const double* __restrict__ Cpart, int g, int nI,
                              int T, int S, double* __restrict__ G, double* __restrict__ csum) {
   const int64_t ne = (int64_t)g * g;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += (int64_t)gridDim.x * blockDim.x) {
@@ -203,7 +211,7 @@ __global__ void k_pca_reduce(const float* __restrict__ Gpart, const double* __re
     const int I = i / kGB, J = j / kGB;
     const size_t at = (size_t)tile_of(I, J, nI) * kGB * kGB + (size_t)(i % kGB) * kGB + (j % kGB);
     double v = 0.0;
-    for (int q = 0; q < S; ++q) v += (double)Gpart[(size_t)q * T * kGB * kGB + at];
+    for (int q = 0; q < S; ++q) v += Gpart[(size_t)q * T * kGB * kGB + at];
     G[(size_t)i * g + j] = v;
     G[(size_t)j * g + i] = v;
   }
@@ -392,9 +400,9 @@ GramPlan gram_plan(int64_t n, int g) {
   const int sms = num_sms();
   int64_t S = std::max<int64_t>(1, (4 * sms + P.T - 1) / P.T);
   S = std::min<int64_t>(S, std::max<int64_t>(1, n / 512));
-  while (S > 1 && (size_t)S * P.T * kGB * kGB * 4 > ((size_t)2 << 30)) --S;
+  while (S > 1 && (size_t)S * P.T * kGB * kGB * 8 > ((size_t)2 << 30)) --S;
   P.S = (int)S;
-  P.part_bytes = align_up((size_t)P.S * P.T * kGB * kGB * 4, 256);
+  P.part_bytes = align_up((size_t)P.S * P.T * kGB * kGB * 8, 256);
   P.cpart_bytes = align_up((size_t)P.S * P.nI * kGB * 8, 256);
   P.err_off = P.part_bytes + P.cpart_bytes;
   P.bytes = P.err_off + 256;
@@ -433,7 +441,7 @@ HB_API int hb_pca_gram(const float* X, int64_t n, int32_t n_genes, int64_t ldx, 
   int* err = (int*)(ws + P.err_off);
   HB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
   GramArgs a{X, n, ldx, n_genes, P.nI, P.T, P.S, ((uintptr_t)X % 16 == 0 && ldx % 4 == 0) ? 1 : 0,
-             (float*)ws, (double*)(ws + P.part_bytes), err};
+             (double*)ws, (double*)(ws + P.part_bytes), err};
   HB_TRY(allow_max_dyn_smem((const void*)k_pca_gram));
   k_pca_gram<<<P.T * P.S, 256, kGramSmem, st>>>(a);
   HB_LAUNCH_CHECK();

@@ -133,6 +133,7 @@ struct Work {
   AccumChunk* m_chunks;
   int32_t* batch_chunk_off;
   ApplyTile* apply_tiles;
+  void* pen_g;      // plain paths: [B][K] penalty table in global memory (many batches)
   MembershipBufs mb;
   MembershipBufs mb1;
 };
@@ -167,6 +168,7 @@ void carve(const hb_plan& P, Carver& cv, Work& w) {
   w.m_chunks = cv.take<AccumChunk>(P.max_m_chunks);
   w.batch_chunk_off = cv.take<int32_t>(B + 1);
   w.apply_tiles = cv.take<ApplyTile>(P.max_apply_tiles);
+  w.pen_g = P.ssz == 2 ? nullptr : (void*)cv.take<char>((size_t)B * K * P.ssz);
   membership_carve(cv, P.ml, w.mb);
   w.cell_index = cv.take<int32_t>((size_t)n);
   membership_carve(cv, P.ml1, w.mb1);
@@ -205,9 +207,16 @@ int validate(const hb_params& p) {
     set_error("n_pcs=%d exceeds 128 for the tensor-core path", p.n_pcs);
     return HB_ERR_UNSUPPORTED;
   }
-  const size_t smem = (size_t)(p.precision == HB_FP64 ? 8 : 4) * 2 * p.n_batches * p.n_clusters;
-  if (smem > 160 * 1024) {
-    set_error("n_batches * n_clusters = %d too large (shared-memory O/penalty tables)", p.n_batches * p.n_clusters);
+  // the 16-bit sweep keeps its penalty and delta tables in shared memory; the plain paths
+  // switch to global tables (k_pen_table, direct atomics) when theirs do not fit
+  const size_t smem = (size_t)4 * 2 * p.n_batches * p.n_clusters;
+  if ((p.precision == HB_BF16 || p.precision == HB_FP16) && smem > 160 * 1024) {
+    set_error("n_batches * n_clusters = %d too large for the tensor-core sweep's shared-memory tables; "
+              "use precision fp32 or fp64", p.n_batches * p.n_clusters);
+    return HB_ERR_UNSUPPORTED;
+  }
+  if ((size_t)16 * p.n_batches > 200 * 1024) {
+    set_error("n_batches=%d exceeds 12800 (ridge solve tables)", p.n_batches);
     return HB_ERR_UNSUPPORTED;
   }
   if (MembershipLayout ml = membership_layout(p.n_cells, p.block_size, 1); ml.cap > 16384) {
@@ -402,6 +411,7 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
   base.Zn = Zn; base.ldz = P->ldz; base.R = R; base.ldr = P->ldr; base.cats = cats;
   base.Yn = Yn; base.ldy = P->ldy; base.Pr = w.Pr; base.theta = w.theta; base.obj_acc = w.obj_acc;
   base.sigma = p.sigma; base.d = d; base.K = K; base.B = B; base.stabilized = p.stabilized_penalty;
+  base.pen_g = w.pen_g;
 
   // ---- initial state (_harmony/__init__.py:292-353) ------------------------
   // padding rows of Z_norm and R (read by the tile loads of the streaming centroid pass) are zero

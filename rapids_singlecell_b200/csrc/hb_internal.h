@@ -102,6 +102,8 @@ struct BlockArgs {
   int d, K, B;
   int stabilized;
   int init_mode;        // no penalty, L1 clamp 1e-12 (initial R)
+  void* pen_g;          // [B][K] of the storage type: the penalty table in global memory, used when
+                        // the B x K tables do not fit in shared memory (many batches)
 };
 int launch_block_update_f32(const BlockArgs& a, const double* O_in, double* O_out, double* O_zero,
                             cudaStream_t st);

@@ -291,7 +291,33 @@ struct BlockArgsDev {
   double* O_zero;
 };
 
-template <typename T, int KPT>
+// Penalty table in global memory for the many-batch form of the block update: one CTA per
+// cluster column k sums the state's column (E / Pr_b) in float64, then writes pen[b][k] for
+// every batch (kernels_pen.cuh:8-21), as the in-kernel table below does.
+template <typename T>
+__global__ void k_pen_table(BlockArgsDev p, T* __restrict__ pen) {
+  __shared__ double red[32];
+  const BlockArgs& a = p.a;
+  const int K = a.K, B = a.B, k = blockIdx.x;
+  double s = 0.0;
+  for (int b = threadIdx.x; b < B; b += blockDim.x) {
+    const size_t e = (size_t)b * K + k;
+    s += p.O_in[e] - (a.Om_cur ? a.Om_cur[e] : 0.0);
+  }
+  const double col = block_sum(s, red);
+  for (int b = threadIdx.x; b < B; b += blockDim.x) {
+    const size_t e = (size_t)b * K + k;
+    const T o = (T)(p.O_in[e] - (a.Om_cur ? a.Om_cur[e] : 0.0));
+    const T E = (T)(a.Pr[b] * col);
+    const T denom = a.stabilized ? (o + E + T(1)) : (o + T(1));
+    pen[e] = num<T>::pow_((E + T(1)) / denom, (T)a.theta[b]);
+  }
+}
+
+// GT (global tables): the penalty table comes from k_pen_table and the observed-count deltas
+// go straight to O_out with float64 atomics, so shared memory holds no B x K table and any
+// number of batches fits.
+template <typename T, int KPT, bool GT>
 __global__ void __launch_bounds__(BU_THREADS) k_block_update(BlockArgsDev p) {
   constexpr int DC = bu_dc<T>();
   constexpr int K16 = 16 * KPT;
@@ -300,9 +326,10 @@ __global__ void __launch_bounds__(BU_THREADS) k_block_update(BlockArgsDev p) {
   const BlockArgs& a = p.a;
   const int K = a.K, B = a.B, d = a.d;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* pen = (T*)smem_raw;                       // [B][K]
-  T* osm = pen + (size_t)B * K;                // [B][K]
-  T* zt = osm + (size_t)B * K;                 // [TM][DC+1]
+  const size_t tab = GT ? 0 : (size_t)B * K;
+  T* pen = GT ? (T*)a.pen_g : (T*)smem_raw;    // [B][K]
+  T* osm = (T*)smem_raw + tab;                 // [B][K] (shared-table form)
+  T* zt = (T*)smem_raw + 2 * tab;              // [TM][DC+1]
   T* yt = zt + BU_TM * (DC + 1);               // [K16][DC+1]
   int64_t* cid = (int64_t*)(yt + (size_t)K16 * (DC + 1));  // [TM]
   int* ccat = (int*)(cid + BU_TM);             // [TM]
@@ -318,7 +345,7 @@ __global__ void __launch_bounds__(BU_THREADS) k_block_update(BlockArgsDev p) {
     for (int e = blockIdx.x * BU_THREADS + tid; e < B * K; e += gridDim.x * BU_THREADS) p.O_zero[e] = 0.0;
 
   // penalty table from the current state (kernels_pen.cuh:8-21)
-  if (a.n_new > 0 && !a.init_mode) {
+  if (!GT && a.n_new > 0 && !a.init_mode) {
     double* ocol = (double*)zt;  // scratch: K doubles fit in zt + yt
     for (int k = tid; k < K; k += BU_THREADS) {
       double s = 0;
@@ -337,7 +364,8 @@ __global__ void __launch_bounds__(BU_THREADS) k_block_update(BlockArgsDev p) {
       pen[e] = num<T>::pow_((E + T(1)) / denom, (T)a.theta[b]);
     }
   }
-  for (int e = tid; e < B * K; e += BU_THREADS) osm[e] = T(0);
+  if (!GT)
+    for (int e = tid; e < B * K; e += BU_THREADS) osm[e] = T(0);
   __syncthreads();
 
   const T term = T(-2) / (T)a.sigma;
@@ -456,7 +484,8 @@ __global__ void __launch_bounds__(BU_THREADS) k_block_update(BlockArgsDev p) {
           const int k = kg + 16 * j;
           if (k < K) {
             Rrow[k] = v[j];
-            atomicAdd(&osm[cat * K + k], v[j]);
+            if (GT) atomicAdd(&p.O_out[(size_t)cat * K + k], (double)v[j]);
+            else atomicAdd(&osm[cat * K + k], v[j]);
           } else if (k < a.ldr) {
             Rrow[k] = T(0);
           }
@@ -468,7 +497,8 @@ __global__ void __launch_bounds__(BU_THREADS) k_block_update(BlockArgsDev p) {
 
   __syncthreads();
   for (int e = tid; e < B * K; e += BU_THREADS) {
-    double v = (double)osm[e];
+    if (GT && blockIdx.x != 0) break;  // the deltas are in O_out already; CTA 0 carries the state
+    double v = GT ? 0.0 : (double)osm[e];
     if (blockIdx.x == 0) {
       // this CTA also carries the state forward: O_in - old(this block) - old(next block)
       if (p.O_in) v += p.O_in[e];
@@ -481,26 +511,40 @@ __global__ void __launch_bounds__(BU_THREADS) k_block_update(BlockArgsDev p) {
   if (tid == 0 && tot != 0.0) atomicAdd(a.obj_acc, tot);
 }
 
+template <typename T, int KPT, bool GT>
+static int launch_block_form(const BlockArgsDev& p, size_t smem, cudaStream_t st) {
+  const BlockArgs& a = p.a;
+  const void* fn = (const void*)k_block_update<T, KPT, GT>;
+  HB_TRY(allow_max_dyn_smem(fn));
+  int occ = 1;
+  HB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_block_update<T, KPT, GT>, BU_THREADS, smem));
+  if (occ < 1) occ = 1;
+  const int64_t tiles = (a.n_new + BU_TM - 1) / BU_TM;
+  int grid = (int)std::min<int64_t>(std::max<int64_t>(tiles, 1), (int64_t)num_sms() * occ);
+  if (GT && a.n_new > 0 && !a.init_mode) {
+    k_pen_table<T><<<a.K, 256, 0, st>>>(p, (T*)a.pen_g);
+    HB_LAUNCH_CHECK();
+  }
+  k_block_update<T, KPT, GT><<<grid, BU_THREADS, smem, st>>>(p);
+  HB_LAUNCH_CHECK();
+  return HB_OK;
+}
+
+// Shared-memory tables while they fit (the O deltas of a CTA summed on chip); global tables
+// and direct float64 atomics for more batches.
 template <typename T, int KPT>
 static int launch_block_kpt(const BlockArgsDev& p, cudaStream_t st) {
   const BlockArgs& a = p.a;
   constexpr int DC = bu_dc<T>();
-  const size_t smem = sizeof(T) * ((size_t)2 * a.B * a.K + BU_TM * (DC + 1) +
-                                    (size_t)16 * KPT * (DC + 1)) +
+  const size_t base = sizeof(T) * (BU_TM * (DC + 1) + (size_t)16 * KPT * (DC + 1)) +
                       BU_TM * (sizeof(int64_t) + sizeof(int)) + 64;
-  if (smem > 227 * 1024) {
-    set_error("block update: B*K too large for shared memory (B=%d K=%d)", a.B, a.K);
-    return HB_ERR_UNSUPPORTED;
+  const size_t tables = sizeof(T) * (size_t)2 * a.B * a.K;
+  if (base + tables <= 160 * 1024) return launch_block_form<T, KPT, false>(p, base + tables, st);
+  if (!a.pen_g) {
+    set_error("block update: no global penalty table for B=%d K=%d", a.B, a.K);
+    return HB_ERR_INTERNAL;
   }
-  HB_TRY(allow_max_dyn_smem((const void*)k_block_update<T, KPT>));
-  int occ = 1;
-  HB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_block_update<T, KPT>, BU_THREADS, smem));
-  if (occ < 1) occ = 1;
-  const int64_t tiles = (a.n_new + BU_TM - 1) / BU_TM;
-  int grid = (int)std::min<int64_t>(std::max<int64_t>(tiles, 1), (int64_t)num_sms() * occ);
-  k_block_update<T, KPT><<<grid, BU_THREADS, smem, st>>>(p);
-  HB_LAUNCH_CHECK();
-  return HB_OK;
+  return launch_block_form<T, KPT, true>(p, base, st);
 }
 
 template <typename T>
@@ -642,7 +686,9 @@ __global__ void k_ridge_solve(CorrArgs a, TW* __restrict__ W) {
 
 template <typename TW>
 int launch_ridge_solve(const CorrArgs& a, TW* W, cudaStream_t st) {
-  k_ridge_solve<TW><<<a.K, 128, sizeof(double) * 2 * a.B, st>>>(a, W);
+  const size_t smem = sizeof(double) * 2 * a.B;
+  if (smem > 48 * 1024) HB_TRY(allow_max_dyn_smem((const void*)k_ridge_solve<TW>));
+  k_ridge_solve<TW><<<a.K, 128, smem, st>>>(a, W);
   HB_LAUNCH_CHECK();
   return HB_OK;
 }

@@ -87,15 +87,18 @@ class HarmonyProblem:
         self.device = X.device
         self.X = X.contiguous()
         n_cells, n_pcs = self.X.shape
-        cats = np.asarray(cats, dtype=np.int32)
         self.n_batches = int(n_batches)
-        N_b = np.bincount(cats, minlength=self.n_batches).astype(np.int64)
-        self.cats = torch.as_tensor(cats, device=self.device)
+        if isinstance(cats, torch.Tensor):  # codes on the device: counted and sorted there
+            self.cats = cats.to(device=self.device, dtype=torch.int32).contiguous()
+            N_b = torch.bincount(self.cats.long(), minlength=self.n_batches).cpu().numpy().astype(np.int64)
+        else:
+            cats = np.asarray(cats, dtype=np.int32)
+            N_b = np.bincount(cats, minlength=self.n_batches).astype(np.int64)
+            self.cats = torch.as_tensor(cats, device=self.device)
         # the engine sorts the cells by batch itself up to 4096 batches
         self.cell_index = None
         if self.n_batches > 4096:
-            self.cell_index = torch.as_tensor(np.argsort(cats, kind="stable").astype(np.int32),
-                                              device=self.device)
+            self.cell_index = torch.sort(self.cats, stable=True).indices.to(torch.int32)
         self.offsets = np.zeros(self.n_batches + 1, dtype=np.int64)
         self.offsets[1:] = np.cumsum(N_b)
         self.theta = np.asarray(theta, dtype=np.float64)
@@ -179,12 +182,20 @@ def from_dlpack(x):
 
 
 def _integer_codes(labels):
-    """Categorical codes of plain non-negative integer labels without pandas:
-    the categories are the sorted distinct values, as ``astype("category")``
-    gives them.  Returns (None, 0) for anything else."""
+    """Categorical codes of plain integer labels without pandas: the categories are the
+    sorted distinct values, as ``astype("category")`` gives them.  Labels already on the GPU
+    (a CUDA tensor, or any DLPack device array) are coded there (``torch.unique``) and stay
+    there: the codes come back as an int32 CUDA tensor, as the reference keeps its ``cats``
+    on the device (_utils/_multi_gpu.py:202-232).  Host labels must be non-negative and come
+    back as a NumPy array.  Returns (None, 0) for anything else."""
     labels = from_dlpack(labels)
+    if isinstance(labels, torch.Tensor) and labels.is_cuda:
+        if labels.dim() != 1 or labels.numel() == 0 or labels.dtype.is_floating_point or labels.dtype == torch.bool:
+            return None, 0
+        uniq, inv = torch.unique(labels, sorted=True, return_inverse=True)
+        return inv.to(torch.int32), int(uniq.numel())
     if isinstance(labels, torch.Tensor):
-        labels = labels.detach().cpu().numpy()
+        labels = labels.detach().numpy()
     if not isinstance(labels, np.ndarray) or labels.ndim != 1 or labels.dtype.kind not in "iu":
         return None, 0
     if labels.size == 0 or labels.min() < 0 or labels.max() > 16 * labels.size + (1 << 20):
@@ -361,7 +372,10 @@ def harmonize(
         cats_np = np.asarray(codes.cat.codes.values, dtype=np.int32)
     if cats_np.shape[0] != n_cells:
         raise ValueError("batch labels must have one entry per cell")
-    N_b = np.bincount(cats_np, minlength=n_batches).astype(np.int64)
+    if isinstance(cats_np, torch.Tensor):  # device codes: only the B counts come to the host
+        N_b = torch.bincount(cats_np.long(), minlength=n_batches).cpu().numpy().astype(np.int64)
+    else:
+        N_b = np.bincount(cats_np, minlength=n_batches).astype(np.int64)
     n_clusters, th = resolve_parameters(
         n_cells, N_b, n_clusters=n_clusters, max_iter_harmony=max_iter_harmony, theta=theta,
         tau=tau, block_proportion=block_proportion, dynamic_lambda=dynamic_lambda, alpha=alpha,

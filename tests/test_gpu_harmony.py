@@ -160,3 +160,69 @@ def test_dlpack_device_input_runs_in_place():
     b = harmonize(Zt, cfg["cats"].astype(np.int64), None, **kw)
     assert a.device.type == "cuda"
     assert (a - b).abs().max().item() <= 1e-5 * b.abs().max().item()
+
+
+def test_device_labels_stay_on_the_device(monkeypatch):
+    """Integer labels already on the GPU are coded, counted and sorted there: no host copy of
+    the per-cell array (the reference keeps cats on the device, _utils/_multi_gpu.py:202-232).
+    Arbitrary integer values (negative, gaps, unsorted) give the same result as the same labels
+    on the host."""
+    from rapids_singlecell_b200.harmony import _integer_codes
+
+    cfg = make_config("C1", seed=13, n_cells=4000)
+    values = np.array([40, -3, 7])[cfg["cats"]]  # categories sorted: -3, 7, 40
+    dev_labels = torch.as_tensor(values, device="cuda")
+    codes, nb = _integer_codes(dev_labels)
+    assert nb == 3 and codes.is_cuda and codes.dtype == torch.int32
+    host = pd.Series(values).astype("category").cat.codes.to_numpy()
+    assert np.array_equal(codes.cpu().numpy(), host)
+    kw = dict(n_clusters=25, max_iter_harmony=2, max_iter_clustering=4, tol_harmony=-np.inf,
+              tol_clustering=-np.inf, init_centroids=cfg["Y0"][:25], precision="fp32")
+    Zt = torch.as_tensor(cfg["Z"], device="cuda")
+    b = harmonize(Zt, pd.Categorical(values), None, **kw)
+    n = cfg["Z"].shape[0]
+    real_cpu = torch.Tensor.cpu
+
+    def guarded_cpu(self, *args, **kwargs):  # the per-cell label array must not come back
+        assert not (self.is_cuda and self.dim() == 1 and self.numel() == n), "per-cell array copied to host"
+        return real_cpu(self, *args, **kwargs)
+
+    monkeypatch.setattr(torch.Tensor, "cpu", guarded_cpu)
+    a = harmonize(Zt, dev_labels, None, **kw)
+    monkeypatch.undo()
+    assert (a - b).abs().max().item() <= 1e-5 * b.abs().max().item()
+
+
+def test_device_labels_with_many_batches():
+    """More than 4096 batches: the batch-sorted cell index is built with a device sort."""
+    from rapids_singlecell_b200.harmony import HarmonyProblem
+
+    n, B = 20_000, 4500  # two clusters keep the B x K tables of the plain path in shared memory
+    rng = np.random.default_rng(3)
+    Z = rng.standard_normal((n, 8)).astype(np.float32)
+    cats = rng.integers(0, B, n).astype(np.int32)
+    Y0 = torch.as_tensor(Z[:2], device="cuda")
+    kw = dict(n_clusters=2, max_iter_harmony=1, max_iter_clustering=2, tol_harmony=-np.inf,
+              tol_clustering=-np.inf)
+    X = torch.as_tensor(Z, device="cuda")
+    p_dev = HarmonyProblem(X, torch.as_tensor(cats, device="cuda"), B, Y0, np.full(B, 2.0), **kw)
+    p_host = HarmonyProblem(X, cats, B, Y0, np.full(B, 2.0), **kw)
+    assert torch.equal(p_dev.cell_index.cpu(),
+                       torch.as_tensor(np.argsort(cats, kind="stable").astype(np.int32)))
+    za = p_dev.run()[0].clone()
+    zb = p_host.run()[0].clone()
+    assert (za - zb).abs().max().item() <= 1e-5 * zb.abs().max().item()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_hundreds_of_batches_on_the_plain_paths(prec):
+    """400 batches x K = 100 (atlas-sized donor counts) on the default float64 path and on fp32:
+    the B x K penalty and count tables no longer fit in shared memory, so the block update runs
+    with global tables and direct float64 atomics; parity with the oracle as for few batches."""
+    spec = MixtureSpec(30_000, 20, 12, 400, "dirichlet", (), 0.5, (0.8, 1.2))
+    Z, cats, _ = make_mixture(spec, 21)
+    Y0 = initial_centroids(Z, 100, 22)
+    out, info, ref = _run_both(Z, cats, 400, Y0, prec, n_clusters=100, max_iter_harmony=2,
+                               max_iter_clustering=3, tol_harmony=-np.inf, tol_clustering=-np.inf)
+    assert info.n_outer == 2
+    assert rel_maxabs(out, ref.Z_hat) < TOL[prec]

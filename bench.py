@@ -56,6 +56,10 @@ def parse():
                          "2M-cell x 100-PC workload), batched (256 independent problems), "
                          "serving (Poisson request stream), pca (500k x 2000 covariance PCA), "
                          "knn (500k x 50 exact kNN); empty for none")
+    ap.add_argument("--serving-requests", type=int, default=64,
+                    help="requests of the serving section (the configuration names 2,000)")
+    ap.add_argument("--serving-rates", default="10,100", help="bf16 arrival rates (req/s), comma-separated")
+    ap.add_argument("--serving-fp32-rates", default="10", help="fp32 arrival rates (req/s)")
     ap.add_argument("--profile-case", action="store_true",
                     help="one short run for ncu: the same workload for 1 outer x 2 k-means "
                          "iterations, then exit")
@@ -366,7 +370,7 @@ def batched_section(dev, n_problems=256, streams=32):
     return out
 
 
-def serving_section(dev, n_requests=64, rates=(10.0, 100.0), fp32_rate=10.0, streams=8):
+def serving_section(dev, n_requests=64, rates=(10.0, 100.0), fp32_rates=(10.0,), streams=8):
     """A Poisson stream of integration requests through HarmonyServer (HBM budget
     160 GB, 8 streams): cells log-uniform in [5k, 1M], d in {30, 50, 100}, B in
     [2, 32], K = min(200, n / 30), 10 outer x 20 k-means iterations fixed.  Each
@@ -425,7 +429,7 @@ def serving_section(dev, n_requests=64, rates=(10.0, 100.0), fp32_rate=10.0, str
                        "d in {30, 50, 100}, B in [2, 32], K = min(200, n/30), "
                        f"{OUTER} outer x {INNER} k-means iterations fixed, HBM budget 160 GB, {streams} streams",
            "bf16": [stream_run("bf16", r) for r in rates],
-           "fp32": [stream_run("fp32", fp32_rate)]}
+           "fp32": [stream_run("fp32", r) for r in fp32_rates]}
     torch.cuda.synchronize()
     return out
 
@@ -551,8 +555,12 @@ def knn_section(dev, n=500_000, d=50, k=15):
 
 def run_sections(args, dev):
     out = {}
+    rates = tuple(float(r) for r in args.serving_rates.split(","))
+    fp32_rates = tuple(float(r) for r in args.serving_fp32_rates.split(","))
     for name in [s for s in args.sections.split(",") if s]:
-        fn = {"wide": wide_section, "batched": batched_section, "serving": serving_section,
+        fn = {"wide": wide_section, "batched": batched_section,
+              "serving": lambda d: serving_section(d, n_requests=args.serving_requests, rates=rates,
+                                                   fp32_rates=fp32_rates),
               "pca": pca_section, "knn": knn_section}[name]
         t0 = time.perf_counter()
         try:

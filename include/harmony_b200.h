@@ -123,6 +123,12 @@ HB_API size_t hb_plan_workspace_bytes(const hb_plan* plan);
  *   theta         host float64 [n_batches] (tau discount already applied)
  *   Y0            device [n_clusters, n_pcs] initial centroids, same dtype as X
  *   Z_hat         device [n_cells, n_pcs] output, same dtype as X
+ * Limits: n_pcs <= 256 (<= 128 on the 16-bit path), n_clusters <= 256.
+ * The call enqueues the whole loop on `stream` without waiting on the device: the k-means stop,
+ * the outer convergence test and the error flags are evaluated on the device, and the launches
+ * after the point where the loop ends return at once.  It synchronises the stream once, at the
+ * end, to read the objectives and the status (non-blocking event queries in between let it
+ * stop enqueuing early).
  */
 HB_API int hb_harmonize(hb_plan* plan, const void* X, const int32_t* cats, const int32_t* cell_index,
                  const int64_t* batch_offsets, const double* theta, const void* Y0,
@@ -180,6 +186,48 @@ HB_API int hb_ridge_inverse(const double* O, const double* lambda_kb, double* in
 HB_API int hb_similarity(const void* Zn, int32_t ldz, const void* Yn, int32_t ldy, const int32_t* idx,
                   int64_t n, int32_t n_pcs, int32_t n_clusters, int32_t dtype, float* S,
                   int32_t* err, void* stream);
+
+/* ---- kernel-level entry points of the 16-bit path (the launchers hb_harmonize drives, run alone).
+ * 16-bit arrays (dtype HB_BF16 / HB_FP16) of cells have rows = 128 ceil(n / 128) + 8 rows, the
+ * rows past n zero (the tiles of 128 cells are read whole); row strides are multiples of 8. ---- */
+
+/* Centroid pass in cell order (TMA tiles, tcgen05): Yn[k] = l2normalise(sum_i R[i][k] Zn[i]) (16-bit
+ * [n_clusters][ldy], zero past n_pcs; inverse norm capped at 1e12) and Osum[key][k] = sum over the
+ * cells i with ckey[i] == key of R[i][k] (float64 [n_keys][n_clusters]), ckey int32 [n] in
+ * [0, n_keys).  With the key (block, batch) the second output is the per-block "remove old"
+ * sums of the sweep.  Replaces the centroid GEMM and normalisation (clustering.cu:272-281) and the
+ * per-block R column sums (clustering.cu:321-332).  n_pcs <= 128, n_clusters <= 256, n_keys <= 256
+ * within the kernel's shared memory (HB_ERR_UNSUPPORTED otherwise).  *err (device int32, cleared
+ * by the call) is set non-zero if a bounded wait gave up. */
+HB_API size_t hb_tc_centroids_workspace_bytes(int64_t n, int32_t n_pcs, int32_t n_clusters, int32_t n_keys);
+HB_API int hb_tc_centroids(const void* Zn, int32_t ldz, const void* R, int32_t ldr, int64_t n, int32_t n_pcs,
+                           int32_t n_clusters, const int32_t* ckey, int32_t n_keys, int32_t dtype, void* Yn,
+                           int32_t ldy, double* Osum, void* workspace, size_t workspace_bytes, int32_t* err,
+                           void* stream);
+
+/* Ridge moments on the tensor core: M[k][b+1][c] = sum over the cells i of batch b of R[i][k] X[i][c]
+ * and M[k][0][c] = the sum over all batches (float64 [n_clusters][n_batches+1][n_pcs]).  X float32
+ * [n][n_pcs] enters as bf16 hi + lo parts; cell_index int32 [n] lists the cells sorted by batch and
+ * batch_offsets (host int64 [n_batches+1]) are its offsets.  Replaces the moment GEMMs of
+ * correction_batched_impl (correction_batched.cu:55-100).  n_pcs <= 256, n_clusters <= 256. */
+HB_API size_t hb_tc_moments_workspace_bytes(int64_t n, int32_t n_pcs, int32_t n_clusters, int32_t n_batches);
+HB_API int hb_tc_moments(const float* X, const void* R, int32_t ldr, const int32_t* cell_index,
+                         const int64_t* batch_offsets, int64_t n, int32_t n_pcs, int32_t n_clusters,
+                         int32_t n_batches, int32_t dtype, double* M, void* workspace, size_t workspace_bytes,
+                         int32_t* err, void* stream);
+
+/* Correction apply on the tensor core: Z_hat[i] = X[i] - sum_k R[i][k] W[b_i][k] (float32 [n][n_pcs])
+ * and Zn[i] = l2normalise(Z_hat[i]) (16-bit [rows][ldz], zero past n_pcs), W float32
+ * [n_batches][n_clusters][n_pcs], b_i the batch of cell i (from cell_index and batch_offsets as for
+ * hb_tc_moments).  X and W enter as bf16 hi + lo parts.  Replaces the apply of
+ * correction_batched_impl (kernels_outer.cuh:41-65) fused with the renormalisation of
+ * _harmony/__init__.py:276.  *err = 7 flags |X| or |W| outside the fp16 range (HB_FP16).
+ * n_pcs <= 128, n_clusters <= 256. */
+HB_API size_t hb_tc_apply_workspace_bytes(int64_t n, int32_t n_batches);
+HB_API int hb_tc_apply(const float* X, const void* R, int32_t ldr, const float* W, const int32_t* cell_index,
+                       const int64_t* batch_offsets, int64_t n, int32_t n_pcs, int32_t n_clusters,
+                       int32_t n_batches, int32_t dtype, float* Z_hat, void* Zn, int32_t ldz, void* workspace,
+                       size_t workspace_bytes, int32_t* err, void* stream);
 
 /* Initial centroids by a seeded k-means on the L2-normalised rows of X (float32 [n, n_pcs],
  * row-major): k-means++ seeding over a sample of min(n, 64 n_clusters, 16384) cells drawn

@@ -31,7 +31,9 @@ EXPORTED = (
     "hb_plan_create", "hb_plan_destroy", "hb_plan_workspace_bytes", "hb_harmonize",
     "hb_l2_normalize", "hb_block_lists_workspace_bytes", "hb_block_lists", "hb_block_lists_static",
     "hb_penalty",
-    "hb_lambda_kb", "hb_ridge_inverse", "hb_similarity", "hb_kmeans_workspace_bytes", "hb_kmeans_init",
+    "hb_lambda_kb", "hb_ridge_inverse", "hb_similarity", "hb_tc_centroids_workspace_bytes", "hb_tc_centroids",
+    "hb_tc_moments_workspace_bytes", "hb_tc_moments", "hb_tc_apply_workspace_bytes", "hb_tc_apply",
+    "hb_kmeans_workspace_bytes", "hb_kmeans_init",
     "hb_pca_gram_workspace_bytes", "hb_pca_gram", "hb_pca_covariance", "hb_pca_project_workspace_bytes",
     "hb_pca_project", "hb_csr_to_dense", "hb_knn_workspace_bytes", "hb_knn",
     "hb_last_error", "hb_version",
@@ -141,6 +143,21 @@ def load() -> ctypes.CDLL:
     lib.hb_similarity.argtypes = [c_void_p, c_i32, c_void_p, c_i32, c_void_p, c_i64, c_i32, c_i32,
                                   c_i32, c_void_p, c_void_p, c_void_p]
     lib.hb_similarity.restype = c_int
+    lib.hb_tc_centroids_workspace_bytes.argtypes = [c_i64, c_i32, c_i32, c_i32]
+    lib.hb_tc_centroids_workspace_bytes.restype = c_size
+    lib.hb_tc_centroids.argtypes = [c_void_p, c_i32, c_void_p, c_i32, c_i64, c_i32, c_i32, c_void_p, c_i32, c_i32,
+                                    c_void_p, c_i32, c_void_p, c_void_p, c_size, c_void_p, c_void_p]
+    lib.hb_tc_centroids.restype = c_int
+    lib.hb_tc_moments_workspace_bytes.argtypes = [c_i64, c_i32, c_i32, c_i32]
+    lib.hb_tc_moments_workspace_bytes.restype = c_size
+    lib.hb_tc_moments.argtypes = [c_void_p, c_void_p, c_i32, c_void_p, P(c_i64), c_i64, c_i32, c_i32, c_i32, c_i32,
+                                  c_void_p, c_void_p, c_size, c_void_p, c_void_p]
+    lib.hb_tc_moments.restype = c_int
+    lib.hb_tc_apply_workspace_bytes.argtypes = [c_i64, c_i32]
+    lib.hb_tc_apply_workspace_bytes.restype = c_size
+    lib.hb_tc_apply.argtypes = [c_void_p, c_void_p, c_i32, c_void_p, c_void_p, P(c_i64), c_i64, c_i32, c_i32, c_i32,
+                                c_i32, c_void_p, c_void_p, c_i32, c_void_p, c_size, c_void_p, c_void_p]
+    lib.hb_tc_apply.restype = c_int
     lib.hb_kmeans_workspace_bytes.argtypes = [c_i64, c_i32, c_i32]
     lib.hb_kmeans_workspace_bytes.restype = c_size
     lib.hb_kmeans_init.argtypes = [c_void_p, c_i64, c_i32, c_i32, c_i32, ctypes.c_double, ctypes.c_uint64,

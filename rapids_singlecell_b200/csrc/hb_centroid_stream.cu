@@ -4,7 +4,8 @@
 // cells of R[cell][cluster] Z_norm[cell][pc] (the centroid GEMM of the reference,
 // _cuda/harmony/clustering/clustering.cu:272-276) and, per (block, batch) key of
 // the coming sweep, the sum of the cells' R rows (the "remove old contribution"
-// terms, clustering.cu:321-332).  Here the cells are read in storage order, so
+// terms, clustering.cu:321-332), and per block their sum over the batches (key
+// (block, B), the column sums).  Here the cells are read in storage order, so
 // each 128-cell tile of Z_norm and of R is one TMA tile load instead of a row
 // gather, and the per-key sums become a second MMA against a one-hot operand:
 //   D1[cluster][pc]  += R_tile^T Z_tile
@@ -194,9 +195,16 @@ __global__ void __launch_bounds__(256, 1) k_tc_centroid_stream(CenStreamArgs a, 
       if (i >= NOH && !tc::mbar_wait(mma_done + b, (uint32_t)(((i - NOH) / NOH) & 1), kMaxPolls))
         atomicExch(a.err, 5);
       unsigned char* oh = sm + L.offOH + (uint32_t)b * L.ohBytes;
-      const int key = kq[0];
-      if (key_old[b] >= 0) *(H*)(oh + oh_off(row, key_old[b])) = zero;
-      if (key >= 0) *(H*)(oh + oh_off(row, key)) = one;
+      const int key = kq[0], ko = key_old[b];
+      // a cell's ones: its key and, with kpb, the column-sum key (block, B) of its block
+      if (ko >= 0) {
+        *(H*)(oh + oh_off(row, ko)) = zero;
+        if (a.kpb) *(H*)(oh + oh_off(row, ko - ko % a.kpb + a.kpb - 1)) = zero;
+      }
+      if (key >= 0) {
+        *(H*)(oh + oh_off(row, key)) = one;
+        if (a.kpb) *(H*)(oh + oh_off(row, key - key % a.kpb + a.kpb - 1)) = one;
+      }
       key_old[b] = key;
       kq[0] = kq[1];
       kq[1] = kq[2];

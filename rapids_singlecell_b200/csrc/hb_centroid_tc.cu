@@ -157,23 +157,32 @@ __device__ __forceinline__ void cen_runs(const int* kr, TileRuns& tr, unsigned c
   tc::fence_proxy_async_smem();
 }
 
-// Running (key, sum) of one cluster over the runs it sees; flushed to Omin with a
-// float64 atomic when the key changes.
+// Running (key, sum) of one cluster over the runs it sees, and the running sum of the
+// key's block (key (block, B): the block's column sums); each flushed to Omin with a
+// float64 atomic when its key changes.
 struct RunAcc {
-  int key = -1;
-  double acc = 0.0;
+  int key = -1, bkey = -1;
+  double acc = 0.0, bacc = 0.0;
   __device__ __forceinline__ void add(const CenArgs& a, int kc, int k, double v) {
     if (k != key) {
       if (key >= 0 && acc != 0.0) atomicAdd(&a.Omin[(size_t)key * a.K + kc], acc);
       key = k;
       acc = 0.0;
+      const int bk = k - k % (a.B + 1) + a.B;
+      if (bk != bkey) {
+        if (bkey >= 0 && bacc != 0.0) atomicAdd(&a.Omin[(size_t)bkey * a.K + kc], bacc);
+        bkey = bk;
+        bacc = 0.0;
+      }
     }
     acc += v;
+    bacc += v;
   }
   __device__ __forceinline__ void flush(const CenArgs& a, int kc) {
     if (key >= 0 && acc != 0.0) atomicAdd(&a.Omin[(size_t)key * a.K + kc], acc);
-    key = -1;
-    acc = 0.0;
+    if (bkey >= 0 && bacc != 0.0) atomicAdd(&a.Omin[(size_t)bkey * a.K + kc], bacc);
+    key = bkey = -1;
+    acc = bacc = 0.0;
   }
 };
 

@@ -60,6 +60,10 @@ template <> __device__ __forceinline__ double from_f<double>(float x) { return x
 template <> __device__ __forceinline__ __half from_f<__half>(float x) { return __float2half_rn(x); }
 template <> __device__ __forceinline__ __nv_bfloat16 from_f<__nv_bfloat16>(float x) { return __float2bfloat16_rn(x); }
 
+// A launch gated on a device flag (the run has stopped): true when the kernel must return at once.
+// The flag is written by an earlier launch on the same stream, so every CTA reads the same value.
+__device__ __forceinline__ bool gated(const int* gate) { return gate && *(volatile const int*)gate; }
+
 __device__ __forceinline__ unsigned lanemask_lt() {
   unsigned m;
   asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));

@@ -67,7 +67,9 @@ template <typename H>
 __global__ void __launch_bounds__(256) k_tc_moments(const H* __restrict__ R, int ldr, const float* __restrict__ X,
                                                     int ldx, const int32_t* __restrict__ cell_index,
                                                     const AccumChunk* __restrict__ chunks, int K, int d,
-                                                    float* __restrict__ Mpart, MomLayout L, int* err) {
+                                                    float* __restrict__ Mpart, MomLayout L, int* err,
+                                                    const int* gate) {
+  if (gated(gate)) return;  // before the TMEM allocation: every thread of the CTA returns
   extern __shared__ __align__(1024) unsigned char smem_dyn[];
   unsigned char* sm = (unsigned char*)(((uintptr_t)smem_dyn + 1023) & ~(uintptr_t)1023);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -176,7 +178,7 @@ __global__ void __launch_bounds__(256) k_tc_moments(const H* __restrict__ R, int
 template <typename H>
 int launch_tc_moments(const H* R, int ldr, const float* X, int ldx, const int32_t* cell_index,
                       const AccumChunk* chunks, int n_chunks, int K, int d, float* Mpart, int* err,
-                      cudaStream_t st) {
+                      cudaStream_t st, const int* gate) {
   if (n_chunks == 0) return HB_OK;
   if (K > 256 || d > 256) {
     set_error("tensor-core correction: unsupported shape (K=%d d=%d)", K, d);
@@ -185,14 +187,16 @@ int launch_tc_moments(const H* R, int ldr, const float* X, int ldx, const int32_
   const MomLayout L = mom_layout(K, d);
   const void* fn = (const void*)k_tc_moments<H>;
   HB_TRY(allow_max_dyn_smem(fn));
-  k_tc_moments<H><<<n_chunks, 256, L.bytes, st>>>(R, ldr, X, ldx, cell_index, chunks, K, d, Mpart, L, err);
+  k_tc_moments<H><<<n_chunks, 256, L.bytes, st>>>(R, ldr, X, ldx, cell_index, chunks, K, d, Mpart, L, err,
+                                                                gate);
   HB_LAUNCH_CHECK();
   return HB_OK;
 }
 template int launch_tc_moments<__half>(const __half*, int, const float*, int, const int32_t*, const AccumChunk*,
-                                       int, int, int, float*, int*, cudaStream_t);
+                                       int, int, int, float*, int*, cudaStream_t, const int*);
 template int launch_tc_moments<__nv_bfloat16>(const __nv_bfloat16*, int, const float*, int, const int32_t*,
-                                              const AccumChunk*, int, int, int, float*, int*, cudaStream_t);
+                                              const AccumChunk*, int, int, int, float*, int*, cudaStream_t,
+                                              const int*);
 
 // ---------------------------------------------------------------------------
 // Apply
@@ -230,7 +234,8 @@ __global__ void __launch_bounds__(256) k_tc_apply(const float* __restrict__ X, i
                                                   const int32_t* __restrict__ cell_index,
                                                   const ApplyTile* __restrict__ tiles, int n_tiles, int K, int d,
                                                   float* __restrict__ Zhat, int ldzh, H* __restrict__ Zn, int ldz,
-                                                  ApLayout L, int* err) {
+                                                  ApLayout L, int* err, const int* gate) {
+  if (gated(gate)) return;  // before the TMEM allocation: every thread of the CTA returns
   extern __shared__ __align__(1024) unsigned char smem_dyn[];
   unsigned char* sm = (unsigned char*)(((uintptr_t)smem_dyn + 1023) & ~(uintptr_t)1023);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -292,14 +297,16 @@ __global__ void __launch_bounds__(256) k_tc_apply(const float* __restrict__ X, i
       tc::cp_async16(sm32 + L.offA + (uint32_t)(c >> 3) * 16384u + tc::sw128_off((uint32_t)r, (uint32_t)(c & 7)),
                      ok ? (const void*)(R + (int64_t)cell * ldr + c * 8) : (const void*)R, ok ? 16u : 0u);
     }
-    // X rows of the tile (coalesced: consecutive threads on consecutive columns of a row)
+    // X rows of the tile (consecutive threads on consecutive columns of a row), all copies in
+    // flight at once with the R rows (zero for missing rows)
     {
-      float* sX = (float*)(sm + L.offX);
+      const uint32_t sX32 = sm32 + L.offX;
       const int dr = 256 / d, dc = 256 % d;
       int r = tid / d, c = tid % d;
       for (; r < 128;) {
         const int cell = ids[r];
-        sX[r * L.ldxs + c] = cell >= 0 ? __ldg(X + (int64_t)cell * ldx + c) : 0.f;
+        tc::cp_async4(sX32 + (uint32_t)(r * L.ldxs + c) * 4u,
+                      cell >= 0 ? (const void*)(X + (int64_t)cell * ldx + c) : (const void*)X, cell >= 0 ? 4u : 0u);
         r += dr;
         c += dc;
         if (c >= d) { c -= d; ++r; }
@@ -395,7 +402,7 @@ __global__ void __launch_bounds__(256) k_tc_apply(const float* __restrict__ X, i
 template <typename H>
 int launch_tc_apply(const float* X, int ldx, const H* R, int ldr, const float* W, const int32_t* cell_index,
                     const ApplyTile* tiles, int n_tiles, int K, int d, float* Zhat, int ldzh, H* Zn, int ldz,
-                    int* err, cudaStream_t st) {
+                    int* err, cudaStream_t st, const int* gate) {
   if (n_tiles == 0) return HB_OK;
   if (K > 256 || d > 128) {
     set_error("tensor-core correction: unsupported shape (K=%d d=%d)", K, d);
@@ -409,14 +416,15 @@ int launch_tc_apply(const float* X, int ldx, const H* R, int ldr, const float* W
   const int per_sm = std::max(1, std::min<int>(512 / L.tcols, (int)(233472u / (L.bytes + 2048u))));
   const int grid = std::max(1, std::min(n_tiles, num_sms() * per_sm));
   k_tc_apply<H><<<grid, 256, L.bytes, st>>>(X, ldx, R, ldr, W, cell_index, tiles, n_tiles, K, d, Zhat, ldzh, Zn,
-                                             ldz, L, err);
+                                             ldz, L, err, gate);
   HB_LAUNCH_CHECK();
   return HB_OK;
 }
 template int launch_tc_apply<__half>(const float*, int, const __half*, int, const float*, const int32_t*,
-                                     const ApplyTile*, int, int, int, float*, int, __half*, int, int*, cudaStream_t);
+                                     const ApplyTile*, int, int, int, float*, int, __half*, int, int*, cudaStream_t,
+                                     const int*);
 template int launch_tc_apply<__nv_bfloat16>(const float*, int, const __nv_bfloat16*, int, const float*,
                                             const int32_t*, const ApplyTile*, int, int, int, float*, int,
-                                            __nv_bfloat16*, int, int*, cudaStream_t);
+                                            __nv_bfloat16*, int, int*, cudaStream_t, const int*);
 
 }  // namespace hb

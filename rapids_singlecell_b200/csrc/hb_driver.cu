@@ -98,9 +98,11 @@ struct hb_plan {
   bool cen_stream;     // 16-bit path: centroid pass in cell order (hb_centroid_stream.cu)
   int nkeys;           // (block, batch) keys: blocks * (batches + 1)
   size_t ws_bytes;
-  std::vector<cudaEvent_t> events;  // profiling pool (created on first profiled run)
+  std::vector<cudaEvent_t> events;       // profiling pool (created on first profiled run)
+  std::vector<cudaEvent_t> flag_events;  // one per outer iteration: its end flags have arrived
   ~hb_plan() {
     for (cudaEvent_t e : events) cudaEventDestroy(e);
+    for (cudaEvent_t e : flag_events) cudaEventDestroy(e);
   }
 };
 
@@ -128,7 +130,11 @@ struct Work {
   float* Opart;     // per-CTA per-key sums of the streaming centroid pass
   int32_t* cell_index;  // cells sorted by batch (stable), built when the caller passes none
   int* err;
-  int* stop;  // device-side k-means stop: iterations run, 0 while running
+  RunCtl* ctl;      // device-side run control (k-means stop, run end, convergence)
+  int* stop;        // &ctl->stop
+  double* objs;     // [max_iter_harmony + 1] objective after each outer iteration
+  double* kobj;     // [max_iter_harmony][max_iter_clustering] k-means objectives
+  int32_t* kiters;  // [max_iter_harmony] k-means iterations run
   AccumChunk* cen_chunks;
   AccumChunk* m_chunks;
   int32_t* batch_chunk_off;
@@ -163,7 +169,11 @@ void carve(const hb_plan& P, Carver& cv, Work& w) {
   w.ckey = P.cen_stream ? cv.take<int32_t>((size_t)kMaxIterChunk * n) : nullptr;
   w.Opart = P.cen_stream ? cv.take<float>((size_t)P.cen_chunks * P.nkeys * K) : nullptr;
   w.err = cv.take<int>(4);
-  w.stop = cv.take<int>(1);
+  w.ctl = cv.take<RunCtl>(1);
+  w.stop = w.ctl ? &w.ctl->stop : nullptr;
+  w.objs = cv.take<double>((size_t)p.max_iter_harmony + 1);
+  w.kobj = cv.take<double>((size_t)p.max_iter_harmony * std::max(p.max_iter_clustering, 1));
+  w.kiters = cv.take<int32_t>(p.max_iter_harmony);
   w.cen_chunks = cv.take<AccumChunk>(P.cen_chunks);
   w.m_chunks = cv.take<AccumChunk>(P.max_m_chunks);
   w.batch_chunk_off = cv.take<int32_t>(B + 1);
@@ -197,7 +207,6 @@ int validate(const hb_params& p) {
     return HB_ERR_UNSUPPORTED;
   }
   if (p.n_clusters > 256) { set_error("n_clusters=%d exceeds the supported maximum of 256", p.n_clusters); return HB_ERR_UNSUPPORTED; }
-  if (p.precision == HB_FP64 && p.n_pcs > 128) { set_error("n_pcs=%d exceeds 128 for float64", p.n_pcs); return HB_ERR_UNSUPPORTED; }
   if (p.n_pcs > 256) { set_error("n_pcs=%d exceeds the supported maximum of 256", p.n_pcs); return HB_ERR_UNSUPPORTED; }
   if (p.precision < HB_FP32 || p.precision > HB_FP16) {
     set_error("unknown precision %d", p.precision);
@@ -399,6 +408,7 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
   for (int i = 0; i < 3; ++i) HB_CUDA(cudaMemsetAsync(w.O[i], 0, sizeof(double) * (B + 1) * K, st));
   HB_CUDA(cudaMemsetAsync(w.obj_acc, 0, sizeof(double), st));
   HB_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
+  HB_CUDA(cudaMemsetAsync(w.ctl, 0, sizeof(RunCtl), st));
   // the splitter's overflow flag is read once per outer iteration: cleared once per run
   HB_TRY(membership_clear_err(w.mb, st));
 
@@ -419,7 +429,7 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
   HB_CUDA(cudaMemsetAsync((char*)R + (size_t)n * P->ldr * P->ssz, 0, (size_t)(P->rows_alloc - n) * P->ldr * P->ssz, st));
   HB_TRY(launch_l2_normalize<T, S>(X, n, d, d, Zn, P->ldz, st));
   HB_TRY(launch_l2_normalize<T, S>(Y0, K, d, d, Yn, P->ldy, st));
-  double* obj_init = w.obj_out + std::max(p.max_iter_clustering, 1);
+  double* obj_init = w.objs;  // objs[0]: the objective of the initial state
   constexpr bool tc_path = !std::is_same<S, float>::value && !std::is_same<S, double>::value;
   // one persistent sweep (16-bit path) over `nblk` blocks of `idx`, objective into obj_dst
   int* sweep_stop = nullptr;  // device-side k-means stop passed to the next sweep launch, with sweep_it
@@ -458,34 +468,35 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
     HB_TRY(launch_objective_finalize(ring.state(), w.Pr, w.theta, p.sigma, B, K, p.stabilized_penalty,
                                      w.obj_acc, obj_init, st));
   }
-  // pinned read-back slots: [0] one objective, [1 ..] the k-means objectives of an outer
-  // iteration, then the error flags
-  PinnedLease host(sizeof(double) * ((size_t)p.max_iter_clustering + 2) + 4 * sizeof(int));
+  const MembershipLayout& ml = P->ml;
+  const int nblk = ml.nblk;
+  const int mc = p.max_iter_clustering, mh = p.max_iter_harmony;
+  const size_t kstride = (size_t)std::max(mc, 1);
+  // pinned read-back: the (ostop, conv) flags of each outer iteration, then the one final read
+  // (run control, objectives, k-means iteration counts and objectives, error flags)
+  const size_t flag_bytes = align_up(sizeof(int) * 2 * mh, 8);
+  const size_t fin_doubles = (size_t)mh + 1 + (size_t)mh * kstride;
+  PinnedLease host(flag_bytes + sizeof(double) * fin_doubles + sizeof(int32_t) * mh + sizeof(RunCtl) +
+                   2 * sizeof(int));
   if (!host.ptr) {
     set_error("pinned host buffer for the read-backs: cudaMallocHost failed");
     return HB_ERR_CUDA;
   }
-  double* h_dbl = (double*)host.ptr;
-  int* h_err = (int*)(h_dbl + p.max_iter_clustering + 2);
-  HB_CUDA(cudaMemcpyAsync(h_dbl, obj_init, sizeof(double), cudaMemcpyDeviceToHost, st));
-  HB_CUDA(cudaStreamSynchronize(st));
-  double h_obj = h_dbl[0];
-  std::vector<double> objs{h_obj};
-  int converged = 0;
-  const MembershipLayout& ml = P->ml;
-  const int nblk = ml.nblk;
-  std::vector<double> kobj;
-  // With tol_clustering = -inf no iteration can stop early, so the per-iteration
-  // objective read-back (a host sync) is deferred to the end of the clustering call.
-  const bool early_stop = !(std::isinf(p.tol_clustering) && p.tol_clustering < 0);
-  // 16-bit path: the window-3 test runs on the device (CTA 0 of the sweep sets a stop flag
-  // that the later launches of the outer iteration check at entry); the host reads the flag
-  // once per chunk of block lists instead of syncing after every k-means iteration
-  const bool dev_stop = tc_path && early_stop;
+  int* h_flag = (int*)host.ptr;
+  double* h_objs = (double*)((char*)host.ptr + flag_bytes);
+  double* h_kobj = h_objs + mh + 1;
+  int32_t* h_kiters = (int32_t*)(h_kobj + (size_t)mh * kstride);
+  RunCtl* h_ctl = (RunCtl*)(h_kiters + mh);
+  int* h_err = (int*)(h_ctl + 1);
+  while ((int)P->flag_events.size() < mh) {
+    cudaEvent_t e;
+    HB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    P->flag_events.push_back(e);
+  }
 
   // optional device-time profile: event pairs around block-update and centroid launches
   hb_profile* prof = out ? out->profile : nullptr;
-  struct Span { int cat; int e0, e1; double bytes; };
+  struct Span { int cat; int e0, e1; double bytes; int outer, it; };
   std::vector<Span> spans;
   size_t next_ev = 0;
   auto ev = [&]() -> cudaEvent_t {
@@ -496,9 +507,9 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
     }
     return P->events[next_ev++];
   };
-  auto span_begin = [&](int cat, double bytes) -> int {
+  auto span_begin = [&](int cat, double bytes, int outer, int it) -> int {
     if (!prof) return -1;
-    spans.push_back(Span{cat, (int)next_ev, -1, bytes});
+    spans.push_back(Span{cat, (int)next_ev, -1, bytes, outer, it});
     cudaEventRecord(ev(), st);
     return (int)spans.size() - 1;
   };
@@ -508,20 +519,22 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
     cudaEventRecord(ev(), st);
   };
   const double zb = (double)d * P->ssz, rb = (double)K * P->ssz;
+  // every k-means launch is gated on the device-side stop, and every correction launch on the
+  // end of the run (RunCtl); with tol_clustering = -inf the window-3 test never passes
+  int* const dstop = w.stop;
+  const int* const ogate = &w.ctl->ostop;
 
-  for (int outer = 0; outer < p.max_iter_harmony; ++outer) {
+  int checked = 0;  // outer iterations whose end flags the host has seen
+  bool host_stop = false;
+  for (int outer = 0; outer < mh && !host_stop; ++outer) {
     const uint32_t seed = (uint32_t)((p.random_state + (uint64_t)outer * 1000003ull) & 0xffffffffull);
-    kobj.clear();
-    bool stop = false;
+    HB_TRY(launch_outer_begin(w.ctl, st));
     const int ring0 = ring.cur;
-    int done = p.max_iter_clustering;  // k-means iterations run (set by the device stop)
-    if (dev_stop) HB_CUDA(cudaMemsetAsync(w.stop, 0, sizeof(int), st));
-    int* const dstop = dev_stop ? w.stop : nullptr;
-    for (int it0 = 0; it0 < p.max_iter_clustering && !stop; it0 += kMaxIterChunk) {
-      const int C = std::min(kMaxIterChunk, p.max_iter_clustering - it0);
+    for (int it0 = 0; it0 < mc; it0 += kMaxIterChunk) {
+      const int C = std::min(kMaxIterChunk, mc - it0);
       HB_TRY(membership_build_dev(ml, w.mb, nullptr, seed + (uint32_t)it0, C, cats, w.idx, st, w.lcat,
-                                  w.ckey, B));
-      for (int c = 0; c < C && !stop; ++c) {
+                                  w.ckey, B, dstop));
+      for (int c = 0; c < C; ++c) {
         const int it = it0 + c;
         const int32_t* idx = w.idx + (size_t)c * n;
         const int32_t* lcat = w.lcat + (size_t)c * n;
@@ -533,11 +546,11 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
         bool writes_omin = false;
         if constexpr (tc_path) writes_omin = P->cen_stream;
         if (!writes_omin) HB_CUDA(cudaMemsetAsync(w.Omin, 0, sizeof(double) * nblk * omsz, st));
-        int sp = span_begin(1, (double)n * (zb + rb + 8));
+        int sp = span_begin(1, (double)n * (zb + rb + 8), outer, it);
         if constexpr (tc_path) {
           if (P->cen_stream) {
             CenStreamArgs ca{n, (int)((P->rows_alloc - 8) / 128), w.ckey + (size_t)c * n, d, K, P->nkeys,
-                             (float*)w.Ypart, w.Opart, w.err, Yn, P->ldy, dstop};
+                             (float*)w.Ypart, w.Opart, w.err, Yn, P->ldy, dstop, B + 1};
             HB_TRY(launch_tc_centroid_stream<S>(ca, Zn, P->ldz, R, P->ldr, P->rows_alloc, P->cen_chunks, w.Omin, st));
           } else {
             CenArgs ca{Zn, P->ldz, R, P->ldr, cats, idx, lcat, n, ml.bs, d, K, B, (float*)w.Ypart, w.Omin, w.err,
@@ -546,7 +559,7 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
           }
         } else {
           HB_TRY(launch_accum<S, S, TA>(R, P->ldr, Zn, P->ldz, idx, w.cen_chunks, P->cen_chunks, K, d,
-                                        (TA*)w.Ypart, st, OminArgs{w.Omin, cats, ml.bs, B}));
+                                        (TA*)w.Ypart, st, OminArgs{w.Omin, cats, ml.bs, B}, dstop));
         }
         bool reduced = false;  // the cell-order pass reduces its partials itself
         if constexpr (tc_path) reduced = P->cen_stream;
@@ -555,115 +568,94 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
         span_end(sp);
         // sweep the blocks (clustering.cu:308-372)
         if constexpr (tc_path) {
-          sp = span_begin(0, (double)n * (zb + rb + 8));
+          sp = span_begin(0, (double)n * (zb + rb + 8), outer, it);
           sweep_stop = dstop;
           sweep_it = it;
           HB_TRY(sweep(idx, lcat, ml.bs, nblk, w.Omin, 0, w.obj_out + it));
           sweep_stop = nullptr;
           span_end(sp);
         } else {
-        for (int j = 0; j < nblk; ++j) {
-          BlockArgs a = base;
-          const int64_t s0 = (int64_t)j * ml.bs;
-          a.idx_new = idx + s0;
-          a.n_new = std::min<int64_t>(ml.bs, n - s0);
-          a.Om_cur = j == 0 ? w.Omin : nullptr;
-          a.Om_next = j + 1 < nblk ? w.Omin + (size_t)(j + 1) * omsz : nullptr;
-          sp = span_begin(0, (double)a.n_new * (zb + rb + 8));
-          HB_TRY(ring.step<S>(a, st));
-          span_end(sp);
-        }
-        HB_TRY(launch_objective_finalize(ring.state(), w.Pr, w.theta, p.sigma, B, K,
-                                         p.stabilized_penalty, w.obj_acc, w.obj_out + it, st));
-        }
-        if (early_stop && !dev_stop) {
-          HB_CUDA(cudaMemcpyAsync(h_dbl, w.obj_out + it, sizeof(double), cudaMemcpyDeviceToHost, st));
-          HB_CUDA(cudaStreamSynchronize(st));
-          h_obj = h_dbl[0];
-          kobj.push_back(h_obj);
-          // window-3 convergence (clustering.cu:380-387)
-          const size_t m = kobj.size();
-          if (m >= 4) {
-            const double o = kobj[m - 2] + kobj[m - 3] + kobj[m - 4];
-            const double nw = kobj[m - 1] + kobj[m - 2] + kobj[m - 3];
-            if ((o - nw) < p.tol_clustering * std::fabs(o)) stop = true;
+          for (int j = 0; j < nblk; ++j) {
+            BlockArgs a = base;
+            const int64_t s0 = (int64_t)j * ml.bs;
+            a.idx_new = idx + s0;
+            a.n_new = std::min<int64_t>(ml.bs, n - s0);
+            a.Om_cur = j == 0 ? w.Omin : nullptr;
+            a.Om_next = j + 1 < nblk ? w.Omin + (size_t)(j + 1) * omsz : nullptr;
+            a.stop = dstop;
+            sp = span_begin(0, (double)a.n_new * (zb + rb + 8), outer, it);
+            HB_TRY(ring.step<S>(a, st));
+            span_end(sp);
           }
-        }
-      }
-      if (dev_stop) {
-        HB_CUDA(cudaMemcpyAsync(h_err + 3, w.stop, sizeof(int), cudaMemcpyDeviceToHost, st));
-        HB_CUDA(cudaStreamSynchronize(st));
-        if (h_err[3] > 0) {
-          done = h_err[3];
-          stop = true;
+          HB_TRY(launch_objective_finalize(ring.state(), w.Pr, w.theta, p.sigma, B, K, p.stabilized_penalty,
+                                           w.obj_acc, w.obj_out + it, st, dstop, it, p.tol_clustering));
         }
       }
     }
-    // the launches after the device stop returned at once: the state buffer advanced only
-    // through the iterations that ran
-    if (dev_stop) ring.cur = (int)((ring0 + (int64_t)done * nblk) % 3);
-    const int n_kobj = !early_stop ? p.max_iter_clustering : (dev_stop ? done : 0);
-    const bool read_kobj = n_kobj > 0;
-    if (read_kobj)
-      HB_CUDA(cudaMemcpyAsync(h_dbl + 1, w.obj_out, sizeof(double) * n_kobj,
-                              cudaMemcpyDeviceToHost, st));
-    {
-      int* err = h_err;
-      HB_CUDA(cudaMemcpyAsync(&err[0], w.mb.err, sizeof(int), cudaMemcpyDeviceToHost, st));
-      HB_CUDA(cudaMemcpyAsync(&err[1], w.err, sizeof(int), cudaMemcpyDeviceToHost, st));
-      HB_CUDA(cudaStreamSynchronize(st));
-      if (read_kobj) kobj.assign(h_dbl + 1, h_dbl + 1 + n_kobj);
-      if (err[0]) { set_error("block splitter candidate buffer overflow"); return HB_ERR_INTERNAL; }
-      if (err[1] == 7) { set_error("fp16 correction: |X| or |W| reaches 65504, outside the fp16 range; use bf16"); return HB_ERR_UNSUPPORTED; }
-      if (err[1]) { set_error("tensor-core wait timed out (code %d)", err[1]); return HB_ERR_TIMEOUT; }
-    }
-    if (out && out->kmeans_objectives) {
-      for (size_t i = 0; i < kobj.size(); ++i)
-        out->kmeans_objectives[(size_t)outer * p.max_iter_clustering + i] = kobj[i];
-    }
-    if (out && out->kmeans_iters) out->kmeans_iters[outer] = (int32_t)kobj.size();
-    objs.push_back(kobj.empty() ? 0.0 : kobj.back());
+    // objectives, ring position, outer convergence test, error flags (on the device)
+    OuterEndArgs oe{w.ctl, w.obj_out, w.objs, w.kobj, w.kiters, {w.O[0], w.O[1], w.O[2]}, outer, mc,
+                    ring0, nblk, (size_t)(B + 1) * K, p.tol_harmony, w.err, w.mb.err};
+    HB_TRY(launch_outer_end(oe, st));
 
     // ---- ridge correction (correction_batched.cu:17-130) -------------------
     if constexpr (tc_path) {
       HB_TRY(launch_tc_moments<S>(R, P->ldr, X, d, cell_index, w.m_chunks, (int)mch.size(), K, d,
-                                  (float*)w.Mpart, w.err, st));
+                                  (float*)w.Mpart, w.err, st, ogate));
     } else {
       HB_TRY(launch_accum<S, T, TA>(R, P->ldr, X, d, cell_index, w.m_chunks, (int)mch.size(), K, d,
-                                    (TA*)w.Mpart, st));
+                                    (TA*)w.Mpart, st, OminArgs{nullptr, nullptr, 1, 1}, ogate));
     }
     HB_TRY(launch_m_reduce<TA>((TA*)w.Mpart, mch.data(), (int)mch.size(), w.batch_chunk_off, K, B, d,
-                               w.M, st));
+                               w.M, st, ogate));
     CorrArgs ca{w.M, ring.state(), w.Pr, w.Nb, p.alpha, p.ridge_lambda, p.batch_prune_threshold,
                 p.prune, p.dynamic_lambda, K, B, d};
-    HB_TRY(launch_ridge_solve<T>(ca, (T*)w.W, st));
+    HB_TRY(launch_ridge_solve<T>(ca, (T*)w.W, st, ogate));
     if constexpr (tc_path) {
       HB_TRY(launch_tc_apply<S>(X, d, R, P->ldr, (const float*)w.W, cell_index, w.apply_tiles, (int)tiles.size(),
-                                K, d, Zhat, d, Zn, P->ldz, w.err, st));
+                                K, d, Zhat, d, Zn, P->ldz, w.err, st, ogate));
     } else {
       HB_TRY(launch_apply_t<T, S, S>(X, d, R, P->ldr, (T*)w.W, cell_index, w.apply_tiles,
-                                     (int)tiles.size(), K, d, Zhat, d, Zn, P->ldz, st));
+                                     (int)tiles.size(), K, d, Zhat, d, Zn, P->ldz, st, ogate));
     }
-    // outer convergence (_harmony/__init__.py:722-734)
-    const size_t m = objs.size();
-    if (m >= 2 && (objs[m - 2] - objs[m - 1]) < p.tol_harmony * std::fabs(objs[m - 2])) {
-      converged = 1;
-      break;
+    // the host stops enqueuing once it sees, without waiting, that an outer iteration ended the
+    // run; the iterations it enqueued before that return at once on the device
+    HB_CUDA(cudaMemcpyAsync(h_flag + 2 * outer, &w.ctl->ostop, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    HB_CUDA(cudaEventRecord(P->flag_events[outer], st));
+    while (checked <= outer) {
+      const cudaError_t q = cudaEventQuery(P->flag_events[checked]);
+      if (q == cudaErrorNotReady) {
+        if (cudaPeekAtLastError() == cudaErrorNotReady) cudaGetLastError();
+        break;
+      }
+      HB_CUDA(q);
+      if (h_flag[2 * checked] || h_flag[2 * checked + 1]) {
+        host_stop = true;
+        break;
+      }
+      ++checked;
     }
   }
-  {
-    // errors of the last correction (the loop checks the flags before each correction)
-    HB_CUDA(cudaMemcpyAsync(h_err + 2, w.err, sizeof(int), cudaMemcpyDeviceToHost, st));
-    HB_CUDA(cudaStreamSynchronize(st));
-    const int err = h_err[2];
-    if (err == 7) { set_error("fp16 correction: |X| or |W| reaches 65504, outside the fp16 range; use bf16"); return HB_ERR_UNSUPPORTED; }
-    if (err) { set_error("tensor-core wait timed out (code %d)", err); return HB_ERR_TIMEOUT; }
-  }
+  // ---- the one read of the run ------------------------------------------------
+  HB_CUDA(cudaMemcpyAsync(h_ctl, w.ctl, sizeof(RunCtl), cudaMemcpyDeviceToHost, st));
+  HB_CUDA(cudaMemcpyAsync(h_objs, w.objs, sizeof(double) * (mh + 1), cudaMemcpyDeviceToHost, st));
+  HB_CUDA(cudaMemcpyAsync(h_kiters, w.kiters, sizeof(int32_t) * mh, cudaMemcpyDeviceToHost, st));
+  if (out && out->kmeans_objectives && mc > 0)
+    HB_CUDA(cudaMemcpyAsync(h_kobj, w.kobj, sizeof(double) * mh * kstride, cudaMemcpyDeviceToHost, st));
+  HB_CUDA(cudaMemcpyAsync(&h_err[0], w.mb.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  HB_CUDA(cudaMemcpyAsync(&h_err[1], w.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  HB_CUDA(cudaStreamSynchronize(st));
+  if (h_err[0]) { set_error("block splitter candidate buffer overflow"); return HB_ERR_INTERNAL; }
+  if (h_err[1] == 7) { set_error("fp16 correction: |X| or |W| reaches 65504, outside the fp16 range; use bf16"); return HB_ERR_UNSUPPORTED; }
+  if (h_err[1]) { set_error("tensor-core wait timed out (code %d)", h_err[1]); return HB_ERR_TIMEOUT; }
+  const int n_outer = std::min(h_ctl->n_outer, mh);
+  const int converged = h_ctl->conv;
   if (prof) {
     *prof = hb_profile{};
     for (const Span& sp : spans) {
       float ms = 0.f;
       if (sp.e1 < 0) continue;
+      // launches after the device-side stop returned at once: not counted
+      if (sp.outer >= n_outer || sp.it >= h_kiters[sp.outer]) continue;
       HB_CUDA(cudaEventElapsedTime(&ms, P->events[sp.e0], P->events[sp.e1]));
       if (sp.cat == 0) { prof->block_launches++; prof->block_ms += ms; prof->block_bytes += sp.bytes; }
       else { prof->centroid_launches++; prof->centroid_ms += ms; prof->centroid_bytes += sp.bytes; }
@@ -672,9 +664,15 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
   }
   if (out) {
     if (out->objectives)
-      for (size_t i = 0; i < objs.size(); ++i) out->objectives[i] = objs[i];
-    if (out->n_objectives) *out->n_objectives = (int32_t)objs.size();
+      for (int i = 0; i <= n_outer; ++i) out->objectives[i] = h_objs[i];
+    if (out->n_objectives) *out->n_objectives = (int32_t)(n_outer + 1);
     if (out->converged) *out->converged = converged;
+    for (int o = 0; o < n_outer; ++o) {
+      if (out->kmeans_iters) out->kmeans_iters[o] = h_kiters[o];
+      if (out->kmeans_objectives)
+        for (int i = 0; i < h_kiters[o]; ++i)
+          out->kmeans_objectives[(size_t)o * mc + i] = h_kobj[(size_t)o * kstride + i];
+    }
   }
   return HB_OK;
 }

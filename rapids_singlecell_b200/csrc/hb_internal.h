@@ -43,10 +43,11 @@ int membership_build(const MembershipLayout& L, const MembershipBufs& B, const u
                      int32_t* lcat = nullptr, int32_t* ckey = nullptr, int n_batches = 0);
 // B.err (candidate overflow) is set by the builds and cleared only by membership_clear_err
 int membership_clear_err(const MembershipBufs& B, cudaStream_t st);
+// gate (optional): every launch of the build returns at once while *gate is non-zero
 int membership_build_dev(const MembershipLayout& L, const MembershipBufs& B, const uint32_t* seeds,
                          uint32_t seed0, int n_iters, const int32_t* cats, int32_t* idx,
                          cudaStream_t st, int32_t* lcat = nullptr, int32_t* ckey = nullptr,
-                         int n_batches = 0);
+                         int n_batches = 0, const int* gate = nullptr);
 
 // ---- SIMT kernels of the plain (fp32 / fp64) path ----------------------------
 // Row L2 normalisation, inverse norm clamped to 1e12 (reference semantics).
@@ -71,10 +72,11 @@ struct OminArgs {
 };
 
 // P[chunk][k][c] = sum over the chunk's cells i of W[i][k] * V[i][c]
+// (gate, here and below: nullptr, or a device flag; the launch returns at once while it is set)
 template <typename TS, typename TV, typename TA>
 int launch_accum(const TS* W, int ldw, const TV* V, int ldv, const int32_t* cell_index,
                  const AccumChunk* chunks, int n_chunks, int K, int d, TA* P, cudaStream_t st,
-                 OminArgs om = OminArgs{nullptr, nullptr, 1, 1});
+                 OminArgs om = OminArgs{nullptr, nullptr, 1, 1}, const int* gate = nullptr);
 
 // Y_norm[k] = l2norm(sum_chunks P[chunk][k]); optional 16-bit copy.
 template <typename TA, typename TY>
@@ -104,15 +106,50 @@ struct BlockArgs {
   int init_mode;        // no penalty, L1 clamp 1e-12 (initial R)
   void* pen_g;          // [B][K] of the storage type: the penalty table in global memory, used when
                         // the B x K tables do not fit in shared memory (many batches)
+  const int* stop;      // nullptr, or the device-side k-means stop: return at once when set
 };
 int launch_block_update_f32(const BlockArgs& a, const double* O_in, double* O_out, double* O_zero,
                             cudaStream_t st);
 int launch_block_update_f64(const BlockArgs& a, const double* O_in, double* O_out, double* O_zero,
                             cudaStream_t st);
 
+// stop (optional): the device-side k-means stop; the launch returns at once when it is set,
+// otherwise it applies the window-3 test to obj_out[-it .. 0] and sets *stop = it + 1
+// (clustering.cu:380-387)
 int launch_objective_finalize(const double* O, const double* Pr, const double* theta, double sigma,
                               int B, int K, int stabilized, double* obj_acc, double* obj_out,
-                              cudaStream_t st);
+                              cudaStream_t st, int* stop = nullptr, int it = 0, double tol = 0.0);
+
+// ---- device-side run control ----------------------------------------------------
+// A run enqueues its whole loop without a host sync: the k-means stop (window-3 test), the
+// outer convergence test and the error flags are evaluated on the device, and every launch
+// after the point where the loop would have ended returns at once (its gate is set).
+struct RunCtl {
+  int stop;     // k-means stop of the current outer iteration: 0 while running, else set
+  int ostop;    // the run has ended (converged, or an error flag was raised)
+  int conv;     // the last outer iteration passed the convergence test
+  int n_outer;  // outer iterations whose k-means loop ran
+};
+struct OuterEndArgs {
+  RunCtl* ctl;
+  const double* obj_out;  // k-means objectives of this outer iteration
+  double* objs;           // [max_iter_harmony + 1]: [0] initial, [o + 1] after outer iteration o
+  double* kobj;           // [max_iter_harmony][max_iter_clustering]
+  int32_t* kiters;        // [max_iter_harmony] k-means iterations run
+  double* Obuf[3];        // the state ring of the block updates
+  int outer, max_iter;    // this outer iteration; k-means launches enqueued per outer iteration
+  int ring0, nblk;        // ring position at the start of the loop; block updates per iteration
+  size_t o_elems;         // doubles per state buffer
+  double tol_harmony;
+  const int* err;         // tensor-core error flag
+  const int* mb_err;      // block splitter overflow flag
+};
+// outer iteration start: a converged run ends; the k-means gate opens unless the run has ended
+int launch_outer_begin(RunCtl* ctl, cudaStream_t st);
+// end of the k-means loop of one outer iteration: records the objectives, moves the state to
+// the ring position the host enqueued against (when the loop stopped early), applies the outer
+// convergence test (_harmony/__init__.py:722-734) and ends the run on an error flag
+int launch_outer_end(const OuterEndArgs& a, cudaStream_t st);
 
 // ---- tensor-core kernels of the 16-bit path ------------------------------------
 // 2-D tensor map over a row-major 16-bit matrix [rows][ld] for row gathers:
@@ -194,6 +231,8 @@ struct CenStreamArgs {
   void* Yn;              // [K][ldy] 16-bit normalised centroids (written by the reduction)
   int ldy;
   const int* stop;       // nullptr, or the device-side k-means stop: return at once when set
+  int kpb;               // keys per block (B + 1): every cell also counts toward key (block, B), the
+                         // block's column sums; 0: keys are independent
 };
 bool cs_supported(int d, int K, int nkeys, int ldz);
 int make_tile_map4(CUtensorMap* tm, const void* base, int64_t rows, int ld, int blocks, bool bf16);
@@ -211,11 +250,12 @@ struct CorrArgs {
   int K, B, d;
 };
 template <typename TW>
-int launch_ridge_solve(const CorrArgs& a, TW* W, cudaStream_t st);
+int launch_ridge_solve(const CorrArgs& a, TW* W, cudaStream_t st, const int* gate = nullptr);
 
 template <typename TA>
 int launch_m_reduce(const TA* P, const AccumChunk* h_chunks, int n_chunks,
-                    const int32_t* d_batch_chunk_off, int K, int B, int d, double* M, cudaStream_t st);
+                    const int32_t* d_batch_chunk_off, int K, int B, int d, double* M, cudaStream_t st,
+                    const int* gate = nullptr);
 
 struct ApplyTile {
   int64_t start;   // position in the batch-sorted cell list
@@ -225,17 +265,17 @@ struct ApplyTile {
 template <typename T, typename TS, typename TZ>
 int launch_apply_t(const T* X, int ldx, const TS* R, int ldr, const T* W, const int32_t* cell_index,
                    const ApplyTile* tiles, int n_tiles, int K, int d, T* Zhat, int ldzh, TZ* Zn,
-                   int ldz, cudaStream_t st);
+                   int ldz, cudaStream_t st, const int* gate = nullptr);
 
 // tensor-core correction of the 16-bit path (X, W float32; R, Z_norm 16-bit)
 template <typename H>
 int launch_tc_moments(const H* R, int ldr, const float* X, int ldx, const int32_t* cell_index,
                       const AccumChunk* chunks, int n_chunks, int K, int d, float* Mpart, int* err,
-                      cudaStream_t st);
+                      cudaStream_t st, const int* gate = nullptr);
 template <typename H>
 int launch_tc_apply(const float* X, int ldx, const H* R, int ldr, const float* W, const int32_t* cell_index,
                     const ApplyTile* tiles, int n_tiles, int K, int d, float* Zhat, int ldzh, H* Zn, int ldz,
-                    int* err, cudaStream_t st);
+                    int* err, cudaStream_t st, const int* gate = nullptr);
 
 // ---- host helpers -------------------------------------------------------------
 // Pinned host buffers for read-backs, reused across runs and never freed.  Copies into

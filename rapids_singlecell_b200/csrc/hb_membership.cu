@@ -23,7 +23,8 @@ __device__ __forceinline__ uint32_t seed_of(const uint32_t* seeds, uint32_t seed
 // ---------------------------------------------------------------------------
 // 1) 12-bit key histogram, one per iteration.
 __global__ void k_key_hist(int64_t n, const uint32_t* __restrict__ seeds,
-                           uint32_t seed0, uint32_t* __restrict__ hist) {
+                           uint32_t seed0, uint32_t* __restrict__ hist, const int* gate) {
+  if (gated(gate)) return;
   __shared__ uint32_t sh[kNumBins];
   const int c = blockIdx.y;
   const uint32_t seed = seed_of(seeds, seed0, c);
@@ -45,7 +46,8 @@ __global__ void k_boundary_bins(int64_t bs, int nb, const uint32_t* __restrict__
                                 int* __restrict__ bnd_slot, uint32_t* __restrict__ bnd_q,
                                 int* __restrict__ slot_bin, int* __restrict__ nslots,
                                 int16_t* __restrict__ lut, uint32_t* __restrict__ cand_cnt,
-                                int max_slots) {
+                                int max_slots, const int* gate) {
+  if (gated(gate)) return;
   __shared__ uint32_t cum[kNumBins];
   __shared__ uint32_t wsum[32];
   __shared__ int pbin[kMaxBlocks];
@@ -113,7 +115,8 @@ __global__ void k_collect_candidates(int64_t n, const uint32_t* __restrict__ see
                                      const int16_t* __restrict__ lut,
                                      uint32_t* __restrict__ cand_cnt,
                                      uint32_t* __restrict__ cand, int max_slots, int cap,
-                                     int* __restrict__ err) {
+                                     int* __restrict__ err, const int* gate) {
+  if (gated(gate)) return;
   __shared__ int16_t sl[kNumBins];
   const int c = blockIdx.y;
   const uint32_t seed = seed_of(seeds, seed0, c);
@@ -140,7 +143,8 @@ __global__ void k_select_splitters(int nb, int cap_pow2, const int* __restrict__
                                    const uint32_t* __restrict__ cand,
                                    const int* __restrict__ bnd_slot,
                                    const uint32_t* __restrict__ bnd_q,
-                                   uint32_t* __restrict__ split, int max_slots, int cap) {
+                                   uint32_t* __restrict__ split, int max_slots, int cap, const int* gate) {
+  if (gated(gate)) return;
   extern __shared__ uint32_t keys[];
   const int c = blockIdx.y, s = blockIdx.x;
   if (s >= nslots[c]) return;
@@ -186,7 +190,9 @@ __device__ __forceinline__ int block_of(uint32_t key, const uint32_t* sp, int nb
 //    block holds long runs of one batch (used by the O accumulation).
 __global__ void k_part_count(int64_t n, int nblk, int nsub, const int32_t* __restrict__ cats,
                              const uint32_t* __restrict__ seeds, uint32_t seed0,
-                             const uint32_t* __restrict__ split, uint32_t* __restrict__ counts, int ntiles) {
+                             const uint32_t* __restrict__ split, uint32_t* __restrict__ counts, int ntiles,
+                             const int* gate) {
+  if (gated(gate)) return;
   extern __shared__ uint32_t cnt[];   // [nblk * nsub]
   __shared__ uint32_t sp[kMaxBlocks];
   const int c = blockIdx.y, tile = blockIdx.x;
@@ -211,7 +217,8 @@ __global__ void k_part_count(int64_t n, int nblk, int nsub, const int32_t* __res
 // 6) Column scan over tiles: offsets[tile][bucket] = sum_{t'<tile} counts[t'][bucket];
 //    totals[bucket] = the column total.
 __global__ void k_part_scan(int nbk, int ntiles, const uint32_t* __restrict__ counts,
-                            uint32_t* __restrict__ offsets, uint32_t* __restrict__ totals) {
+                            uint32_t* __restrict__ offsets, uint32_t* __restrict__ totals, const int* gate) {
+  if (gated(gate)) return;
   __shared__ uint32_t wsum[32];
   __shared__ uint32_t carry_s;
   const int bk = blockIdx.x, c = blockIdx.y;
@@ -261,7 +268,8 @@ __global__ void __launch_bounds__(256) k_part_scatter(int64_t n, int64_t bs, int
                                                       const uint32_t* __restrict__ totals,
                                                       int ntiles, int32_t* __restrict__ idx,
                                                       int32_t* __restrict__ lcat, int32_t* __restrict__ ckey,
-                                                      int B) {
+                                                      int B, const int* gate) {
+  if (gated(gate)) return;
   extern __shared__ uint32_t dyn[];
   const int nbk = nblk * nsub;
   uint32_t* base = dyn;               // [nbk]
@@ -380,7 +388,7 @@ int membership_clear_err(const MembershipBufs& B, cudaStream_t st) {
 // overflow and never clears it (membership_clear_err).
 int membership_build_dev(const MembershipLayout& L, const MembershipBufs& B, const uint32_t* seeds,
                          uint32_t seed0, int n_iters, const int32_t* cats, int32_t* idx,
-                         cudaStream_t st, int32_t* lcat, int32_t* ckey, int n_batches) {
+                         cudaStream_t st, int32_t* lcat, int32_t* ckey, int n_batches, const int* gate) {
   const int nb = L.nblk - 1;
   const int sms = num_sms();
   const int nsub = cats ? L.nsub : 1;
@@ -389,34 +397,34 @@ int membership_build_dev(const MembershipLayout& L, const MembershipBufs& B, con
   int g = std::min(div_up(L.n, 256 * 8), 2 * sms);
   if (g < 1) g = 1;
   if (nb > 0) {
-  k_key_hist<<<dim3(g, n_iters), 256, 0, st>>>(L.n, seeds, seed0, B.hist);
+  k_key_hist<<<dim3(g, n_iters), 256, 0, st>>>(L.n, seeds, seed0, B.hist, gate);
   HB_LAUNCH_CHECK();
   k_boundary_bins<<<n_iters, 1024, 0, st>>>(L.bs, nb, B.hist, B.bnd_slot, B.bnd_q, B.slot_bin,
-                                            B.nslots, B.lut, B.cand_cnt, L.max_slots);
+                                            B.nslots, B.lut, B.cand_cnt, L.max_slots, gate);
   HB_LAUNCH_CHECK();
   k_collect_candidates<<<dim3(g, n_iters), 256, 0, st>>>(L.n, seeds, seed0, B.lut, B.cand_cnt, B.cand,
-                                                         L.max_slots, L.cap, B.err);
+                                                         L.max_slots, L.cap, B.err, gate);
   HB_LAUNCH_CHECK();
   const size_t smem = sizeof(uint32_t) * (size_t)L.cap;
   if (smem > 48 * 1024)
     HB_TRY(allow_max_dyn_smem((const void*)k_select_splitters));
   k_select_splitters<<<dim3(L.max_slots, n_iters), 512, smem, st>>>(
-      nb, L.cap, B.nslots, B.cand_cnt, B.cand, B.bnd_slot, B.bnd_q, B.split, L.max_slots, L.cap);
+      nb, L.cap, B.nslots, B.cand_cnt, B.cand, B.bnd_slot, B.bnd_q, B.split, L.max_slots, L.cap, gate);
   HB_LAUNCH_CHECK();
   }
   if (sizeof(uint32_t) * nbk > 48 * 1024)
     HB_TRY(allow_max_dyn_smem((const void*)k_part_count));
   k_part_count<<<dim3(L.ntiles, n_iters), 256, sizeof(uint32_t) * nbk, st>>>(
-      L.n, L.nblk, nsub, cats, seeds, seed0, B.split, B.counts, L.ntiles);
+      L.n, L.nblk, nsub, cats, seeds, seed0, B.split, B.counts, L.ntiles, gate);
   HB_LAUNCH_CHECK();
-  k_part_scan<<<dim3(nbk, n_iters), 1024, 0, st>>>(nbk, L.ntiles, B.counts, B.offsets, B.totals);
+  k_part_scan<<<dim3(nbk, n_iters), 1024, 0, st>>>(nbk, L.ntiles, B.counts, B.offsets, B.totals, gate);
   HB_LAUNCH_CHECK();
   const size_t ssm = sizeof(uint32_t) * 9 * (size_t)nbk;
   if (ssm > 48 * 1024)
     HB_TRY(allow_max_dyn_smem((const void*)k_part_scatter));
   k_part_scatter<<<dim3(L.ntiles, n_iters), 256, ssm, st>>>(L.n, L.bs, L.nblk, nsub, cats, seeds, seed0,
                                                            B.split, B.offsets, B.totals, L.ntiles, idx, lcat, ckey,
-                                                           n_batches);
+                                                           n_batches, gate);
   HB_LAUNCH_CHECK();
   return HB_OK;
 }

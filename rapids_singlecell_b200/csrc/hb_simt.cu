@@ -62,7 +62,9 @@ __global__ void __launch_bounds__(256) k_accum(const TS* __restrict__ W, int ldw
                                                const TV* __restrict__ V, int ldv,
                                                const int32_t* __restrict__ cell_index,
                                                const AccumChunk* __restrict__ chunks, int K,
-                                               int d, int ktiles, TA* __restrict__ P, OminArgs om) {
+                                               int d, int ktiles, TA* __restrict__ P, OminArgs om,
+                                               const int* gate) {
+  if (gated(gate)) return;
   constexpr int ROWS = sizeof(TA) == 8 ? 16 : 32;
   constexpr int NW = ROWS * ACC_BK / 256;  // W elements per thread per step
   constexpr int NV = ROWS * ACC_BD / 256;  // V elements per thread per step
@@ -178,29 +180,24 @@ __global__ void __launch_bounds__(256) k_accum(const TS* __restrict__ W, int ldw
 template <typename TS, typename TV, typename TA>
 int launch_accum(const TS* W, int ldw, const TV* V, int ldv, const int32_t* cell_index,
                  const AccumChunk* chunks, int n_chunks, int K, int d, TA* P, cudaStream_t st,
-                 OminArgs om) {
+                 OminArgs om, const int* gate) {
   if (n_chunks == 0) return HB_OK;
   const int ktiles = div_up(K, ACC_BK), dtiles = div_up(d, ACC_BD);
   k_accum<TS, TV, TA><<<dim3(n_chunks, ktiles * dtiles), 256, 0, st>>>(W, ldw, V, ldv, cell_index,
-                                                                       chunks, K, d, ktiles, P, om);
+                                                                       chunks, K, d, ktiles, P, om, gate);
   HB_LAUNCH_CHECK();
   return HB_OK;
 }
-template int launch_accum<float, float, float>(const float*, int, const float*, int, const int32_t*,
-                                               const AccumChunk*, int, int, int, float*, cudaStream_t, OminArgs);
-template int launch_accum<double, double, double>(const double*, int, const double*, int, const int32_t*,
-                                                  const AccumChunk*, int, int, int, double*, cudaStream_t, OminArgs);
-template int launch_accum<__half, float, float>(const __half*, int, const float*, int, const int32_t*,
-                                                const AccumChunk*, int, int, int, float*, cudaStream_t, OminArgs);
-template int launch_accum<__nv_bfloat16, float, float>(const __nv_bfloat16*, int, const float*, int,
-                                                       const int32_t*, const AccumChunk*, int, int, int,
-                                                       float*, cudaStream_t, OminArgs);
-template int launch_accum<__half, __half, float>(const __half*, int, const __half*, int, const int32_t*,
-                                                 const AccumChunk*, int, int, int, float*, cudaStream_t, OminArgs);
-template int launch_accum<__nv_bfloat16, __nv_bfloat16, float>(const __nv_bfloat16*, int,
-                                                               const __nv_bfloat16*, int, const int32_t*,
-                                                               const AccumChunk*, int, int, int, float*,
-                                                               cudaStream_t, OminArgs);
+#define HB_ACCUM_INST(TS, TV, TA)                                                                  \
+  template int launch_accum<TS, TV, TA>(const TS*, int, const TV*, int, const int32_t*, const AccumChunk*, \
+                                        int, int, int, TA*, cudaStream_t, OminArgs, const int*);
+HB_ACCUM_INST(float, float, float)
+HB_ACCUM_INST(double, double, double)
+HB_ACCUM_INST(__half, float, float)
+HB_ACCUM_INST(__nv_bfloat16, float, float)
+HB_ACCUM_INST(__half, __half, float)
+HB_ACCUM_INST(__nv_bfloat16, __nv_bfloat16, float)
+#undef HB_ACCUM_INST
 
 // Y_norm[k] = l2normalise(sum over chunks of P[chunk][k]) -- fixed summation
 // order (deterministic), float64 accumulation.  One CTA per centroid row; 8
@@ -298,6 +295,7 @@ template <typename T>
 __global__ void k_pen_table(BlockArgsDev p, T* __restrict__ pen) {
   __shared__ double red[32];
   const BlockArgs& a = p.a;
+  if (gated(a.stop)) return;
   const int K = a.K, B = a.B, k = blockIdx.x;
   double s = 0.0;
   for (int b = threadIdx.x; b < B; b += blockDim.x) {
@@ -339,6 +337,7 @@ __global__ void __launch_bounds__(BU_THREADS) k_block_update(BlockArgsDev p) {
   const T* Zn = (const T*)a.Zn;
   const T* Yn = (const T*)a.Yn;
   T* R = (T*)a.R;
+  if (gated(a.stop)) return;
 
   // zero the buffer the previous launch read
   if (p.O_zero)
@@ -573,8 +572,9 @@ int launch_block_update_f64(const BlockArgs& a, const double* O_in, double* O_ou
 __global__ void k_objective_finalize(const double* __restrict__ O, const double* __restrict__ Pr,
                                      const double* __restrict__ theta, double sigma, int B, int K,
                                      int stabilized, double* __restrict__ obj_acc,
-                                     double* __restrict__ obj_out) {
+                                     double* __restrict__ obj_out, int* stop, int it, double tol) {
   __shared__ double red[32];
+  if (gated(stop)) return;
   double acc = 0;
   for (int k = threadIdx.x; k < K; k += blockDim.x) {
     double col = 0;
@@ -588,15 +588,71 @@ __global__ void k_objective_finalize(const double* __restrict__ O, const double*
   }
   acc = block_sum(acc, red);
   if (threadIdx.x == 0) {
-    *obj_out = *obj_acc + sigma * acc;
+    const double obj = *obj_acc + sigma * acc;
+    *obj_out = obj;
     *obj_acc = 0.0;
+    // window-3 convergence of the k-means loop (clustering.cu:380-387) on this and the three
+    // previous objectives of the loop
+    if (stop && it >= 3) {
+      const double o = obj_out[-1] + obj_out[-2] + obj_out[-3];
+      const double nw = obj + obj_out[-1] + obj_out[-2];
+      if ((o - nw) < tol * fabs(o)) *stop = it + 1;
+    }
   }
 }
 
 int launch_objective_finalize(const double* O, const double* Pr, const double* theta, double sigma,
                               int B, int K, int stabilized, double* obj_acc, double* obj_out,
-                              cudaStream_t st) {
-  k_objective_finalize<<<1, 256, 0, st>>>(O, Pr, theta, sigma, B, K, stabilized, obj_acc, obj_out);
+                              cudaStream_t st, int* stop, int it, double tol) {
+  k_objective_finalize<<<1, 256, 0, st>>>(O, Pr, theta, sigma, B, K, stabilized, obj_acc, obj_out, stop,
+                                          it, tol);
+  HB_LAUNCH_CHECK();
+  return HB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Run control (one thread / one CTA; the flags are read by the gates of later launches)
+__global__ void k_outer_begin(RunCtl* c) {
+  if (c->conv) c->ostop = 1;
+  c->stop = c->ostop;
+}
+
+int launch_outer_begin(RunCtl* ctl, cudaStream_t st) {
+  k_outer_begin<<<1, 1, 0, st>>>(ctl);
+  HB_LAUNCH_CHECK();
+  return HB_OK;
+}
+
+__global__ void __launch_bounds__(256) k_outer_end(OuterEndArgs a) {
+  RunCtl* c = a.ctl;
+  if (gated(&c->ostop)) return;
+  const int st = *(volatile const int*)&c->stop;
+  const int done = st > 0 ? min(st, a.max_iter) : a.max_iter;
+  for (int i = threadIdx.x; i < done; i += blockDim.x) a.kobj[(size_t)a.outer * a.max_iter + i] = a.obj_out[i];
+  // the launches after the stop left the state where the last iteration put it; the host
+  // enqueued the rest of the loop against the ring position of a loop that ran to the end
+  const int s = (int)((a.ring0 + (int64_t)done * a.nblk) % 3);
+  const int e = (int)((a.ring0 + (int64_t)a.max_iter * a.nblk) % 3);
+  if (s != e) {
+    for (size_t i = threadIdx.x; i < a.o_elems; i += blockDim.x) a.Obuf[e][i] = a.Obuf[s][i];
+    __syncthreads();
+    // the buffer after the state is the next accumulation target: zero on entry
+    double* z = a.Obuf[(e + 1) % 3];
+    for (size_t i = threadIdx.x; i < a.o_elems; i += blockDim.x) z[i] = 0.0;
+  }
+  if (threadIdx.x == 0) {
+    a.kiters[a.outer] = done;
+    const double prev = a.objs[a.outer];
+    const double cur = done > 0 ? a.obj_out[done - 1] : 0.0;
+    a.objs[a.outer + 1] = cur;
+    c->n_outer = a.outer + 1;
+    if (*a.err || *a.mb_err) c->ostop = 1;
+    else if ((prev - cur) < a.tol_harmony * fabs(prev)) c->conv = 1;
+  }
+}
+
+int launch_outer_end(const OuterEndArgs& a, cudaStream_t st) {
+  k_outer_end<<<1, 256, 0, st>>>(a);
   HB_LAUNCH_CHECK();
   return HB_OK;
 }
@@ -605,7 +661,8 @@ int launch_objective_finalize(const double* O, const double* Pr, const double* t
 // Ridge moments: M[k][b+1][c] = sum over batch-b chunks of P, M[k][0] = sum_b.
 template <typename TA>
 __global__ void k_m_reduce(const TA* __restrict__ P, const int32_t* __restrict__ batch_chunk_off,
-                           int K, int B, int d, double* __restrict__ M) {
+                           int K, int B, int d, double* __restrict__ M, const int* gate) {
+  if (gated(gate)) return;
   extern __shared__ double sm[];
   double* part = sm;              // [RED_Y][d]
   double* row = sm + RED_Y * d;   // [d]
@@ -627,14 +684,16 @@ __global__ void k_m_reduce(const TA* __restrict__ P, const int32_t* __restrict__
 
 template <typename TA>
 int launch_m_reduce(const TA* P, const AccumChunk*, int, const int32_t* d_batch_chunk_off, int K,
-                    int B, int d, double* M, cudaStream_t st) {
+                    int B, int d, double* M, cudaStream_t st, const int* gate) {
   k_m_reduce<TA><<<K, dim3(32, RED_Y), sizeof(double) * (RED_Y + 2) * d, st>>>(P, d_batch_chunk_off,
-                                                                              K, B, d, M);
+                                                                              K, B, d, M, gate);
   HB_LAUNCH_CHECK();
   return HB_OK;
 }
-template int launch_m_reduce<float>(const float*, const AccumChunk*, int, const int32_t*, int, int, int, double*, cudaStream_t);
-template int launch_m_reduce<double>(const double*, const AccumChunk*, int, const int32_t*, int, int, int, double*, cudaStream_t);
+template int launch_m_reduce<float>(const float*, const AccumChunk*, int, const int32_t*, int, int, int, double*,
+                                    cudaStream_t, const int*);
+template int launch_m_reduce<double>(const double*, const AccumChunk*, int, const int32_t*, int, int, int, double*,
+                                     cudaStream_t, const int*);
 
 // ---------------------------------------------------------------------------
 // Ridge lambda (_harmony/__init__.py:454-480), closed-form arrowhead inverse
@@ -644,7 +703,8 @@ template int launch_m_reduce<double>(const double*, const AccumChunk*, int, cons
 // u = (M[0] + sum_j p_j M[j+1]) / c, so W costs O(B d) per cluster.
 // W is written as [B][K][d] so that each batch's K x d slice is contiguous.
 template <typename TW>
-__global__ void k_ridge_solve(CorrArgs a, TW* __restrict__ W) {
+__global__ void k_ridge_solve(CorrArgs a, TW* __restrict__ W, const int* gate) {
+  if (gated(gate)) return;
   extern __shared__ double sh[];
   double* f = sh;          // [B]
   double* p = sh + a.B;    // [B]
@@ -685,15 +745,15 @@ __global__ void k_ridge_solve(CorrArgs a, TW* __restrict__ W) {
 }
 
 template <typename TW>
-int launch_ridge_solve(const CorrArgs& a, TW* W, cudaStream_t st) {
+int launch_ridge_solve(const CorrArgs& a, TW* W, cudaStream_t st, const int* gate) {
   const size_t smem = sizeof(double) * 2 * a.B;
   if (smem > 48 * 1024) HB_TRY(allow_max_dyn_smem((const void*)k_ridge_solve<TW>));
-  k_ridge_solve<TW><<<a.K, 128, smem, st>>>(a, W);
+  k_ridge_solve<TW><<<a.K, 128, smem, st>>>(a, W, gate);
   HB_LAUNCH_CHECK();
   return HB_OK;
 }
-template int launch_ridge_solve<float>(const CorrArgs&, float*, cudaStream_t);
-template int launch_ridge_solve<double>(const CorrArgs&, double*, cudaStream_t);
+template int launch_ridge_solve<float>(const CorrArgs&, float*, cudaStream_t, const int*);
+template int launch_ridge_solve<double>(const CorrArgs&, double*, cudaStream_t, const int*);
 
 // ---------------------------------------------------------------------------
 // Correction apply (kernels_outer.cuh:41-65) fused with the L2 renormalisation
@@ -710,11 +770,15 @@ __global__ void __launch_bounds__(256) k_apply(const T* __restrict__ X, int ldx,
                                                const int32_t* __restrict__ cell_index,
                                                const ApplyTile* __restrict__ tiles, int K, int d,
                                                T* __restrict__ Zhat, int ldzh, TZ* __restrict__ Zn,
-                                               int ldz) {
+                                               int ldz, const int* gate) {
   using TC = compute_t<T>;
-  __shared__ TC rt[AP_TM][AP_KC + 1];
-  __shared__ TC wt[AP_KC][32 * DQ];
+  // clusters per staged W slice: 16 for float64 above 128 PCs, so the slice stays within the
+  // 48 KB of static shared memory
+  constexpr int KC = (sizeof(TC) == 8 && DQ > 4) ? 16 : AP_KC;
+  __shared__ TC rt[AP_TM][KC + 1];
+  __shared__ TC wt[KC][32 * DQ];
   __shared__ int64_t cid[AP_TM];
+  if (gated(gate)) return;
   const ApplyTile tl = tiles[blockIdx.x];
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   if (tid < AP_TM) cid[tid] = tid < tl.len ? (int64_t)cell_index[tl.start + tid] : -1;
@@ -724,20 +788,20 @@ __global__ void __launch_bounds__(256) k_apply(const T* __restrict__ X, int ldx,
 #pragma unroll
     for (int q = 0; q < DQ; ++q) acc[i][q] = TC(0);
   const T* Wb = W + (size_t)tl.batch * K * d;
-  for (int k0 = 0; k0 < K; k0 += AP_KC) {
+  for (int k0 = 0; k0 < K; k0 += KC) {
     __syncthreads();
-    for (int e = tid; e < AP_TM * AP_KC; e += 256) {
-      const int r = e / AP_KC, kk = e % AP_KC;
+    for (int e = tid; e < AP_TM * KC; e += 256) {
+      const int r = e / KC, kk = e % KC;
       const int64_t cell = cid[r];
       rt[r][kk] = (cell >= 0 && k0 + kk < K) ? (TC)to_f(R[cell * ldr + k0 + kk]) : TC(0);
     }
-    for (int e = tid; e < AP_KC * 32 * DQ; e += 256) {
+    for (int e = tid; e < KC * 32 * DQ; e += 256) {
       const int kk = e / (32 * DQ), c = e % (32 * DQ);
       wt[kk][c] = (k0 + kk < K && c < d) ? (TC)Wb[(size_t)(k0 + kk) * d + c] : TC(0);
     }
     __syncthreads();
 #pragma unroll 4
-    for (int kk = 0; kk < AP_KC; ++kk) {
+    for (int kk = 0; kk < KC; ++kk) {
       TC r[4];
 #pragma unroll
       for (int i = 0; i < 4; ++i) r[i] = rt[w * 4 + i][kk];
@@ -777,23 +841,18 @@ __global__ void __launch_bounds__(256) k_apply(const T* __restrict__ X, int ldx,
 template <typename T, typename TS, typename TZ>
 int launch_apply_t(const T* X, int ldx, const TS* R, int ldr, const T* W, const int32_t* cell_index,
                    const ApplyTile* tiles, int n_tiles, int K, int d, T* Zhat, int ldzh, TZ* Zn,
-                   int ldz, cudaStream_t st) {
+                   int ldz, cudaStream_t st, const int* gate) {
   if (n_tiles == 0) return HB_OK;
   const int dq = div_up(std::max(d, ldz), 32);
 #define HB_AP(DQv)                                                                                 \
   k_apply<T, TS, TZ, DQv><<<n_tiles, 256, 0, st>>>(X, ldx, R, ldr, W, cell_index, tiles, K, d, Zhat, \
-                                                   ldzh, Zn, ldz)
+                                                   ldzh, Zn, ldz, gate)
   if (dq <= 1) HB_AP(1);
   else if (dq <= 2) HB_AP(2);
   else if (dq <= 4) HB_AP(4);
-  else if constexpr (sizeof(T) == 4) {
-    if (dq <= 8) HB_AP(8);
-    else {
-      set_error("n_pcs=%d exceeds the supported maximum of 256", d);
-      return HB_ERR_UNSUPPORTED;
-    }
-  } else {
-    set_error("n_pcs=%d exceeds the supported maximum (256 for fp32, 128 for fp64)", d);
+  else if (dq <= 8) HB_AP(8);
+  else {
+    set_error("n_pcs=%d exceeds the supported maximum of 256", d);
     return HB_ERR_UNSUPPORTED;
   }
 #undef HB_AP
@@ -802,16 +861,16 @@ int launch_apply_t(const T* X, int ldx, const TS* R, int ldr, const T* W, const 
 }
 template int launch_apply_t<float, float, float>(const float*, int, const float*, int, const float*,
                                                  const int32_t*, const ApplyTile*, int, int, int,
-                                                 float*, int, float*, int, cudaStream_t);
+                                                 float*, int, float*, int, cudaStream_t, const int*);
 template int launch_apply_t<double, double, double>(const double*, int, const double*, int,
                                                     const double*, const int32_t*, const ApplyTile*,
                                                     int, int, int, double*, int, double*, int,
-                                                    cudaStream_t);
+                                                    cudaStream_t, const int*);
 template int launch_apply_t<float, __half, __half>(const float*, int, const __half*, int, const float*,
                                                    const int32_t*, const ApplyTile*, int, int, int,
-                                                   float*, int, __half*, int, cudaStream_t);
+                                                   float*, int, __half*, int, cudaStream_t, const int*);
 template int launch_apply_t<float, __nv_bfloat16, __nv_bfloat16>(
     const float*, int, const __nv_bfloat16*, int, const float*, const int32_t*, const ApplyTile*, int,
-    int, int, float*, int, __nv_bfloat16*, int, cudaStream_t);
+    int, int, float*, int, __nv_bfloat16*, int, cudaStream_t, const int*);
 
 }  // namespace hb

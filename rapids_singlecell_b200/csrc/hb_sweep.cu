@@ -205,21 +205,6 @@ __device__ __forceinline__ void stage_tile(const SweepArgs& a, TileIds t, int gt
   }
 }
 
-// ocol[k] += sum over batches b of (O[b][k] - Om[b][k]) (ocol zeroed by the caller).  The
-// loads of the first 2 nt entries are issued together (one L2 round trip when B K <= 2 nt),
-// then added into ocol.
-__device__ __forceinline__ void column_sums(const double* O, const double* Om, int B, int K, float* ocol,
-                                            int nt) {
-  const int ne = B * K;
-  double v0 = 0.0, v1 = 0.0;
-  const int e0 = threadIdx.x, e1 = threadIdx.x + nt;
-  if (e0 < ne) v0 = O[e0] - (Om ? Om[e0] : 0.0);
-  if (e1 < ne) v1 = O[e1] - (Om ? Om[e1] : 0.0);
-  if (e0 < ne) atomicAdd(&ocol[e0 % K], (float)v0);
-  if (e1 < ne) atomicAdd(&ocol[e1 % K], (float)v1);
-  for (int e = threadIdx.x + 2 * nt; e < ne; e += nt) atomicAdd(&ocol[e % K], (float)(O[e] - (Om ? Om[e] : 0.0)));
-}
-
 // Starts of the runs of equal batch in a tile (rows are ordered by batch inside
 // a block), ascending, terminated by nvalid.  Executed by one full warp.
 __device__ __forceinline__ void tile_runs(const int* cc, int nvalid, int* runs, int* nruns) {
@@ -277,9 +262,10 @@ __global__ void __launch_bounds__(128 * QS * NG, 1) k_tc_sweep(SweepArgs a, Swee
                           tc::smem_u32(sm + SL.offA + (uint32_t)(SL.nbuf * g + SL.nbuf - 1) * SL.atile)};
   const uint32_t sB = tc::smem_u32(sm + SL.offB);
   const size_t ldo = (size_t)(B + 1) * K;
-  // this CTA's share of the state carry (the batch rows; the column-sum row is not kept)
-  const int carry0 = (int)((int64_t)B * K * blockIdx.x / gridDim.x);
-  const int carry1 = (int)((int64_t)B * K * (blockIdx.x + 1) / gridDim.x);
+  // this CTA's share of the state carry: the batch rows and the column-sum row B, which the
+  // flush keeps equal to the sum of the batch rows
+  const int carry0 = (int)((int64_t)(B + 1) * K * blockIdx.x / gridDim.x);
+  const int carry1 = (int)((int64_t)(B + 1) * K * (blockIdx.x + 1) / gridDim.x);
 
   if (warp == 0) {
     tc::tmem_alloc(tmem_slot, (uint32_t)(NG * L.tcols));
@@ -338,7 +324,6 @@ __global__ void __launch_bounds__(128 * QS * NG, 1) k_tc_sweep(SweepArgs a, Swee
     crange[j] = make_int2(cmin, lo < hi ? cmax : cmin - 1);
   }
 
-  for (int k = tid; k < 256; k += NT) ocol_s[0][k] = 0.f;
   __syncthreads();
   for (int j = 0; j < a.nblk; ++j) {
     HB_TRACE(j, 0);
@@ -350,8 +335,8 @@ __global__ void __launch_bounds__(128 * QS * NG, 1) k_tc_sweep(SweepArgs a, Swee
     for (size_t e = (size_t)blockIdx.x * NT + tid; e < ldo; e += (size_t)gridDim.x * NT) Ozero[e] = 0.0;
     // one round of loads: this CTA's share of the state carry (O_in - old(this block) -
     // old(next block); the first NT entries, parked in shared memory below so that the flush
-    // before the grid arrival does not wait for L2), the column sums (into ocol, zeroed in the
-    // previous block) and the state entries of the first penalty rows
+    // before the grid arrival does not wait for L2), the column sums (row B of the state) and
+    // the state entries of the first penalty rows
     const bool carry_mine = carry0 + tid < carry1;
     double c_in = 0.0, c_mc = 0.0, c_mn = 0.0;
     if (carry_mine) {
@@ -373,9 +358,12 @@ __global__ void __launch_bounds__(128 * QS * NG, 1) k_tc_sweep(SweepArgs a, Swee
         opre[q] = (float)(Oin[o_at] - (Omc ? Omc[o_at] : 0.0));
       }
     }
-    if (!a.init_mode) column_sums(Oin, Omc, B, K, ocol, NT);
+    if (!a.init_mode)
+      for (int k = tid; k < K; k += NT) {
+        const size_t o_at = (size_t)B * K + k;
+        ocol[k] = (float)(Oin[o_at] - (Omc ? Omc[o_at] : 0.0));
+      }
     if (carry_mine) carry_s[tid] = c_in - c_mc - c_mn;  // read back by this thread at the flush
-    for (int k = tid; k < K; k += NT) ocol_s[(j + 1) & 1][k] = 0.f;
     __syncthreads();
     HB_TRACE(j, 1);
     // exponent offsets of the batches present: v = exp2(c2 (1 - s) + log2 pen)
@@ -397,7 +385,7 @@ __global__ void __launch_bounds__(128 * QS * NG, 1) k_tc_sweep(SweepArgs a, Swee
           if (q >= kPre) o = (float)(Oin[o_at] - (Omc ? Omc[o_at] : 0.0));
           const float E = prb[b] * ocol[k];
           const float denom = a.stabilized ? (o + E + 1.f) : (o + 1.f);
-          lp = thb[b] * log2f((E + 1.f) / denom);
+          lp = thb[b] * (tc::lg2_approx(E + 1.f) - tc::lg2_approx(denom));
         }
         pc = c2 + lp;
       }
@@ -540,12 +528,18 @@ __global__ void __launch_bounds__(128 * QS * NG, 1) k_tc_sweep(SweepArgs a, Swee
     // ---- flush the CTA's deltas and carry the state ------------------------------
     HB_TRACE(j, 6);
     __syncthreads();
-    for (int e = tid; e < (cmax - cmin + 1) * K; e += NT) {
-      const size_t o_at = (size_t)cmin * K + e;
-      float v = 0.f;
+    // one thread per cluster column: the CTA's batch rows, then their sum into row B
+    for (int k = tid; k < K; k += NT) {
+      float colv = 0.f;
+      for (int b = cmin; b <= cmax; ++b) {
+        const size_t o_at = (size_t)b * K + k;
+        float v = 0.f;
 #pragma unroll
-      for (int q = 0; q < NG; ++q) v += ((const float*)(sm + SL.offOsm + q * SL.osmBytes))[o_at];
-      if (v != 0.f) atomicAdd(&Oout[o_at], (double)v);
+        for (int q = 0; q < NG; ++q) v += ((const float*)(sm + SL.offOsm + q * SL.osmBytes))[o_at];
+        if (v != 0.f) atomicAdd(&Oout[o_at], (double)v);
+        colv += v;
+      }
+      if (colv != 0.f) atomicAdd(&Oout[(size_t)B * K + k], (double)colv);
     }
     // carry the state forward (O_in - old(this block) - old(next block)), spread over the CTAs
     if (carry_mine && carry_s[tid] != 0.0) atomicAdd(&Oout[carry0 + tid], carry_s[tid]);
@@ -589,9 +583,7 @@ __global__ void __launch_bounds__(128 * QS * NG, 1) k_tc_sweep(SweepArgs a, Swee
   if (blockIdx.x == 0) {
     const double* Of = a.Obuf[(a.b0 + a.nblk) % 3];
     float* ocol = ocol_s[0];
-    for (int k = tid; k < K; k += NT) ocol[k] = 0.f;
-    __syncthreads();
-    column_sums(Of, nullptr, B, K, ocol, NT);
+    for (int k = tid; k < K; k += NT) ocol[k] = (float)Of[(size_t)B * K + k];
     __syncthreads();
     double acc = 0.0;
     for (int e = tid; e < B * K; e += NT) {

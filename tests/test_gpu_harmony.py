@@ -226,3 +226,47 @@ def test_hundreds_of_batches_on_the_plain_paths(prec):
                                max_iter_clustering=3, tol_harmony=-np.inf, tol_clustering=-np.inf)
     assert info.n_outer == 2
     assert rel_maxabs(out, ref.Z_hat) < TOL[prec]
+
+
+def test_fp64_above_128_pcs():
+    """The default float64 dtype with 200 PCs and the default tolerances: both loops stop where
+    the oracle's stop, and Z_hat matches it to float64 rounding."""
+    spec = MixtureSpec(3000, 200, 6, 3, "dirichlet", (), 0.5, (0.8, 1.2))
+    Z, cats, _ = make_mixture(spec, 31)
+    Y0 = initial_centroids(Z, 30, 32)
+    out, info, ref = _run_both(Z, cats, 3, Y0, "fp64", n_clusters=30, max_iter_harmony=10,
+                               max_iter_clustering=20)
+    assert info.converged == ref.converged and info.n_outer == ref.n_outer
+    assert [len(k) for k in info.kmeans_objectives] == [len(k) for k in ref.kmeans_objectives]
+    np.testing.assert_allclose(info.objectives_harmony, ref.objectives_harmony, rtol=1e-9)
+    assert rel_maxabs(out, ref.Z_hat) < TOL["fp64"]
+
+
+@pytest.mark.parametrize("prec", ["fp32", "bf16"])
+def test_device_stops_and_profiled_launches(prec):
+    """The run enqueues its loops without waiting on the device: the k-means and outer stops are
+    taken on the device and the launches after them return at once.  The iteration counts are
+    the oracle's (same objectives), and the profile counts only the block updates that ran."""
+    from rapids_singlecell_b200.harmony import HarmonyProblem
+
+    cfg = make_config("C1", seed=5, n_cells=6000)
+    B, K = cfg["n_batches"], 40
+    Y0 = cfg["Y0"][:K]
+    kw = dict(n_clusters=K, max_iter_harmony=8, max_iter_clustering=30, tol_harmony=1e-3,
+              tol_clustering=1e-4)
+    X = torch.as_tensor(cfg["Z"], device="cuda")
+    prob = HarmonyProblem(X, cfg["cats"], B, torch.as_tensor(Y0, device="cuda"), np.full(B, 2.0),
+                          precision=prec, **kw)
+    _, info = prob.run(profile=True)
+    prob.close()
+    iters = [len(k) for k in info.kmeans_objectives]
+    assert info.n_outer == len(iters) and info.n_outer < 8 and info.converged, (info.n_outer, iters)
+    # the k-means loop stopped early in at least one outer iteration
+    assert all(0 < i <= 30 for i in iters) and min(iters) < 30, iters
+    nblk = -(-6000 // int(6000 * 0.05))
+    per_iter = 1 if prec == "bf16" else nblk  # one persistent sweep, or one launch per block
+    assert info.profile["block_launches"] == sum(iters) * per_iter
+    if prec == "fp32":
+        ref = ho.harmonize(cfg["Z"], cfg["cats"], B, Y0, dtype=np.float32,
+                           **{k: v for k, v in kw.items()})
+        assert iters == [len(k) for k in ref.kmeans_objectives]

@@ -124,11 +124,13 @@ HB_API size_t hb_plan_workspace_bytes(const hb_plan* plan);
  *   Y0            device [n_clusters, n_pcs] initial centroids, same dtype as X
  *   Z_hat         device [n_cells, n_pcs] output, same dtype as X
  * Limits: n_pcs <= 256 (<= 128 on the 16-bit path), n_clusters <= 256.
- * The call enqueues the whole loop on `stream` without waiting on the device: the k-means stop,
- * the outer convergence test and the error flags are evaluated on the device, and the launches
- * after the point where the loop ends return at once.  It synchronises the stream once, at the
- * end, to read the objectives and the status (non-blocking event queries in between let it
- * stop enqueuing early).
+ * The call enqueues the loop on `stream` without reading results back: the k-means stop, the
+ * outer convergence test and the error flags are evaluated on the device, and the launches after
+ * the point where the loop ends return at once.  The host stays at most two outer iterations
+ * ahead of the device (it sleeps on the end event of iteration o - 2 before enqueuing iteration
+ * o, while iteration o - 1 is still queued, so the device never waits for the host), stops
+ * enqueuing once an ended run shows in those events, and synchronises the stream once, at the
+ * end, to read the objectives and the status.
  */
 HB_API int hb_harmonize(hb_plan* plan, const void* X, const int32_t* cats, const int32_t* cell_index,
                  const int64_t* batch_offsets, const double* theta, const void* Y0,

@@ -490,7 +490,7 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
   int* h_err = (int*)(h_ctl + 1);
   while ((int)P->flag_events.size() < mh) {
     cudaEvent_t e;
-    HB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    HB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming | cudaEventBlockingSync));
     P->flag_events.push_back(e);
   }
 
@@ -521,13 +521,25 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
   const double zb = (double)d * P->ssz, rb = (double)K * P->ssz;
   // every k-means launch is gated on the device-side stop, and every correction launch on the
   // end of the run (RunCtl); with tol_clustering = -inf the window-3 test never passes
-  int* const dstop = w.stop;
-  const int* const ogate = &w.ctl->ostop;
+  // A run with both tolerances at -inf cannot stop early: its launches carry no gate (an error
+  // flag raised on the way is reported at the end of the run).
+  const bool can_stop = !(std::isinf(p.tol_clustering) && p.tol_clustering < 0) ||
+                        !(std::isinf(p.tol_harmony) && p.tol_harmony < 0);
+  int* const dstop = can_stop ? w.stop : nullptr;
+  const int* const ogate = can_stop ? &w.ctl->ostop : nullptr;
 
   int checked = 0;  // outer iterations whose end flags the host has seen
   bool host_stop = false;
   for (int outer = 0; outer < mh && !host_stop; ++outer) {
     const uint32_t seed = (uint32_t)((p.random_state + (uint64_t)outer * 1000003ull) & 0xffffffffull);
+    // the host stays at most two outer iterations ahead of the device: it sleeps on the end event
+    // of iteration outer - 2 while the device still has iteration outer - 1 queued
+    if (outer >= 2) {
+      HB_CUDA(cudaEventSynchronize(P->flag_events[outer - 2]));
+      for (; checked <= outer - 2 && !host_stop; ++checked)
+        host_stop = h_flag[2 * checked] || h_flag[2 * checked + 1];
+      if (host_stop) break;
+    }
     HB_TRY(launch_outer_begin(w.ctl, st));
     const int ring0 = ring.cur;
     for (int it0 = 0; it0 < mc; it0 += kMaxIterChunk) {

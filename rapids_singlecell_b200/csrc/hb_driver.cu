@@ -409,6 +409,8 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
   HB_CUDA(cudaMemsetAsync(w.obj_acc, 0, sizeof(double), st));
   HB_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
   HB_CUDA(cudaMemsetAsync(w.ctl, 0, sizeof(RunCtl), st));
+  // the sweep's grid-barrier counts (each sweep launch leaves them zero for the next)
+  HB_CUDA(cudaMemsetAsync(w.barrier, 0, 4 * sizeof(unsigned), st));
   // the splitter's overflow flag is read once per outer iteration: cleared once per run
   HB_TRY(membership_clear_err(w.mb, st));
 
@@ -448,7 +450,6 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
       sa.wait_ns = p.sweep_wait_ns > 0 ? (uint64_t)p.sweep_wait_ns : 2000000000ull;
       sa.unmet = (unsigned)p.test_unmet_arrivals;
       sa.stop = sweep_stop; sa.it = sweep_it; sa.tol = p.tol_clustering;
-      HB_CUDA(cudaMemsetAsync(w.barrier, 0, sizeof(unsigned), st));
       HB_TRY(launch_tc_sweep<S>(sa, st));
       ring.cur = (ring.cur + nb) % 3;
       return HB_OK;

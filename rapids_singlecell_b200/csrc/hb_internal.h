@@ -185,7 +185,7 @@ struct SweepArgs {
   int init_mode;
   int batch_sorted;        // the list is ordered by batch within each block
   int max_ctas;            // 0: one CTA per SM; otherwise at most this many CTAs
-  unsigned* barrier;       // zero on entry
+  unsigned* barrier;       // [2] arrival and exit counts: zero on entry, zeroed again by the launch
   uint64_t wait_ns;        // bound of each grid-barrier wait
   unsigned unmet;          // arrivals the barrier waits for beyond the grid's (test hook; 0)
   int* err;

@@ -615,6 +615,12 @@ __global__ void __launch_bounds__(128 * QS * NG, 1) k_tc_sweep(SweepArgs a, Swee
     tc::fence_after_sync();
     tc::tmem_dealloc(*tmem_slot, (uint32_t)(NG * L.tcols));
   }
+  // the grid barrier resets itself for the next launch: the last CTA out (every other CTA has
+  // passed its final wait) zeroes the arrival and exit counts
+  if (tid == 0 && atomicAdd(a.barrier + 1, 1u) == gridDim.x - 1) {
+    a.barrier[0] = 0u;
+    a.barrier[1] = 0u;
+  }
 }
 
 template <typename H, int NG, int QS>

@@ -82,7 +82,7 @@ class HarmonyProblem:
                  tol_clustering=1e-5, ridge_lambda=1.0, sigma=0.1, block_proportion=0.05,
                  random_state=0, stabilized_penalty=True, dynamic_lambda=True, alpha=0.2,
                  batch_prune_threshold=1e-5, stream=None, max_sweep_ctas=0, sweep_wait_ns=0,
-                 test_unmet_arrivals=0):
+                 test_unmet_arrivals=0, counts=None):
         self.lib = _lib.load()
         self.device = X.device
         self.X = X.contiguous()
@@ -90,11 +90,14 @@ class HarmonyProblem:
         self.n_batches = int(n_batches)
         if isinstance(cats, torch.Tensor):  # codes on the device: counted and sorted there
             self.cats = cats.to(device=self.device, dtype=torch.int32).contiguous()
-            N_b = torch.bincount(self.cats.long(), minlength=self.n_batches).cpu().numpy().astype(np.int64)
+            N_b = None if counts is not None else \
+                torch.bincount(self.cats.long(), minlength=self.n_batches).cpu().numpy().astype(np.int64)
         else:
             cats = np.asarray(cats, dtype=np.int32)
-            N_b = np.bincount(cats, minlength=self.n_batches).astype(np.int64)
+            N_b = None if counts is not None else np.bincount(cats, minlength=self.n_batches).astype(np.int64)
             self.cats = torch.as_tensor(cats, device=self.device)
+        if counts is not None:  # the cells per batch, already counted by the caller
+            N_b = np.asarray(counts, dtype=np.int64)
         # the engine sorts the cells by batch itself up to 4096 batches
         self.cell_index = None
         if self.n_batches > 4096:
@@ -411,7 +414,7 @@ def harmonize(
         tol_harmony=tol_harmony, tol_clustering=tol_clustering, ridge_lambda=ridge_lambda,
         sigma=sigma, block_proportion=block_proportion, random_state=random_state,
         stabilized_penalty=stabilized_penalty, dynamic_lambda=dynamic_lambda, alpha=alpha,
-        batch_prune_threshold=batch_prune_threshold)
+        batch_prune_threshold=batch_prune_threshold, counts=N_b)
     Z_hat, info = problem.run()
     problem.close()
     if info.converged and verbose:

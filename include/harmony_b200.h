@@ -236,7 +236,8 @@ HB_API int hb_tc_apply(const float* X, const void* R, int32_t ldr, const float* 
  * from `seed`, then up to max_iter Lloyd iterations over all cells with tensor-core (bf16)
  * assignment, stopping when |Y_new - Y_old|_F <= tol |Y_new|_F.  Y_out (float32
  * [n_clusters, n_pcs], device) receives the centres (not normalised); *n_iter_out the Lloyd
- * iterations run.  n_pcs <= 128, n_clusters <= 256 and <= n.  Synchronises the stream once
+ * iterations run.  n_pcs <= 128 with n_clusters <= 256, or n_pcs <= 256 with n_clusters <= 128;
+ * n_clusters <= n.  Synchronises the stream once
  * per iteration.  Replaces the cuML KMeans(init="k-means||", max_iter=25) fit of the
  * reference's _initialize_centroids (preprocessing/_harmony/__init__.py:290-323); cuML's
  * random streams are not reproduced. */

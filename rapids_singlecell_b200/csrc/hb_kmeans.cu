@@ -152,21 +152,27 @@ __global__ void __launch_bounds__(kSeedThreads) k_km_pick(const double* __restri
 struct KmLayout {
   TcLayout t;     // similarity tile geometry (dpad, kblk, npad, tcols)
   int nbK;        // 64-cluster blocks of the one-hot operand
+  int nM;         // 128-PC row blocks of the centre sums (M = 128 per MMA): 2 above 128 PCs
+  int nbufA;      // tile buffers: 2, or 1 above 128 PCs (the 64 KB tiles)
   int tcols_all;  // TMEM columns allocated
   uint32_t offA, offB, offH, offHn, offCnt, offBest, offRows, offMisc, bytes;
 };
 
 inline KmLayout km_layout(int d, int K) {
   KmLayout L{};
-  L.t.dpad = d <= 64 ? 64 : 128;
+  L.t.dpad = d <= 64 ? 64 : (d <= 128 ? 128 : 256);
   L.t.kblk = L.t.dpad / 64;
   L.t.npad = (K + 15) / 16 * 16;
   L.t.tcols = L.t.npad <= 128 ? 128 : 256;
   L.nbK = (L.t.npad + 63) / 64;
-  L.tcols_all = 2 * L.t.tcols;
+  L.nM = L.t.dpad > 128 ? 2 : 1;
+  L.nbufA = L.t.dpad > 128 ? 1 : 2;
+  int t = 32;
+  while (t < (1 + L.nM) * L.t.tcols) t <<= 1;
+  L.tcols_all = t;
   auto al = [](uint32_t x, uint32_t a) { return (x + a - 1) / a * a; };
   uint32_t o = 0;
-  L.offA = o; o += 2u * (uint32_t)L.t.kblk * 16384u;
+  L.offA = o; o += (uint32_t)L.nbufA * (uint32_t)L.t.kblk * 16384u;
   L.offB = o; o += (uint32_t)L.t.kblk * (uint32_t)L.t.npad * 128u;
   L.offH = al(o, 1024); o = L.offH + (uint32_t)L.nbK * 16384u;
   L.offHn = al(o, 16); o = L.offHn + (uint32_t)L.t.npad * 4u;
@@ -224,7 +230,8 @@ __global__ void __launch_bounds__(256, 1) k_km_assign(const H* __restrict__ Zh, 
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t tmem = *tmem_slot;
-  const uint32_t tacc = tmem + (uint32_t)L.tcols;  // centre sums: lane = PC, column = cluster
+  // centre sums: lane = PC (128-PC block mb at tacc + mb * tcols), column = cluster
+  const uint32_t tacc = tmem + (uint32_t)L.tcols;
   const int64_t ntiles = (n + 127) / 128;
   const uint32_t idesc1 = tc::idesc_f16(128, L.npad, is_bf16<H>::value, false, false);
   const uint32_t idesc2 = tc::idesc_f16(128, L.npad, is_bf16<H>::value, true, true);
@@ -242,7 +249,8 @@ __global__ void __launch_bounds__(256, 1) k_km_assign(const H* __restrict__ Zh, 
   uint32_t phase = 0;
   if ((int64_t)blockIdx.x < ntiles) gather_rows_swizzled(Zh, ldz, nullptr, 0, n, blockIdx.x, sA0, L, cid, ccat, nullptr);
   int buf = 0, it = 0;
-  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, buf ^= 1, ++it) {
+  const int bstep = KL.nbufA == 2 ? 1 : 0;  // with one tile buffer the next tile waits for this one's sums
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, buf ^= bstep, ++it) {
     tc::cp_async_wait_all();  // this tile's rows have landed
     tc::fence_proxy_async_smem();
     tc::fence_before_sync();
@@ -254,7 +262,7 @@ __global__ void __launch_bounds__(256, 1) k_km_assign(const H* __restrict__ Zh, 
     // the commit also covers the previous tile's sum MMA: its tile buffer and the one-hot
     // are free; the next tile's rows land while this one is assigned
     const int64_t nxt = tile + gridDim.x;
-    if (nxt < ntiles)
+    if (KL.nbufA == 2 && nxt < ntiles)
       gather_rows_swizzled(Zh, ldz, nullptr, 0, n, nxt, sA0 + (uint32_t)(buf ^ 1) * atile, L, cid + (buf ^ 1) * 128,
                            ccat + (buf ^ 1) * 128, nullptr);
     float best = -INFINITY;
@@ -296,22 +304,34 @@ __global__ void __launch_bounds__(256, 1) k_km_assign(const H* __restrict__ Zh, 
     if (tid == 0) {
       tc::fence_after_sync();
       const uint32_t sA = sA0 + (uint32_t)buf * atile;
-      for (int k = 0; k < 8; ++k) {  // 8 steps of 16 cells
-        const uint64_t ad = tc::sdesc_sw128(sA + (uint32_t)k * 2048u, 16384u, 1024u);
-        const uint64_t bd = tc::sdesc_sw128(sH + (uint32_t)k * 2u * (uint32_t)nbK * 1024u, 1024u, (uint32_t)nbK * 1024u);
-        tc::mma_f16(tacc, ad, bd, idesc2, (it > 0 || k > 0) ? 1u : 0u);
+      for (int mb = 0; mb < KL.nM; ++mb) {  // 128 PCs (two 64-value blocks) per MMA row block
+        for (int k = 0; k < 8; ++k) {  // 8 steps of 16 cells
+          const uint64_t ad = tc::sdesc_sw128(sA + (uint32_t)mb * 32768u + (uint32_t)k * 2048u, 16384u, 1024u);
+          const uint64_t bd =
+              tc::sdesc_sw128(sH + (uint32_t)k * 2u * (uint32_t)nbK * 1024u, 1024u, (uint32_t)nbK * 1024u);
+          tc::mma_f16(tacc + (uint32_t)(mb * L.tcols), ad, bd, idesc2, (it > 0 || k > 0) ? 1u : 0u);
+        }
       }
+      if (KL.nbufA == 1) tc::mma_commit(mbar);
+    }
+    if (KL.nbufA == 1) {
+      // one tile buffer: the next tile's rows are gathered once this tile's sums have read it
+      if (!tc::mbar_wait(mbar, phase, kMaxPolls)) atomicExch(err, 9);
+      phase ^= 1u;
+      tc::fence_after_sync();
+      if (tile + gridDim.x < ntiles)
+        gather_rows_swizzled(Zh, ldz, nullptr, 0, n, tile + gridDim.x, sA0, L, cid, ccat, nullptr);
     }
   }
-  // the sums out of TMEM: warp w reads PCs 32 (w % 4) .. + 31, its half of the clusters
+  // the sums out of TMEM: warp w reads PCs 128 mb + 32 (w % 4) .. + 31, its half of the clusters
   if (it > 0) {
     if (tid == 0) tc::mma_commit(mbar);
     if (!tc::mbar_wait(mbar, phase, kMaxPolls)) atomicExch(err, 9);
     tc::fence_after_sync();
   }
-  {
-    const int c = (warp & 3) * 32 + lane;
-    const uint32_t ta = tacc + ((uint32_t)((warp & 3) * 32) << 16);
+  for (int mb = 0; mb < KL.nM; ++mb) {
+    const int c = mb * 128 + (warp & 3) * 32 + lane;
+    const uint32_t ta = tacc + (uint32_t)(mb * L.tcols) + ((uint32_t)((warp & 3) * 32) << 16);
     float* out = P + (size_t)blockIdx.x * K * d;
     for (int k0 = c_lo; k0 < c_hi; k0 += 8) {
       float v[8];
@@ -340,12 +360,12 @@ template <typename H>
 __global__ void __launch_bounds__(256) k_km_update(const float* __restrict__ P, const float* __restrict__ C, int G,
                                                    int K, int d, float* __restrict__ Yf, H* __restrict__ Yh, int ldy,
                                                    float* __restrict__ hn, double* __restrict__ shift) {
-  __shared__ double part[8][128];
+  __shared__ double part[8][256];
   __shared__ double cpart[8];
   __shared__ double red[32];
   const int lane = threadIdx.x, y = threadIdx.y, t = y * 32 + lane;
   const int k = blockIdx.x;
-  for (int c = lane; c < d; c += 32) {  // d <= 128
+  for (int c = lane; c < d; c += 32) {  // d <= 256
     double s = 0.0;
 #pragma unroll 8
     for (int g = y; g < G; g += 8) s += (double)__ldg(P + ((size_t)g * K + k) * d + c);
@@ -449,8 +469,9 @@ HB_API int hb_kmeans_init(const float* X, int64_t n, int32_t n_pcs, int32_t n_cl
     set_error("hb_kmeans_init: bad argument");
     return HB_ERR_INVALID;
   }
-  if (d > 128 || K > 256) {
-    set_error("hb_kmeans_init: n_pcs=%d (at most 128) or n_clusters=%d (at most 256) out of range", d, K);
+  if (d > 256 || K > 256 || (d > 128 && K > 128)) {
+    set_error("hb_kmeans_init: n_pcs=%d, n_clusters=%d out of range (n_pcs <= 128 with n_clusters <= 256, "
+              "or n_pcs <= 256 with n_clusters <= 128)", d, K);
     return HB_ERR_UNSUPPORTED;
   }
   const int G = num_sms();

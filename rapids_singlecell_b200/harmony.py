@@ -204,6 +204,8 @@ def _integer_codes(labels):
     if labels.size == 0 or labels.min() < 0 or labels.max() > 16 * labels.size + (1 << 20):
         return None, 0
     present = np.bincount(labels) > 0
+    if present.all():  # every value 0 .. max present: the labels are their own codes
+        return labels.astype(np.int32, copy=False), int(present.size)
     remap = np.cumsum(present, dtype=np.int64) - 1
     return remap[labels].astype(np.int32), int(present.sum())
 
@@ -251,8 +253,8 @@ def default_n_clusters(n_cells: int) -> int:
 
 def seeded_centroids(Z: torch.Tensor, n_clusters: int, random_state: int) -> torch.Tensor:
     """``n_clusters`` distinct cells chosen by ``numpy.random.default_rng(random_state)``:
-    the initial centroids when the k-means initialisation does not apply (more than 128
-    PCs or more than 256 clusters)."""
+    the initial centroids when the k-means initialisation does not apply (more than 256
+    PCs or clusters, or more than 128 of both)."""
     rng = np.random.default_rng(random_state)
     idx = rng.choice(Z.shape[0], size=n_clusters, replace=False)
     return Z[torch.as_tensor(idx, device=Z.device)].contiguous()
@@ -398,7 +400,7 @@ def harmonize(
     X = X.to(torch.float64 if prec == "fp64" else torch.float32).contiguous()
 
     if init_centroids is None:
-        if n_pcs <= 128 and n_clusters <= 256:
+        if (n_pcs <= 128 and n_clusters <= 256) or (n_pcs <= 256 and n_clusters <= 128):
             Y0 = kmeans_centroids(X, n_clusters, random_state)
         else:
             Y0 = seeded_centroids(X, n_clusters, random_state)

@@ -75,7 +75,8 @@ def test_kmeans_init_validation_without_gpu():
     assert call(100, 10, 200) == _lib.HB_ERR_INVALID        # more clusters than cells
     assert call(100, 10, 5, max_iter=-1) == _lib.HB_ERR_INVALID
     assert call(100, 10, 5, tol=float("nan")) == _lib.HB_ERR_INVALID
-    assert call(1000, 129, 5) == _lib.HB_ERR_UNSUPPORTED    # more than 128 PCs
+    assert call(1000, 257, 5) == _lib.HB_ERR_UNSUPPORTED    # more than 256 PCs
+    assert call(1000, 129, 129) == _lib.HB_ERR_UNSUPPORTED  # more than 128 PCs and clusters
     assert call(1000, 10, 257) == _lib.HB_ERR_UNSUPPORTED   # more than 256 clusters
     assert call(1000, 10, 5, ws_bytes=16) == _lib.HB_ERR_WORKSPACE
     assert b"workspace" in lib.hb_last_error()

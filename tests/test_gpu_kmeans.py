@@ -64,7 +64,8 @@ def test_kmeans_rejects_sizes_out_of_range():
     assert st == _lib.HB_ERR_INVALID  # more clusters than cells
 
 
-@pytest.mark.parametrize("n,d,K", [(1000, 5, 7), (2500, 128, 256), (129, 64, 3), (4100, 33, 129)])
+@pytest.mark.parametrize("n,d,K", [(1000, 5, 7), (2500, 128, 256), (129, 64, 3), (4100, 33, 129),
+                                   (3000, 200, 100), (700, 256, 128), (5000, 129, 20)])
 def test_odd_shapes(n, d, K):
     """Few and many PCs and clusters, a last tile of one cell, clusters just past a 64-block:
     the seeding bit for bit, and Lloyd within the oracle's inertia."""

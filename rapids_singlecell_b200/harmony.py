@@ -185,29 +185,38 @@ def from_dlpack(x):
 
 
 def _integer_codes(labels):
+    """(codes, number of categories) of plain integer labels: ``_integer_codes_counts``
+    without the counts."""
+    codes, n, _ = _integer_codes_counts(labels)
+    return codes, n
+
+
+def _integer_codes_counts(labels):
     """Categorical codes of plain integer labels without pandas: the categories are the
     sorted distinct values, as ``astype("category")`` gives them.  Labels already on the GPU
     (a CUDA tensor, or any DLPack device array) are coded there (``torch.unique``) and stay
     there: the codes come back as an int32 CUDA tensor, as the reference keeps its ``cats``
     on the device (_utils/_multi_gpu.py:202-232).  Host labels must be non-negative and come
-    back as a NumPy array.  Returns (None, 0) for anything else."""
+    back as a NumPy array, with the cells per category (int64) as the third value (None for
+    device labels).  Returns (None, 0, None) for anything else."""
     labels = from_dlpack(labels)
     if isinstance(labels, torch.Tensor) and labels.is_cuda:
         if labels.dim() != 1 or labels.numel() == 0 or labels.dtype.is_floating_point or labels.dtype == torch.bool:
-            return None, 0
+            return None, 0, None
         uniq, inv = torch.unique(labels, sorted=True, return_inverse=True)
-        return inv.to(torch.int32), int(uniq.numel())
+        return inv.to(torch.int32), int(uniq.numel()), None
     if isinstance(labels, torch.Tensor):
         labels = labels.detach().numpy()
     if not isinstance(labels, np.ndarray) or labels.ndim != 1 or labels.dtype.kind not in "iu":
-        return None, 0
+        return None, 0, None
     if labels.size == 0 or labels.min() < 0 or labels.max() > 16 * labels.size + (1 << 20):
-        return None, 0
-    present = np.bincount(labels) > 0
+        return None, 0, None
+    counts = np.bincount(labels)
+    present = counts > 0
     if present.all():  # every value 0 .. max present: the labels are their own codes
-        return labels.astype(np.int32, copy=False), int(present.size)
+        return labels.astype(np.int32, copy=False), int(present.size), counts.astype(np.int64)
     remap = np.cumsum(present, dtype=np.int64) - 1
-    return remap[labels].astype(np.int32), int(present.sum())
+    return remap[labels].astype(np.int32), int(present.sum()), counts[present].astype(np.int64)
 
 
 def get_batch_codes(batch_mat, batch_key):
@@ -370,17 +379,18 @@ def harmonize(
     """
     Z = from_dlpack(Z)
     n_cells, n_pcs = (int(v) for v in Z.shape)
-    cats_np, n_batches = _integer_codes(batch_mat) if batch_key is None else (None, 0)
+    cats_np, n_batches, N_b = _integer_codes_counts(batch_mat) if batch_key is None else (None, 0, None)
     if cats_np is None:
         codes = get_batch_codes(batch_mat, batch_key)
         n_batches = int(codes.cat.categories.size)
         cats_np = np.asarray(codes.cat.codes.values, dtype=np.int32)
     if cats_np.shape[0] != n_cells:
         raise ValueError("batch labels must have one entry per cell")
-    if isinstance(cats_np, torch.Tensor):  # device codes: only the B counts come to the host
-        N_b = torch.bincount(cats_np.long(), minlength=n_batches).cpu().numpy().astype(np.int64)
-    else:
-        N_b = np.bincount(cats_np, minlength=n_batches).astype(np.int64)
+    if N_b is None:  # (host labels are counted with their codes)
+        if isinstance(cats_np, torch.Tensor):  # device codes: only the B counts come to the host
+            N_b = torch.bincount(cats_np.long(), minlength=n_batches).cpu().numpy().astype(np.int64)
+        else:
+            N_b = np.bincount(cats_np, minlength=n_batches).astype(np.int64)
     n_clusters, th = resolve_parameters(
         n_cells, N_b, n_clusters=n_clusters, max_iter_harmony=max_iter_harmony, theta=theta,
         tau=tau, block_proportion=block_proportion, dynamic_lambda=dynamic_lambda, alpha=alpha,

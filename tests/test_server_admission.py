@@ -21,16 +21,28 @@ def _server(sms=148, streams=8, budget=1 << 40):
     return srv
 
 
-def _req(n, block_proportion=0.05):
+def _req(n, block_proportion=0.05, n_clusters=4, precision="bf16"):
     return HarmonyRequest(np.zeros((n, 2), np.float32), np.zeros(n, np.int32), 1, None, np.ones(1),
-                          dict(n_clusters=4, block_proportion=block_proportion))
+                          dict(n_clusters=n_clusters, block_proportion=block_proportion), precision=precision)
 
 
 def test_sweep_ctas_wanted():
-    assert sweep_ctas_wanted(_req(1_000_000), 148) == 148   # 50,000-cell blocks: 391 tiles
-    assert sweep_ctas_wanted(_req(20_000), 148) == 8         # 1,000-cell blocks
+    # one CTA per two tiles of a block (two tile streams per CTA up to 128 clusters)
+    assert sweep_ctas_wanted(_req(1_000_000), 148) == 148    # 50,000-cell blocks: 391 tiles
+    assert sweep_ctas_wanted(_req(20_000), 148) == 4          # 1,000-cell blocks: 8 tiles
+    assert sweep_ctas_wanted(_req(20_000, n_clusters=200), 148) == 8  # one tile stream per CTA
     assert sweep_ctas_wanted(_req(100), 148) == 1
     assert sweep_ctas_wanted(_req(100_000, 1.0), 148) == 148
+    # the plain paths have no cooperative sweep: no SMs asked for
+    assert sweep_ctas_wanted(_req(20_000, precision="fp32"), 148) == 0
+    assert sweep_ctas_wanted(_req(20_000, precision="fp64"), 148) == 0
+
+
+def test_plain_requests_take_no_sms():
+    srv = _server(sms=148, streams=8)
+    assert srv._admit(10, 148) == 148   # a 16-bit request holds every SM
+    assert srv._admit(10, 0) == 0       # a plain request is admitted all the same
+    assert srv.sms_in_use == 148
 
 
 def test_grants_stay_within_the_sms():

@@ -49,7 +49,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="bf16", choices=["bf16", "fp16", "fp32"])
+    ap.add_argument("--precision", default="bf16", choices=["bf16", "fp16", "fp32", "fp64"],
+                    help="path of the headline line (bf16, fp16, fp32); fp64 with --profile-case only")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--sections", default="wide,batched,serving,pca,knn",
                     help="extra measurements on rank 0 beside the headline line: wide (the "
@@ -77,8 +78,9 @@ def run_profile_case(args):
     from rapids_singlecell_b200.synthetic import make_config
 
     cfg = make_config(WORKLOAD, seed=0, n_cells=args.profile_cells)
-    X = torch.as_tensor(cfg["Z"], device="cuda")
-    prob = HarmonyProblem(X, cfg["cats"], cfg["n_batches"], torch.as_tensor(cfg["Y0"], device="cuda"),
+    dt = torch.float64 if args.precision == "fp64" else torch.float32
+    X = torch.as_tensor(cfg["Z"], device="cuda").to(dt)
+    prob = HarmonyProblem(X, cfg["cats"], cfg["n_batches"], torch.as_tensor(cfg["Y0"], device="cuda").to(dt),
                           np.full(cfg["n_batches"], 2.0), precision=args.precision,
                           n_clusters=cfg["n_clusters"], max_iter_harmony=1,
                           max_iter_clustering=args.profile_inner,
@@ -695,6 +697,14 @@ def run_ours(args):
                  "max_abs_diff_16bit_vs_fp32": diff,
                  "rel_max_abs_diff_16bit_vs_fp32": diff / max(z32.abs().max().item(), 1e-300)}
         prob32.close()
+        del z32, z16
+        # the float64 plain path: the reference's default dtype, the drop-in of a bare
+        # harmony_integrate call (one timed step after one warm-up)
+        prob64 = HarmonyProblem(X.double(), cats, B, torch.as_tensor(cfg["Y0"], device=dev).double(), theta,
+                                precision="fp64", **common)
+        ms64, _ = timed(lambda: prob64.run(), 1, 1)
+        plain["fp64"] = {"value": cell_iters * world / (ms64 / 1e3), "ms_per_step": ms64}
+        prob64.close()
 
     if rank != 0:
         if dist is not None:
@@ -788,6 +798,9 @@ def run_ours(args):
 
 def main():
     args = parse()
+    if args.precision == "fp64" and not args.profile_case:
+        raise SystemExit("--precision fp64 is for --profile-case; the line reports the float64 path "
+                         "as plain_fp32.fp64")
     if args.profile_case:
         run_profile_case(args)
     elif args.impl == "reference":

@@ -149,8 +149,10 @@ __global__ void __launch_bounds__(256) k_accum(const TS* __restrict__ W, int ldw
 #pragma unroll 4
     for (int r = 0; r < ROWS; ++r) {
       TA wv[8], vv[4];
+      // cluster tk + 16 a: the 16 threads of a half-warp read 16 consecutive values (no bank
+      // conflicts; with tk * 8 + a they were 8 (fp64) or 4 (fp32) ways)
 #pragma unroll
-      for (int a = 0; a < 8; ++a) wv[a] = ws[r][tk * 8 + a];
+      for (int a = 0; a < 8; ++a) wv[a] = ws[r][tk + 16 * a];
 #pragma unroll
       for (int b = 0; b < 4; ++b) vv[b] = vs[r][td * 4 + b];
 #pragma unroll
@@ -167,7 +169,7 @@ __global__ void __launch_bounds__(256) k_accum(const TS* __restrict__ W, int ldw
   TA* out = P + (size_t)blockIdx.x * K * d;
 #pragma unroll
   for (int a = 0; a < 8; ++a) {
-    const int k = k0 + tk * 8 + a;
+    const int k = k0 + tk + 16 * a;
     if (k >= K) continue;
 #pragma unroll
     for (int b = 0; b < 4; ++b) {

@@ -317,8 +317,10 @@ __global__ void k_pen_table(BlockArgsDev p, T* __restrict__ pen) {
 // GT (global tables): the penalty table comes from k_pen_table and the observed-count deltas
 // go straight to O_out with float64 atomics, so shared memory holds no B x K table and any
 // number of batches fits.
+// Two CTAs per SM up to 128 clusters (at most 128 registers; in float64 the compiler otherwise
+// took 142, and one CTA of 8 warps per SM left the kernel latency-bound).
 template <typename T, int KPT, bool GT>
-__global__ void __launch_bounds__(BU_THREADS) k_block_update(BlockArgsDev p) {
+__global__ void __launch_bounds__(BU_THREADS, KPT <= 8 ? 2 : 1) k_block_update(BlockArgsDev p) {
   constexpr int DC = bu_dc<T>();
   constexpr int K16 = 16 * KPT;
   constexpr int NZ = BU_TM * DC / BU_THREADS;   // Z elements per thread per chunk
@@ -517,6 +519,10 @@ static int launch_block_form(const BlockArgsDev& p, size_t smem, cudaStream_t st
   const BlockArgs& a = p.a;
   const void* fn = (const void*)k_block_update<T, KPT, GT>;
   HB_TRY(allow_max_dyn_smem(fn));
+  // float64: the largest shared-memory carveout, so that two CTAs fit on an SM (563 -> 500 ms
+  // per C2 step with the 128-register bound); the float32 forms keep the default, which leaves
+  // them more L1 (with the largest carveout they measured 285 -> 334 ms)
+  if (sizeof(T) == 8) HB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   int occ = 1;
   HB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_block_update<T, KPT, GT>, BU_THREADS, smem));
   if (occ < 1) occ = 1;

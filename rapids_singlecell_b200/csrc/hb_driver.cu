@@ -411,7 +411,8 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
   HB_CUDA(cudaMemsetAsync(w.ctl, 0, sizeof(RunCtl), st));
   // the sweep's grid-barrier counts (each sweep launch leaves them zero for the next)
   HB_CUDA(cudaMemsetAsync(w.barrier, 0, 4 * sizeof(unsigned), st));
-  // the splitter's overflow flag is read once per outer iteration: cleared once per run
+  // the splitter's overflow flag ends the run on the device (k_outer_end) and is read at the
+  // end: cleared once per run
   HB_TRY(membership_clear_err(w.mb, st));
 
   S* Zn = (S*)w.Zn;

@@ -20,6 +20,7 @@ cell-iterations / max-over-ranks time.
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import subprocess
@@ -625,6 +626,10 @@ def run_ours(args):
         torch.cuda.synchronize()
         barrier()
         torch.cuda.synchronize()
+        # as timeit does: no garbage-collector pass inside the timed steps (a collection of the
+        # harness's objects once added ~95 ms to one end-to-end step)
+        gc.collect()
+        gc.disable()
         per = []
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -639,6 +644,7 @@ def run_ours(args):
             per.append(e0.elapsed_time(e1))
         end.record()
         torch.cuda.synchronize()
+        gc.enable()
         barrier()
         total_ms = start.elapsed_time(end)
         return max_over_ranks(total_ms) / steps, per

@@ -270,3 +270,25 @@ def test_device_stops_and_profiled_launches(prec):
         ref = ho.harmonize(cfg["Z"], cfg["cats"], B, Y0, dtype=np.float32,
                            **{k: v for k, v in kw.items()})
         assert iters == [len(k) for k in ref.kmeans_objectives]
+
+
+@pytest.mark.parametrize("prec", ["fp32", "bf16"])
+@pytest.mark.parametrize("kw", [dict(max_iter_harmony=1, max_iter_clustering=5),
+                                dict(max_iter_harmony=5, max_iter_clustering=10, tol_harmony=1e6),
+                                dict(max_iter_harmony=4, max_iter_clustering=12, tol_clustering=1.0)],
+                         ids=["one_outer", "converged_at_first_outer", "earliest_kmeans_stop"])
+def test_loop_edges_of_the_device_run_control(prec, kw):
+    """The edges of the device-side run control: a single outer iteration, a run that converges
+    after its first outer iteration (the later ones enqueued, or not, and skipped on the device),
+    and k-means loops that stop at the earliest point the window-3 rule allows (4 iterations)."""
+    cfg = make_config("C1", seed=7, n_cells=3000)
+    B = cfg["n_batches"]
+    labels = pd.Categorical.from_codes(cfg["cats"], categories=[f"b{i}" for i in range(B)])
+    Zt = torch.as_tensor(cfg["Z"], device="cuda")
+    out, info = harmonize(Zt, labels, None, init_centroids=cfg["Y0"][:20], precision=prec, return_info=True,
+                          n_clusters=20, **kw)
+    ref = ho.harmonize(cfg["Z"], cfg["cats"], B, cfg["Y0"][:20], dtype=np.float32, n_clusters=20, **kw)
+    assert info.n_outer == ref.n_outer and info.converged == ref.converged
+    assert [len(k) for k in info.kmeans_objectives] == [len(k) for k in ref.kmeans_objectives]
+    assert len(info.objectives_harmony) == ref.n_outer + 1
+    assert rel_maxabs(out.cpu().numpy(), ref.Z_hat) < (TOL["fp32"] if prec == "fp32" else 1e-3)

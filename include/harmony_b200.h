@@ -85,7 +85,18 @@ typedef struct hb_params {
   int32_t test_unmet_arrivals;  /* test hook, 0 in normal use: the sweep's grid barrier waits for this many
                                    arrivals more than its CTAs make, so every wait runs out (bounded by
                                    sweep_wait_ns) and the run must return HB_ERR_TIMEOUT */
+  int32_t sweep_form;           /* layout of the persistent sweep (16-bit path): 0 the engine's choice;
+                                   HB_SWEEP_2x2_2BUF ... HB_SWEEP_1x4_1BUF force one (HB_ERR_UNSUPPORTED
+                                   at the run when it does not fit the shared memory); set by the
+                                   autotuner (rapids_singlecell_b200.autotune) */
 } hb_params;
+
+/* Layouts of the persistent sweep: thread groups x threads per row, A tiles per group */
+#define HB_SWEEP_AUTO 0
+#define HB_SWEEP_2x2_2BUF 1  /* two 256-thread tile streams, two threads per row, two A tiles each */
+#define HB_SWEEP_2x2_1BUF 2
+#define HB_SWEEP_1x4_2BUF 3  /* one 512-thread tile stream, four threads per row */
+#define HB_SWEEP_1x4_1BUF 4
 
 typedef struct hb_plan hb_plan;
 

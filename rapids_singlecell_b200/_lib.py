@@ -24,6 +24,8 @@ HB_ERR_UNSUPPORTED = 6
 
 HB_FP32, HB_FP64, HB_BF16, HB_FP16 = 0, 1, 2, 3
 HB_KNN_SQEUCLIDEAN, HB_KNN_EUCLIDEAN, HB_KNN_COSINE, HB_KNN_INNER_PRODUCT = 0, 1, 2, 3
+# persistent-sweep layouts (hb_params.sweep_form): (thread groups, threads per row, A tiles)
+SWEEP_FORMS = {1: (2, 2, 2), 2: (2, 2, 1), 3: (1, 4, 2), 4: (1, 4, 1)}
 PRECISIONS = {"fp32": HB_FP32, "fp64": HB_FP64, "bf16": HB_BF16, "fp16": HB_FP16}
 
 # every symbol include/harmony_b200.h declares
@@ -63,6 +65,7 @@ class HbParams(ctypes.Structure):
         ("random_state", ctypes.c_uint64),
         ("sweep_wait_ns", ctypes.c_int64),
         ("test_unmet_arrivals", ctypes.c_int32),
+        ("sweep_form", ctypes.c_int32),
     ]
 
 

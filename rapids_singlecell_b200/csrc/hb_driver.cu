@@ -201,6 +201,10 @@ int validate(const hb_params& p) {
     set_error("test_unmet_arrivals must be 0 or 1");
     return HB_ERR_INVALID;
   }
+  if (p.sweep_form < HB_SWEEP_AUTO || p.sweep_form > HB_SWEEP_1x4_1BUF) {
+    set_error("sweep_form must be in [0, 4]");
+    return HB_ERR_INVALID;
+  }
   const int64_t nblk = (p.n_cells + p.block_size - 1) / p.block_size;
   if (nblk > kMaxBlocks) {
     set_error("block_proportion too small: %lld blocks per iteration (max %d)", (long long)nblk, kMaxBlocks);
@@ -450,6 +454,7 @@ int run_impl(hb_plan* P, const T* X, const int32_t* cats, const int32_t* cell_in
       sa.max_ctas = p.max_sweep_ctas; sa.barrier = w.barrier; sa.err = w.err;
       sa.wait_ns = p.sweep_wait_ns > 0 ? (uint64_t)p.sweep_wait_ns : 2000000000ull;
       sa.unmet = (unsigned)p.test_unmet_arrivals;
+      sa.form = p.sweep_form;
       sa.stop = sweep_stop; sa.it = sweep_it; sa.tol = p.tol_clustering;
       HB_TRY(launch_tc_sweep<S>(sa, st));
       ring.cur = (ring.cur + nb) % 3;

@@ -188,6 +188,7 @@ struct SweepArgs {
   unsigned* barrier;       // [2] arrival and exit counts: zero on entry, zeroed again by the launch
   uint64_t wait_ns;        // bound of each grid-barrier wait
   unsigned unmet;          // arrivals the barrier waits for beyond the grid's (test hook; 0)
+  int form;                // HB_SWEEP_*: 0 the launcher's choice, else a forced layout
   int* err;
   // device-side k-means stop (nullptr: none): the launch returns at once when *stop is set;
   // otherwise CTA 0 applies the window-3 test to obj_out[-it .. 0] and sets *stop = it + 1

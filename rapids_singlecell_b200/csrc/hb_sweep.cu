@@ -664,6 +664,20 @@ static int sweep_fits(const SweepLayout& SL, bool& fits) {
 template <typename H>
 int launch_tc_sweep(const SweepArgs& a, cudaStream_t st) {
   bool fits = false;
+  if (a.form != HB_SWEEP_AUTO) {  // a forced layout (the autotuner's choice)
+    const int ng = a.form <= HB_SWEEP_2x2_1BUF ? 2 : 1;
+    const int nbuf = (a.form == HB_SWEEP_2x2_2BUF || a.form == HB_SWEEP_1x4_2BUF) ? 2 : 1;
+    const SweepLayout SF = sweep_layout(a.d, a.K, a.B, a.ldr, ng, nbuf);
+    if (ng == 2) {
+      HB_TRY((sweep_fits<H, 2, 2>(SF, fits)));
+      if (fits) return launch_sweep_ng<H, 2, 2>(a, SF, st);
+    } else {
+      HB_TRY((sweep_fits<H, 1, 4>(SF, fits)));
+      if (fits) return launch_sweep_ng<H, 1, 4>(a, SF, st);
+    }
+    set_error("tensor-core sweep: layout %d does not fit in shared memory (B=%d K=%d d=%d)", a.form, a.B, a.K, a.d);
+    return HB_ERR_UNSUPPORTED;
+  }
   for (int nbuf = 2; nbuf >= 1; --nbuf) {
     const SweepLayout S2 = sweep_layout(a.d, a.K, a.B, a.ldr, 2, nbuf);
     HB_TRY((sweep_fits<H, 2, 2>(S2, fits)));

@@ -37,10 +37,11 @@ def make_params(n_cells, n_pcs, n_clusters, n_batches, *, precision="fp32", max_
                 max_iter_clustering=200, tol_harmony=1e-4, tol_clustering=1e-5, ridge_lambda=1.0,
                 sigma=0.1, block_proportion=0.05, random_state=0, stabilized_penalty=True,
                 dynamic_lambda=True, alpha=0.2, batch_prune_threshold=1e-5, max_sweep_ctas=0,
-                sweep_wait_ns=0, test_unmet_arrivals=0) -> HbParams:
+                sweep_wait_ns=0, test_unmet_arrivals=0, sweep_form=0) -> HbParams:
     """The engine's plan parameters (``hb_params``) for one problem.  ``sweep_wait_ns`` bounds each
     grid-barrier wait of the 16-bit sweep (0: 2 s); ``test_unmet_arrivals`` is a test hook that
-    makes those waits run out (0 in normal use)."""
+    makes those waits run out (0 in normal use); ``sweep_form`` forces a layout of the sweep
+    (``HB_SWEEP_*``, 0: the engine's choice; see ``rapids_singlecell_b200.autotune``)."""
     p = HbParams()
     p.n_cells = int(n_cells)
     p.n_pcs = int(n_pcs)
@@ -63,6 +64,7 @@ def make_params(n_cells, n_pcs, n_clusters, n_batches, *, precision="fp32", max_
     p.max_sweep_ctas = int(max_sweep_ctas)
     p.sweep_wait_ns = int(sweep_wait_ns)
     p.test_unmet_arrivals = int(test_unmet_arrivals)
+    p.sweep_form = int(sweep_form)
     return p
 
 
@@ -82,7 +84,7 @@ class HarmonyProblem:
                  tol_clustering=1e-5, ridge_lambda=1.0, sigma=0.1, block_proportion=0.05,
                  random_state=0, stabilized_penalty=True, dynamic_lambda=True, alpha=0.2,
                  batch_prune_threshold=1e-5, stream=None, max_sweep_ctas=0, sweep_wait_ns=0,
-                 test_unmet_arrivals=0, counts=None):
+                 test_unmet_arrivals=0, counts=None, sweep_form=0):
         self.lib = _lib.load()
         self.device = X.device
         self.X = X.contiguous()
@@ -116,7 +118,8 @@ class HarmonyProblem:
                         sigma=sigma, block_proportion=block_proportion, random_state=random_state,
                         stabilized_penalty=stabilized_penalty, dynamic_lambda=dynamic_lambda, alpha=alpha,
                         batch_prune_threshold=batch_prune_threshold, max_sweep_ctas=max_sweep_ctas,
-                        sweep_wait_ns=sweep_wait_ns, test_unmet_arrivals=test_unmet_arrivals)
+                        sweep_wait_ns=sweep_wait_ns, test_unmet_arrivals=test_unmet_arrivals,
+                        sweep_form=sweep_form)
         self.params = p
         self.plan = ctypes.c_void_p()
         _lib.check(self.lib.hb_plan_create(ctypes.byref(p), ctypes.byref(self.plan)))
@@ -364,6 +367,7 @@ def harmonize(
     precision: str | None = None,
     return_info: bool = False,
     device=None,
+    autotune=False,
 ):
     """Integrate ``Z`` (cells x PCs) across the batches in ``batch_mat[batch_key]``.
 
@@ -373,6 +377,9 @@ def harmonize(
     ``init_centroids`` (n_clusters x PCs) fixes the starting centroids,
     ``precision`` is one of "fp32", "fp64" (plain paths) or "bf16"/"fp16"
     (tensor-core paths); by default it follows the dtype of ``Z``.
+    ``autotune`` (16-bit paths): True times the persistent sweep's launch shapes on this
+    problem once per shape (``rapids_singlecell_b200.autotune``), a path also keeps the choices
+    in that JSON file.
     Returns the corrected embedding as a torch tensor on the GPU (and a
     ``HarmonyInfo`` when ``return_info``).  ``Z`` and integer ``batch_mat`` labels may
     be arrays of any library that exports DLPack; device arrays are used in place.
@@ -420,13 +427,24 @@ def harmonize(
             raise ValueError(
                 f"init_centroids must have shape ({n_clusters}, {n_pcs}), got {tuple(Y0.shape)}"
             )
+    tuned = {}
+    if autotune and prec in ("bf16", "fp16"):
+        from .autotune import tune_sweep
+
+        choice = tune_sweep(X, cats_np, n_batches, Y0, th, precision=prec, n_clusters=n_clusters,
+                            block_proportion=block_proportion, ridge_lambda=ridge_lambda, sigma=sigma,
+                            random_state=random_state, stabilized_penalty=stabilized_penalty,
+                            dynamic_lambda=dynamic_lambda, alpha=alpha,
+                            batch_prune_threshold=batch_prune_threshold, counts=N_b,
+                            cache_path=None if autotune is True else str(autotune))
+        tuned = {"sweep_form": choice["sweep_form"], "max_sweep_ctas": choice["max_sweep_ctas"]}
     problem = HarmonyProblem(
         X, cats_np, n_batches, Y0, th, precision=prec, n_clusters=n_clusters,
         max_iter_harmony=max_iter_harmony, max_iter_clustering=max_iter_clustering,
         tol_harmony=tol_harmony, tol_clustering=tol_clustering, ridge_lambda=ridge_lambda,
         sigma=sigma, block_proportion=block_proportion, random_state=random_state,
         stabilized_penalty=stabilized_penalty, dynamic_lambda=dynamic_lambda, alpha=alpha,
-        batch_prune_threshold=batch_prune_threshold, counts=N_b)
+        batch_prune_threshold=batch_prune_threshold, counts=N_b, **tuned)
     Z_hat, info = problem.run()
     problem.close()
     if info.converged and verbose:

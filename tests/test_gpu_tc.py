@@ -161,3 +161,38 @@ def test_device_kmeans_stop_follows_the_window_rule():
     assert its == [len(k) for k in ref_info.kmeans_objectives]
     assert min(its) < kw["max_iter_clustering"]  # the stop was exercised
     assert rel_maxabs(out.cpu().numpy(), ref.cpu().numpy()) < 5e-3
+
+
+def test_forced_sweep_forms_and_autotune(tmp_path):
+    """Every sweep layout that ``hb_params.sweep_form`` can force gives the plain fp32 result on
+    C2's shapes (150,000 cells), with and without a CTA cap; the autotuner picks one of them,
+    stores it in its cache and ``harmonize(autotune=path)`` reproduces the plain result."""
+    from rapids_singlecell_b200 import autotune as at
+
+    cfg = make_config("C2", seed=4, n_cells=150_000)
+    kw = dict(n_clusters=100, max_iter_harmony=2, max_iter_clustering=3, tol_harmony=-np.inf,
+              tol_clustering=-np.inf)
+    labels = pd.Categorical.from_codes(cfg["cats"], categories=[f"b{i}" for i in range(cfg["n_batches"])])
+    Z = torch.as_tensor(cfg["Z"], device="cuda", dtype=torch.float32)
+    ref = harmonize(Z, labels, None, init_centroids=cfg["Y0"], precision="fp32", **kw).cpu().numpy()
+    from rapids_singlecell_b200.harmony import HarmonyProblem
+    Y0 = torch.as_tensor(cfg["Y0"], device="cuda", dtype=torch.float32)
+    theta = np.full(cfg["n_batches"], 2.0)
+    for form, cap in [(1, 0), (2, 0), (3, 0), (4, 0), (1, 74), (4, 111)]:
+        prob = HarmonyProblem(Z, cfg["cats"].astype(np.int32), cfg["n_batches"], Y0, theta, precision="bf16",
+                              sweep_form=form, max_sweep_ctas=cap, **kw)
+        out, _ = prob.run()
+        prob.close()
+        err = rel_maxabs(out.cpu().numpy(), ref)
+        print(f"sweep form {form}, cap {cap}: rel max-abs vs plain fp32 {err:.3e}")
+        assert err < 5e-3
+    path = str(tmp_path / "sweep.json")
+    at._cache.clear()
+    out = harmonize(Z, labels, None, init_centroids=cfg["Y0"], precision="bf16", autotune=path, **kw)
+    key = at.shape_key(Z.device, "bf16", Z.shape[0], Z.shape[1], 100, cfg["n_batches"])
+    choice = at.cached(key)
+    print("autotune choice:", choice)
+    assert (choice["sweep_form"], choice["max_sweep_ctas"]) in at.candidates(
+        torch.cuda.get_device_properties(0).multi_processor_count)
+    assert sum(v is not None for v in choice["timings"].values()) >= 4
+    assert rel_maxabs(out.cpu().numpy(), ref) < 5e-3

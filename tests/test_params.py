@@ -121,3 +121,39 @@ def test_dlpack_inputs_share_memory():
     assert nb == 3 and codes.tolist() == [1, 0, 1, 2]
     a = np.zeros(3)
     assert from_dlpack(a) is a and from_dlpack([1, 2]) == [1, 2]
+
+
+def test_sweep_autotune_keys_and_cache(tmp_path):
+    """The autotuner's host side: shape keys bucket the cell count by half octaves, the candidates
+    cover every sweep layout, and choices round-trip through the JSON cache."""
+    from rapids_singlecell_b200 import _lib
+    from rapids_singlecell_b200 import autotune as at
+
+    k1 = at.shape_key("cpu", "bf16", 500_000, 50, 100, 8)
+    assert k1 == at.shape_key("cpu", "bf16", 520_000, 50, 100, 8)      # same half-octave bucket
+    assert k1 != at.shape_key("cpu", "bf16", 800_000, 50, 100, 8)
+    assert k1 != at.shape_key("cpu", "fp16", 500_000, 50, 100, 8)
+    cands = at.candidates(148)
+    assert {f for f, _ in cands} == set(_lib.SWEEP_FORMS) and {c for _, c in cands} == {0, 111, 74}
+    path = str(tmp_path / "sweep.json")
+    at.remember(k1, {"sweep_form": 2, "max_sweep_ctas": 74, "us_per_launch": 1.0, "timings": {}})
+    at.save_cache(path)
+    at._cache.clear()
+    assert at.cached(k1) is None
+    at.load_cache(path)
+    assert at.cached(k1)["sweep_form"] == 2
+
+
+def test_sweep_form_validation():
+    import ctypes
+
+    from rapids_singlecell_b200 import _lib
+    from rapids_singlecell_b200.harmony import make_params
+
+    lib = _lib.load()
+    plan = ctypes.c_void_p()
+    p = make_params(1000, 20, 10, 3, precision="bf16", sweep_form=5)
+    assert lib.hb_plan_create(ctypes.byref(p), ctypes.byref(plan)) == _lib.HB_ERR_INVALID
+    p = make_params(1000, 20, 10, 3, precision="bf16", sweep_form=3)
+    assert lib.hb_plan_create(ctypes.byref(p), ctypes.byref(plan)) == _lib.HB_OK
+    lib.hb_plan_destroy(plan)

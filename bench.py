@@ -754,7 +754,8 @@ def run_ours(args):
         "p50_ms": float(np.percentile(per, 50)), "p99_ms": float(np.percentile(per, 99)),
         "e2e": {"value": e2e_value, "unit": "cell-iters/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e,
-                "p50_ms": float(np.percentile(per_e2e, 50)), "p99_ms": float(np.percentile(per_e2e, 99))},
+                "p50_ms": float(np.percentile(per_e2e, 50)), "p99_ms": float(np.percentile(per_e2e, 99)),
+                "per_step_ms": [round(float(t), 2) for t in per_e2e]},
         "plain_fp32": plain,
         "roofline": roofline,
         "cpu_baseline": None,            # filled after the sections (host-side legs last)

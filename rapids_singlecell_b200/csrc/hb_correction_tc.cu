@@ -229,7 +229,7 @@ inline ApLayout ap_layout(int K, int d) {
 }
 
 template <typename H>
-__global__ void __launch_bounds__(256) k_tc_apply(const float* __restrict__ X, int ldx, const H* __restrict__ R,
+__global__ void __launch_bounds__(256, 2) k_tc_apply(const float* __restrict__ X, int ldx, const H* __restrict__ R,
                                                   int ldr, const float* __restrict__ W,
                                                   const int32_t* __restrict__ cell_index,
                                                   const ApplyTile* __restrict__ tiles, int n_tiles, int K, int d,
@@ -266,28 +266,43 @@ __global__ void __launch_bounds__(256) k_tc_apply(const float* __restrict__ X, i
   int cur_b = -1;
   bool bad = false;
   uint32_t phase = 0;
+  // the tile descriptor and row ids of the next tile are loaded a tile ahead (registers)
+  ApplyTile nxt = t0 < t1 ? tiles[t0] : ApplyTile{0, 0, 0};
+  int nid = (t0 < t1 && tid < nxt.len) ? cell_index[nxt.start + tid] : -1;
   for (int t = t0; t < t1; ++t) {
-    const ApplyTile tile = tiles[t];
+    const ApplyTile tile = nxt;
     if (tile.batch != cur_b) {
       // W_b (clusters x PCs) split into hi / lo parts; MN-major B operand, rows past K zero
       cur_b = tile.batch;
       const float* Wb = W + (size_t)cur_b * K * d;
-      for (int e = tid; e < L.npad * xch; e += 256) {
-        const int k = e / xch, c = e % xch;
-        float x[8];
+      constexpr int kWB = 4;  // (cluster, 8-PC chunk) items whose loads are in flight together
+      for (int e0 = tid; e0 < L.npad * xch; e0 += 256 * kWB) {
+        float x[kWB][8];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          const int col = c * 8 + i;
-          x[i] = (k < K && col < d) ? __ldg(Wb + (size_t)k * d + col) : 0.f;
+        for (int u = 0; u < kWB; ++u) {
+          const int e = e0 + u * 256;
+          const int k = e / xch, c = e % xch;
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            const int col = c * 8 + i;
+            x[u][i] = (e < L.npad * xch && k < K && col < d) ? __ldg(Wb + (size_t)k * d + col) : 0.f;
+          }
         }
-        __align__(16) H hi[8], lo[8];
-        split8<H>(x, hi, lo, bad);
-        const uint32_t off = mn_off((uint32_t)k, (uint32_t)(c >> 3), (uint32_t)(c & 7), (uint32_t)L.nbX);
-        *(uint4*)(sm + L.offWh + off) = *(const uint4*)hi;
-        *(uint4*)(sm + L.offWl + off) = *(const uint4*)lo;
+#pragma unroll
+        for (int u = 0; u < kWB; ++u) {
+          const int e = e0 + u * 256;
+          if (e < L.npad * xch) {
+            const int k = e / xch, c = e % xch;
+            __align__(16) H hi[8], lo[8];
+            split8<H>(x[u], hi, lo, bad);
+            const uint32_t off = mn_off((uint32_t)k, (uint32_t)(c >> 3), (uint32_t)(c & 7), (uint32_t)L.nbX);
+            *(uint4*)(sm + L.offWh + off) = *(const uint4*)hi;
+            *(uint4*)(sm + L.offWl + off) = *(const uint4*)lo;
+          }
+        }
       }
     }
-    if (tid < 128) ids[tid] = tid < tile.len ? cell_index[tile.start + tid] : -1;
+    if (tid < 128) ids[tid] = nid;
     __syncthreads();
     // R rows, K-major A tile (zero past ldr and for missing rows)
     for (int e = tid; e < 128 * rch; e += 256) {
@@ -311,6 +326,10 @@ __global__ void __launch_bounds__(256) k_tc_apply(const float* __restrict__ X, i
         c += dc;
         if (c >= d) { c -= d; ++r; }
       }
+    }
+    if (t + 1 < t1) {  // the next tile's descriptor and ids, in flight with this tile's copies
+      nxt = tiles[t + 1];
+      nid = tid < nxt.len ? cell_index[nxt.start + tid] : -1;
     }
     tc::cp_async_wait_all();
     tc::fence_proxy_async_smem();

@@ -558,8 +558,8 @@ def knn_section(dev, n=500_000, d=50, k=15):
 
 def run_sections(args, dev):
     out = {}
-    rates = tuple(float(r) for r in args.serving_rates.split(","))
-    fp32_rates = tuple(float(r) for r in args.serving_fp32_rates.split(","))
+    rates = tuple(float(r) for r in args.serving_rates.split(",") if r.strip())
+    fp32_rates = tuple(float(r) for r in args.serving_fp32_rates.split(",") if r.strip())
     for name in [s for s in args.sections.split(",") if s]:
         fn = {"wide": wide_section, "batched": batched_section,
               "serving": lambda d: serving_section(d, n_requests=args.serving_requests, rates=rates,

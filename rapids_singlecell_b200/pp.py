@@ -47,12 +47,16 @@ def harmony_integrate(
     verbose: bool = False,
     init_centroids=None,
     precision: str | None = None,
+    autotune=False,
     nclust: int | None = None,
     lamb: float | None = None,
     block_size: float | None = None,
     max_iter_kmeans: int | None = None,
 ) -> None:
-    """Integrate experiments with Harmony; writes ``adata.obsm[adjusted_basis]``."""
+    """Integrate experiments with Harmony; writes ``adata.obsm[adjusted_basis]``.
+
+    ``precision`` and ``autotune`` are this engine's own options (see ``harmonize``); every
+    other argument is the reference's (_harmony_integrate.py:15-250)."""
     if nclust is not None:
         n_clusters = nclust
     if lamb is not None:
@@ -122,7 +126,7 @@ def harmony_integrate(
         random_state=random_state, stabilized_penalty=stabilized_penalty,
         dynamic_lambda=dynamic_lambda, alpha=alpha,
         batch_prune_threshold=batch_prune_threshold, verbose=verbose,
-        init_centroids=init_centroids, precision=precision,
+        init_centroids=init_centroids, precision=precision, autotune=autotune,
     )
     adata.obsm[adjusted_basis] = Z_hat.cpu().numpy()
 

@@ -280,7 +280,7 @@ template int launch_centroid_reduce<float, __nv_bfloat16>(const float*, int, int
 // O_in + delta into O_out (zeroed beforehand), and zeroes O_zero (the buffer
 // the previous launch read), so no CTA ever reads a buffer another CTA of the
 // same launch is writing.
-constexpr int BU_TM = 64, BU_THREADS = 256;
+constexpr int BU_THREADS = 256;
 template <typename T> constexpr int bu_dc() { return sizeof(T) == 8 ? 16 : 32; }
 
 struct BlockArgsDev {
@@ -319,10 +319,12 @@ __global__ void k_pen_table(BlockArgsDev p, T* __restrict__ pen) {
 // number of batches fits.
 // Two CTAs per SM up to 128 clusters (at most 128 registers; in float64 the compiler otherwise
 // took 142, and one CTA of 8 warps per SM left the kernel latency-bound).
-template <typename T, int KPT, bool GT>
+// RPT rows per thread: tiles of TM = 16 RPT cells, each thread RPT rows x KPT clusters.
+template <typename T, int KPT, bool GT, int RPT>
 __global__ void __launch_bounds__(BU_THREADS, KPT <= 8 ? 2 : 1) k_block_update(BlockArgsDev p) {
   constexpr int DC = bu_dc<T>();
   constexpr int K16 = 16 * KPT;
+  constexpr int BU_TM = 16 * RPT;
   constexpr int NZ = BU_TM * DC / BU_THREADS;   // Z elements per thread per chunk
   constexpr int NY = K16 * DC / BU_THREADS;     // Y elements per thread per chunk
   const BlockArgs& a = p.a;
@@ -402,9 +404,9 @@ __global__ void __launch_bounds__(BU_THREADS, KPT <= 8 ? 2 : 1) k_block_update(B
     }
     __syncthreads();
     load_chunk(0);
-    T s[4][KPT];
+    T s[RPT][KPT];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < RPT; ++i)
 #pragma unroll
       for (int j = 0; j < KPT; ++j) s[i][j] = T(0);
     for (int ck = 0; ck < nchunk; ++ck) {
@@ -417,21 +419,21 @@ __global__ void __launch_bounds__(BU_THREADS, KPT <= 8 ? 2 : 1) k_block_update(B
       if (ck + 1 < nchunk) load_chunk((ck + 1) * DC);
 #pragma unroll 4
       for (int c = 0; c < DC; ++c) {
-        T z[4], y[KPT];
+        T z[RPT], y[KPT];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) z[i] = zt[(cg * 4 + i) * (DC + 1) + c];
+        for (int i = 0; i < RPT; ++i) z[i] = zt[(cg * RPT + i) * (DC + 1) + c];
 #pragma unroll
         for (int j = 0; j < KPT; ++j) y[j] = yt[(kg + 16 * j) * (DC + 1) + c];
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < RPT; ++i)
 #pragma unroll
           for (int j = 0; j < KPT; ++j) s[i][j] += z[i] * y[j];
       }
     }
     // epilogue: exp * penalty, L1 normalise, write, O delta, objective terms
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int row = cg * 4 + i;
+    for (int i = 0; i < RPT; ++i) {
+      const int row = cg * RPT + i;
       const int64_t cell = cid[row];
       const int cat = ccat[row];
       T v[KPT];
@@ -514,27 +516,54 @@ __global__ void __launch_bounds__(BU_THREADS, KPT <= 8 ? 2 : 1) k_block_update(B
   if (tid == 0 && tot != 0.0) atomicAdd(a.obj_acc, tot);
 }
 
-template <typename T, int KPT, bool GT>
-static int launch_block_form(const BlockArgsDev& p, size_t smem, cudaStream_t st) {
-  const BlockArgs& a = p.a;
-  const void* fn = (const void*)k_block_update<T, KPT, GT>;
+// Sets the form's function attributes and returns its CTAs per SM for `smem` bytes.
+template <typename T, int KPT, bool GT, int RPT>
+static int block_form_occ(size_t smem, int& occ) {
+  const void* fn = (const void*)k_block_update<T, KPT, GT, RPT>;
   HB_TRY(allow_max_dyn_smem(fn));
   // float64: the largest shared-memory carveout, so that two CTAs fit on an SM (563 -> 500 ms
   // per C2 step with the 128-register bound); the float32 forms keep the default, which leaves
   // them more L1 (with the largest carveout they measured 285 -> 334 ms)
   if (sizeof(T) == 8) HB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-  int occ = 1;
-  HB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_block_update<T, KPT, GT>, BU_THREADS, smem));
+  occ = 1;
+  HB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_block_update<T, KPT, GT, RPT>, BU_THREADS, smem));
   if (occ < 1) occ = 1;
-  const int64_t tiles = (a.n_new + BU_TM - 1) / BU_TM;
+  return HB_OK;
+}
+
+template <typename T, int KPT, bool GT, int RPT>
+static int launch_block_form(const BlockArgsDev& p, size_t smem, int occ, cudaStream_t st) {
+  const BlockArgs& a = p.a;
+  const int64_t tiles = (a.n_new + 16 * RPT - 1) / (16 * RPT);
   int grid = (int)std::min<int64_t>(std::max<int64_t>(tiles, 1), (int64_t)num_sms() * occ);
   if (GT && a.n_new > 0 && !a.init_mode) {
     k_pen_table<T><<<a.K, 256, 0, st>>>(p, (T*)a.pen_g);
     HB_LAUNCH_CHECK();
   }
-  k_block_update<T, KPT, GT><<<grid, BU_THREADS, smem, st>>>(p);
+  k_block_update<T, KPT, GT, RPT><<<grid, BU_THREADS, smem, st>>>(p);
   HB_LAUNCH_CHECK();
   return HB_OK;
+}
+
+// Rows per thread: 4 (64-cell tiles), or 3 (48-cell tiles) when that takes fewer row rounds per
+// CTA slot.  The tiles of a block are spread over all CTA slots, so a block of 391 tiles of 64
+// cells on 296 slots (C2, 25,000 cells) runs two rounds of 4 rows, as 521 tiles of 48 cells run
+// two rounds of 3.
+template <typename T, int KPT, bool GT>
+static int launch_block_rows(const BlockArgsDev& p, size_t tables, cudaStream_t st) {
+  constexpr int DC = bu_dc<T>();
+  auto smem_of = [&](int tm) {
+    return sizeof(T) * (tm * (DC + 1) + (size_t)16 * KPT * (DC + 1)) + tm * (sizeof(int64_t) + sizeof(int)) +
+           64 + tables;
+  };
+  int occ4 = 1, occ3 = 1;
+  HB_TRY((block_form_occ<T, KPT, GT, 4>(smem_of(64), occ4)));
+  HB_TRY((block_form_occ<T, KPT, GT, 3>(smem_of(48), occ3)));
+  const int64_t n = std::max<int64_t>(p.a.n_new, 1), sms = num_sms();
+  const int64_t rounds4 = ((n + 63) / 64 + sms * occ4 - 1) / (sms * occ4);
+  const int64_t rounds3 = ((n + 47) / 48 + sms * occ3 - 1) / (sms * occ3);
+  if (3 * rounds3 < 4 * rounds4) return launch_block_form<T, KPT, GT, 3>(p, smem_of(48), occ3, st);
+  return launch_block_form<T, KPT, GT, 4>(p, smem_of(64), occ4, st);
 }
 
 // Shared-memory tables while they fit (the O deltas of a CTA summed on chip); global tables
@@ -543,15 +572,15 @@ template <typename T, int KPT>
 static int launch_block_kpt(const BlockArgsDev& p, cudaStream_t st) {
   const BlockArgs& a = p.a;
   constexpr int DC = bu_dc<T>();
-  const size_t base = sizeof(T) * (BU_TM * (DC + 1) + (size_t)16 * KPT * (DC + 1)) +
-                      BU_TM * (sizeof(int64_t) + sizeof(int)) + 64;
+  const size_t base = sizeof(T) * (64 * (DC + 1) + (size_t)16 * KPT * (DC + 1)) +
+                      64 * (sizeof(int64_t) + sizeof(int)) + 64;
   const size_t tables = sizeof(T) * (size_t)2 * a.B * a.K;
-  if (base + tables <= 160 * 1024) return launch_block_form<T, KPT, false>(p, base + tables, st);
+  if (base + tables <= 160 * 1024) return launch_block_rows<T, KPT, false>(p, tables, st);
   if (!a.pen_g) {
     set_error("block update: no global penalty table for B=%d K=%d", a.B, a.K);
     return HB_ERR_INTERNAL;
   }
-  return launch_block_form<T, KPT, true>(p, base, st);
+  return launch_block_rows<T, KPT, true>(p, 0, st);
 }
 
 template <typename T>

@@ -221,6 +221,15 @@ class ClockSampler:
         except Exception:  # noqa: BLE001
             self.p = None
 
+    def wait_first_sample(self, limit_s=5.0):
+        """Returns once nvidia-smi has written its first line (its start-up, NVML included, is
+        then over), or after `limit_s`."""
+        t0 = time.perf_counter()
+        while self.p is not None and time.perf_counter() - t0 < limit_s:
+            if os.path.getsize(self.f.name) > 0 or self.p.poll() is not None:
+                return
+            time.sleep(0.02)
+
     def stop(self):
         if self.p is None:
             return None
@@ -664,7 +673,10 @@ def run_ours(args):
         if info.profile is not None:
             last["info"] = info
 
+    # the clock sampler starts before the warm-up steps, so that its start-up is not timed
     clocks = ClockSampler(local) if rank == 0 else None
+    if clocks:
+        clocks.wait_first_sample()
     ms, per = timed(step_resident, args.steps, args.warmup)
     clk = clocks.stop() if clocks else None
     prof = last["info"].profile
@@ -752,6 +764,7 @@ def run_ours(args):
         "config": config_dict(cfg, {"precision": args.precision,
                                     "parallelism": "replicas" if world > 1 else "single"}),
         "p50_ms": float(np.percentile(per, 50)), "p99_ms": float(np.percentile(per, 99)),
+        "per_step_ms": [round(float(t), 2) for t in per],
         "e2e": {"value": e2e_value, "unit": "cell-iters/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e,
                 "p50_ms": float(np.percentile(per_e2e, 50)), "p99_ms": float(np.percentile(per_e2e, 99)),

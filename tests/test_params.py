@@ -157,3 +157,19 @@ def test_sweep_form_validation():
     p = make_params(1000, 20, 10, 3, precision="bf16", sweep_form=3)
     assert lib.hb_plan_create(ctypes.byref(p), ctypes.byref(plan)) == _lib.HB_OK
     lib.hb_plan_destroy(plan)
+
+
+def test_sweep_autotune_host_rules():
+    """The tuner refuses the plain paths before touching a device, and its CTA caps stay valid on
+    a GPU with few SMs (0 = every SM, otherwise at least one CTA)."""
+    import numpy as np
+    import pytest
+
+    from rapids_singlecell_b200 import autotune as at
+
+    with pytest.raises(ValueError):
+        at.tune_sweep(np.zeros((10, 4), np.float32), np.zeros(10, np.int32), 1, None, np.ones(1),
+                      precision="fp32", n_clusters=2)
+    for sms in (1, 2, 3, 148):
+        caps = {c for _, c in at.candidates(sms)}
+        assert 0 in caps and all(c == 0 or 1 <= c <= sms for c in caps)

@@ -121,6 +121,10 @@ typedef struct hb_outputs {
   hb_profile* profile;        /* optional: filled when not NULL */
 } hb_outputs;
 
+/* Validates the parameters and builds a plan (no device memory).  HB_ERR_UNSUPPORTED for shapes
+ * the engine does not run: n_clusters > 256, n_pcs > 256 (> 128 on the 16-bit paths), and on the
+ * 16-bit paths a (n_pcs, n_clusters, n_batches) whose sweep tables and tiles do not fit one CTA's
+ * shared memory (asked of the sweep's layouts when a device is present, else at the launch). */
 HB_API int hb_plan_create(const hb_params* params, hb_plan** plan);
 HB_API void hb_plan_destroy(hb_plan* plan);
 HB_API size_t hb_plan_workspace_bytes(const hb_plan* plan);

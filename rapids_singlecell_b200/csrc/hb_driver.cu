@@ -228,6 +228,21 @@ int validate(const hb_params& p) {
               "use precision fp32 or fp64", p.n_batches * p.n_clusters);
     return HB_ERR_UNSUPPORTED;
   }
+  if (p.precision == HB_BF16 || p.precision == HB_FP16) {
+    // the sweep's shared memory also holds the tile buffers, the centroid tile and the staged
+    // R rows beside those tables: ask the layouts themselves (as the launch will)
+    bool fits = true;
+    if (tc_sweep_fits_any((int)p.n_pcs, (int)p.n_clusters, (int)p.n_batches, fits) != HB_OK) {
+      (void)cudaGetLastError();  // no device to ask here: the launch makes the same test
+      set_error("%s", "");
+      fits = true;
+    }
+    if (!fits) {
+      set_error("n_batches=%d with n_clusters=%d and n_pcs=%d does not fit the tensor-core sweep's shared "
+                "memory; use precision fp32 or fp64", p.n_batches, p.n_clusters, p.n_pcs);
+      return HB_ERR_UNSUPPORTED;
+    }
+  }
   if ((size_t)16 * p.n_batches > 200 * 1024) {
     set_error("n_batches=%d exceeds 12800 (ridge solve tables)", p.n_batches);
     return HB_ERR_UNSUPPORTED;

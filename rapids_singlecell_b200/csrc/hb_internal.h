@@ -197,6 +197,9 @@ struct SweepArgs {
   double tol;
 };
 
+// Whether one of the sweep's layouts fits a (d, K, B) shape in one CTA (the layouts and the
+// test launch_tc_sweep uses); an error status when the kernel's attributes cannot be read.
+int tc_sweep_fits_any(int d, int K, int B, bool& fits);
 template <typename H>
 int launch_tc_sweep(const SweepArgs& a, cudaStream_t st);
 

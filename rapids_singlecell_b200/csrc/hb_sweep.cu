@@ -706,6 +706,21 @@ int launch_tc_sweep(const SweepArgs& a, cudaStream_t st) {
 template int launch_tc_sweep<__half>(const SweepArgs&, cudaStream_t);
 template int launch_tc_sweep<__nv_bfloat16>(const SweepArgs&, cudaStream_t);
 
+int tc_sweep_fits_any(int d, int K, int B, bool& fits) {
+  const int ldr = (K + 7) / 8 * 8;
+  fits = false;
+  for (int ng = 2; ng >= 1 && !fits; --ng)
+    for (int nbuf = 2; nbuf >= 1 && !fits; --nbuf) {
+      const SweepLayout S = sweep_layout(d, K, B, ldr, ng, nbuf);
+      if (ng == 2) {
+        HB_TRY((sweep_fits<__nv_bfloat16, 2, 2>(S, fits)));
+      } else {
+        HB_TRY((sweep_fits<__nv_bfloat16, 1, 4>(S, fits)));
+      }
+    }
+  return HB_OK;
+}
+
 }  // namespace hb
 
 #ifdef HB_SWEEP_TRACE

@@ -196,3 +196,25 @@ def test_forced_sweep_forms_and_autotune(tmp_path):
         torch.cuda.get_device_properties(0).multi_processor_count)
     assert sum(v is not None for v in choice["timings"].values()) >= 4
     assert rel_maxabs(out.cpu().numpy(), ref) < 5e-3
+
+
+@pytest.mark.parametrize("d,K,B,ok", [(128, 256, 8, True), (128, 256, 64, False), (50, 100, 160, True),
+                                      (50, 100, 200, False)])
+def test_plan_rejects_sweep_shapes_that_do_not_fit(d, K, B, ok):
+    """The 16-bit plan asks the sweep's own layouts whether its tables, tiles and staged rows fit
+    one CTA's shared memory, so a shape that would fail at the launch (B * K within the table
+    bound, but 128 PCs with K = 256 and 64 batches, or 200 batches at K = 100) is refused when
+    the plan is made; no kernel runs here."""
+    import ctypes
+
+    from rapids_singlecell_b200.harmony import make_params
+
+    p = make_params(100_000, d, K, B, precision="bf16")
+    plan = ctypes.c_void_p()
+    st = lib().hb_plan_create(ctypes.byref(p), ctypes.byref(plan))
+    if ok:
+        assert st == _lib.HB_OK, lib().hb_last_error()
+        lib().hb_plan_destroy(plan)
+    else:
+        assert st == _lib.HB_ERR_UNSUPPORTED
+        assert b"shared" in lib().hb_last_error()

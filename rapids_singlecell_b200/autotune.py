@@ -16,6 +16,7 @@ import json
 import math
 import os
 import threading
+import warnings
 
 import numpy as np
 import torch
@@ -44,12 +45,22 @@ def candidates(sms: int) -> list[tuple[int, int]]:
 
 
 def load_cache(path: str) -> None:
-    """Adds the choices stored at ``path`` (JSON) to the in-memory cache."""
-    if os.path.exists(path):
+    """Adds the choices stored at ``path`` (JSON) to the in-memory cache; a file that cannot be
+    read as a JSON object of choices is ignored with a warning (the shapes are then re-timed and
+    the file rewritten)."""
+    if not os.path.exists(path):
+        return
+    try:
         with open(path) as f:
             data = json.load(f)
-        with _lock:
-            _cache.update(data)
+        if not isinstance(data, dict) or not all(isinstance(v, dict) and "sweep_form" in v
+                                                 for v in data.values()):
+            raise ValueError("not a map of sweep choices")
+    except (OSError, ValueError) as e:
+        warnings.warn(f"sweep autotune cache {path!r} ignored: {e}", RuntimeWarning, stacklevel=2)
+        return
+    with _lock:
+        _cache.update(data)
 
 
 def save_cache(path: str) -> None:

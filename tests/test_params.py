@@ -173,3 +173,19 @@ def test_sweep_autotune_host_rules():
     for sms in (1, 2, 3, 148):
         caps = {c for _, c in at.candidates(sms)}
         assert 0 in caps and all(c == 0 or 1 <= c <= sms for c in caps)
+
+
+def test_sweep_autotune_bad_cache_file_is_ignored(tmp_path):
+    import pytest
+
+    from rapids_singlecell_b200 import autotune as at
+
+    bad = tmp_path / "sweep.json"
+    bad.write_text("{not json")
+    at._cache.clear()
+    with pytest.warns(RuntimeWarning):
+        at.load_cache(str(bad))
+    bad.write_text('{"k": 3}')
+    with pytest.warns(RuntimeWarning):
+        at.load_cache(str(bad))
+    assert at._cache == {}
